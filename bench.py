@@ -1,0 +1,317 @@
+"""Benchmark of the B200 flux pass (one JSON line on rank 0).
+
+Workload (N=1): the 3D Sedov-type blast on a static Voronoi mesh of 262,144
+generators uniform in the reflective unit cube (seed 2), gamma 5/3, HLLC
+solver, global CFL-0.4 time step; a "step" is one full pass of the hot path
+(gradients -> face fluxes -> update_Q/get_W) over the mesh.  The metric is
+face-steps per second (one nonzero-area face processed in one time step,
+with its share of the gradient and update work).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|split]
+
+Timing: CUDA events on the stream the library launches on, barrier +
+synchronize on both sides, max over ranks; W untimed warm-up steps.  The
+step's working set (about 300 MB: faces, cells, gradients, per-face fluxes)
+is larger than the 126 MB L2, so no separate L2 flush is done.
+
+N>1: every rank runs its own replica of the mesh (independent meshes, no
+data-path collective): weak scaling.
+
+--impl reference times the reference's own CPU flux pass (the unmodified
+Shadowfax sources built into oracle/_ref) on the host cores on the same mesh.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_GEN = 262_144
+SEED = 2
+METRIC = "faces/s (face-steps per second) of the flux pass"
+UNIT = "face-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--n", type=int, default=N_GEN, help="generators (default: config size)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region"""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(dim: int, n_cells: int, n_faces: int, nnz: int, precision: str):
+    """bytes each kernel of one step must move at least once (FP64 plain):
+    gradients: read W, pos, centroid, volume, CSR (offsets + entries) per
+    cell; per face area, midpoint, left, right, kind, right generator
+    position; write the gradient (dim*S) per cell.
+    faces: read the face record, per cell W, gradient, centroid, pos, Q.m,
+    total area; write dQ (S) per face.
+    update: read Q, volume, CSR, dQ per face; write Q and W per cell."""
+    S = dim + 2
+    face_rec = 8 + 8 * dim + 4 + 4 + 4 + 8 * dim
+    cell_grad_in = 8 * S + 8 * dim + 8 * dim + 8 + 4
+    grad = n_cells * (cell_grad_in + 8 * dim * S) + nnz * 4 + n_faces * face_rec
+    faces = n_faces * (face_rec + 8 * S) + n_cells * (8 * S + 8 * dim * S + 8 * dim + 8 * dim + 8 + 8)
+    update = n_cells * (8 * S + 8 + 4 + 8 * S * 2) + nnz * 4 + n_faces * (8 * S + 8)
+    return {"gradients": grad, "faces": faces, "update": update}
+
+
+def build_problem(n: int):
+    from shadowfax_b200 import workloads as wl
+    return wl.sedov3d(n=n, seed=SEED, solver="HLLC")
+
+
+def cpu_baseline(pr, steps: int = 3):
+    """reference CPU pass (oracle/_ref, unmodified Shadowfax sources), one
+    core, on the same mesh for a bounded number of steps"""
+    from oracle.oracle import Params, ref_binary, run_reference
+    exe = ref_binary(3, "libm")
+    if not exe.exists():
+        return None
+    p = Params(solver=pr.solver, gamma=pr.gamma, use_libm_pow=True)
+    r = run_reference(pr.mesh, p, pr.dt, steps + 1, pr.W0, pow_kind="libm")
+    secs = float(np.sum(r["step_seconds"][1:]))
+    value = pr.mesh.n_active_faces * steps / secs
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{steps} timed steps (+1 warm-up) of the full {pr.mesh.n_cells}-cell "
+                      f"mesh, reference VorCell/VorFace/HLLC loops, 1 MPI rank (single thread)"}
+
+
+def run_reference_arm(args, rank, world):
+    """--impl reference: the reference's own CPU pass on the host cores"""
+    if rank != 0:
+        return
+    pr = build_problem(args.n)
+    steps = max(1, min(args.steps, 5))
+    from oracle.oracle import ref_binary
+    if not ref_binary(3, "libm").exists():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref reference harness not built (needs the reference tree)"}))
+        return
+    cb = cpu_baseline(pr, steps)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * pr.mesh.n_active_faces / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"sedov3d HLLC, {pr.mesh.n_cells} generators, "
+                                   f"{pr.mesh.n_active_faces} faces, reflective unit cube",
+                       "solver": "HLLC", "precision": "fp64"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    torch.cuda.set_device(local)
+    from shadowfax_b200 import _lib as L
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    pr = build_problem(args.n)
+    mesh = pr.mesh
+    prec = L.PREC_FP64 if args.precision == "fp64" else L.PREC_SPLIT
+    ctx = Context(3, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec, device=local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    fp = FluxPass(ctx, mesh)
+    fp.set_primitive(pr.W0)
+    faces = mesh.n_active_faces
+    dt = pr.dt
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            fp.step(dt, 1, stats=False)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                fp.step(dt, 1, stats=False)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            dist.barrier()
+        st = fp.step(dt, 1)  # status check after the timed region
+        assert st.status == 0, st.status
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = faces * args.steps * world / (ms_max / 1e3)
+
+    # per-kernel device times (events around every launch) for the roofline
+    kms, launches = fp.step_timed(dt, args.steps)
+    names = ["gradients", "faces", "update"]
+    per_launch = kms / args.steps
+    top = int(np.argmax(per_launch))
+    alg = algorithmic_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz, args.precision)
+    peak, peak_kind = peaks()
+    achieved = alg[names[top]] / (per_launch[top] / 1e3) / 1e9
+    step_bytes = sum(alg.values())
+    roof = {"bound": "hbm", "kernel": f"k_{names[top]}", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "peak_source": f"hbm_gbs {peak_kind}",
+            "algorithmic_bytes_per_launch": alg[names[top]],
+            "kernel_ms": {n: float(v) for n, v in zip(names, per_launch)},
+            "step_achieved_gbs": step_bytes / (ms_max / args.steps / 1e3) / 1e9}
+
+    # end to end through the C ABI with host buffers: per step upload W and Q
+    # from host memory, one step, download W and Q
+    W0, Q0 = fp.state()
+    W = W0.copy()
+    Q = Q0.copy()
+    nbytes = W.nbytes + Q.nbytes
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fp.set_state(W, Q)
+        fp.step(dt, 1, stats=False)
+        W, Q = fp.state()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(e2.elapsed_time(e3), wall * 1e3)
+    e2e_val = faces * args.steps * world / (e2e_ms / 1e3)
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(pr)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32/f64",
+            "data": "synthetic",
+            "config": {"workload": f"sedov3d HLLC, {mesh.n_cells} generators (seed {SEED}), "
+                                   f"{faces} faces, reflective unit cube, CFL-0.4 dt",
+                       "solver": pr.solver, "precision": args.precision,
+                       "l2": "working set > L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "clocks": clk.summary(),
+            "roofline": roof,
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": 3 * args.steps,
+        }
+        print(json.dumps(line))
+    fp.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,234 @@
+/*
+ * sfxflux — B200-native finite-volume flux pass over a static Voronoi mesh.
+ *
+ * C ABI (extern "C", plain pointers and sizes, no exceptions).  Every entry
+ * point returns an int status (SFX_OK == 0).  It replaces, in Shadowfax's
+ * own C++ host code:
+ *
+ *   - the gradient loop   for i: VorTessManager::estimate_gradients(i, g);
+ *                                gas(i)->set_gradients(g)
+ *                         (src/Simulation.cpp:414-420,
+ *                          src/VorTessManager.cpp:290-296,
+ *                          src/VorCell.cpp:464-530)
+ *   - the face loop       VorTessManager::hydro -> VorFace::calculate_flux
+ *                         (src/VorTessManager.cpp:198-212,
+ *                          src/VorFace.cpp:670-1024)
+ *   - update_Q / get_W    (src/Simulation.cpp:473-483 and 791-836,
+ *                          src/utilities/GasParticle.cpp:617-624)
+ *
+ * keeping the RiemannSolver plugin selection (tag "EXAC" / "HLLC", gamma,
+ * tolerance, cutoff: src/riemann/RiemannSolverFactory.hpp) and the
+ * VorTess/VorFace face-list contract (src/VorTess.cpp:153-396).
+ *
+ * Array conventions on the host side: per-cell and per-face vectors are
+ * row-major [n][dim]; states are [n][S] with S = dim + 2 and the component
+ * order of StateVector (rho, vx, vy[, vz], p for primitive variables;
+ * m, px, py[, pz], e for conserved ones), src/StateVector.hpp:52-116.
+ */
+#ifndef SFXFLUX_H
+#define SFXFLUX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference's exceptions map onto these) ---- */
+#define SFX_OK 0
+#define SFX_ERR_INVALID 1     /* bad argument or mesh layout               */
+#define SFX_ERR_CUDA 2        /* CUDA runtime failure                      */
+#define SFX_ERR_RIEMANN 3     /* RiemannSolverException (RiemannSolver.hpp:202) */
+#define SFX_ERR_NAN_FLUX 4    /* FluxCalculationException (VorFace.cpp:1022)    */
+#define SFX_ERR_NEG_STATE 5   /* UpdateQException (GasParticle.cpp:619-621) and
+                                 ConservedVariablesException in get_Q          */
+#define SFX_ERR_NOCONV 6      /* exact solver hit its iteration cap       */
+#define SFX_ERR_BOUNDS 7      /* face/cell index outside the mesh          */
+#define SFX_ERR_UNSUPPORTED 8 /* solver tag other than EXAC/HLLC, etc.     */
+#define SFX_ERR_MESH 9        /* tessellation failed                       */
+#define SFX_ERR_NOMEM 10      /* device memory budget exceeded             */
+#define SFX_ERR_NOT_READY 11  /* server: result not available yet          */
+#define SFX_ERR_CLOSED 12     /* server: shut down                         */
+
+/* ---- solver kinds and precision modes ---- */
+#define SFX_SOLVER_EXACT 0 /* ExactRiemannSolver, tag "EXAC" */
+#define SFX_SOLVER_HLLC 1  /* HLLCRiemannSolver, tag "HLLC"  */
+
+#define SFX_PREC_FP64 0  /* plain FP64, bit-identical to the CPU oracle      */
+#define SFX_PREC_SPLIT 1 /* FP32 reconstruction/prediction/HLLC, FP64 p*
+                            iteration, FP64 accumulation of Q              */
+
+/* ---- face kinds (the right generator of a VorFace) ---- */
+#define SFX_FACE_REAL 0     /* right is a local cell                        */
+#define SFX_FACE_PERIODIC 1 /* right is a periodic image (id 1, has particle)*/
+#define SFX_FACE_MIRROR 2   /* right is a reflective mirror (no particle)    */
+
+/* ---- exact-solver branch codes (per face, debug output) ----
+ * bits 0-2   vacuum case: 0 none, 1 both sides vacuum, 2 right vacuum,
+ *            3 left vacuum, 4 vacuum generation
+ *            (ExactRiemannSolver.cpp:304-446)
+ * bits 3-4   pressure iteration: 1 Newton only (f(0) < cutoff),
+ *            2 Newton (converged), 3 Newton then Brent
+ *            (ExactRiemannSolver.cpp:142-176)
+ * bits 5-8   sampled region at x/t = 0 (see SFX_BRANCH_S_*)
+ * bits 9-15  Newton steps (saturating at 127)
+ * bits 16-22 Brent steps (saturating at 127)
+ * bit  23    Brent error exit (f(a) f(b) >= 0, ExactRiemannSolver.cpp:480-486)
+ * bit  24    set for HLLC faces; bits 5-8 then hold SFX_BRANCH_HLLC_*
+ * bit  25/26 over-flux limiter applied on the left / right side
+ *            (VorFace.cpp:837-866)
+ * bit  27    face skipped (zero area)                                       */
+#define SFX_BRANCH_VAC_MASK 0x7
+#define SFX_BRANCH_S_SHIFT 5
+#define SFX_BRANCH_S_MASK (0xf << 5)
+#define SFX_BRANCH_S_RSHOCK_STAR (1 << 5)
+#define SFX_BRANCH_S_RUP_SHOCK (2 << 5)
+#define SFX_BRANCH_S_RFAN (3 << 5)
+#define SFX_BRANCH_S_RRARE_STAR (4 << 5)
+#define SFX_BRANCH_S_RUP (5 << 5)
+#define SFX_BRANCH_S_LSHOCK_STAR (6 << 5)
+#define SFX_BRANCH_S_LUP_SHOCK (7 << 5)
+#define SFX_BRANCH_S_LFAN (8 << 5)
+#define SFX_BRANCH_S_LRARE_STAR (9 << 5)
+#define SFX_BRANCH_S_LUP (10 << 5)
+#define SFX_BRANCH_S_VAC (11 << 5)
+#define SFX_BRANCH_HLLC (1 << 24)
+#define SFX_BRANCH_HLLC_L (1 << 5)
+#define SFX_BRANCH_HLLC_LSTAR (2 << 5)
+#define SFX_BRANCH_HLLC_R (3 << 5)
+#define SFX_BRANCH_HLLC_RSTAR (4 << 5)
+#define SFX_BRANCH_LIMIT_L (1 << 25)
+#define SFX_BRANCH_LIMIT_R (1 << 26)
+#define SFX_BRANCH_SKIPPED (1 << 27)
+
+/* ---- configuration: what the RiemannSolver factory carries ---- */
+typedef struct sfx_config {
+    int32_t dim;       /* 2 or 3                                        */
+    int32_t solver;    /* SFX_SOLVER_EXACT or SFX_SOLVER_HLLC           */
+    double gamma;      /* adiabatic index (factory default 5/3)          */
+    double tolerance;  /* exact solver p* tolerance (default 1e-8)       */
+    double cutoff;     /* Newton-only threshold on f(0) (default -5)     */
+    int32_t precision; /* SFX_PREC_FP64 or SFX_PREC_SPLIT                */
+    int32_t device;    /* CUDA device ordinal                            */
+} sfx_config;
+
+/* ---- the face list exported once per tessellation (host arrays) ----
+ * Faces follow the VorTess order (each face owned by the first cell that
+ * meets it).  For face f: face_left[f] is the owner cell; face_right[f] is
+ * the neighbour cell (or, for a periodic image, the cell it is an image of;
+ * -1 for a reflective mirror); face_right_pos is the right generator's
+ * position (image/mirror position), used for the normal and the gradient
+ * geometry.  The per-cell face list (CSR) is the VorCell::_faces order;
+ * it lists every face whose left is the cell or whose right is the cell
+ * with kind SFX_FACE_REAL.  face_velocity may be NULL for a static mesh.  */
+typedef struct sfx_mesh_desc {
+    int32_t dim;
+    int32_t n_cells;
+    int32_t n_faces;
+    const double* cell_pos;         /* [n_cells][dim] generator positions  */
+    const double* cell_centroid;    /* [n_cells][dim]                      */
+    const double* cell_volume;      /* [n_cells]                           */
+    const double* cell_total_area;  /* [n_cells]                           */
+    const int32_t* cell_face_offset; /* [n_cells + 1]                      */
+    const int32_t* cell_face_index;  /* [cell_face_offset[n_cells]]        */
+    const double* face_area;        /* [n_faces]                           */
+    const double* face_midpoint;    /* [n_faces][dim]                      */
+    const int32_t* face_left;       /* [n_faces]                           */
+    const int32_t* face_right;      /* [n_faces]                           */
+    const int32_t* face_kind;       /* [n_faces] SFX_FACE_*                */
+    const double* face_right_pos;   /* [n_faces][dim]                      */
+    const double* face_velocity;    /* [n_faces][dim] or NULL (static)     */
+} sfx_mesh_desc;
+
+/* ---- per-call statistics ---- */
+typedef struct sfx_stats {
+    int32_t status;      /* first error of the call, SFX_OK otherwise    */
+    int32_t bad_face;    /* face index of a face error, else -1          */
+    int32_t bad_cell;    /* cell index of a cell error, else -1          */
+    int32_t steps_done;  /* completed steps                              */
+    double totals[5];    /* sum over cells of Q (m, p[dim], e) after the
+                            call, deterministic FP64 reduction           */
+} sfx_stats;
+
+typedef struct sfx_ctx sfx_ctx;
+typedef struct sfx_mesh sfx_mesh;
+
+/* ---- context: one per device and solver configuration ----
+ * Replaces RiemannSolverFactory::generate (RiemannSolverFactory.hpp:60-81);
+ * any other solver kind returns SFX_ERR_UNSUPPORTED. */
+int sfx_ctx_create(const sfx_config* cfg, sfx_ctx** out);
+int sfx_ctx_destroy(sfx_ctx* ctx);
+/* run all work of this context on a caller stream (cudaStream_t); NULL =
+ * the context's own stream */
+int sfx_ctx_set_stream(sfx_ctx* ctx, void* cuda_stream);
+/* block until the context's stream is idle */
+int sfx_ctx_synchronize(sfx_ctx* ctx);
+
+/* ---- mesh: upload the face list once per tessellation ----
+ * (VorTess::construct output, src/VorTess.cpp:153-396).  The caller keeps
+ * ownership of the host arrays and may free them after return. */
+int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out);
+int sfx_mesh_free(sfx_mesh* mesh);
+/* bytes of device memory a mesh of this size needs (admission control) */
+int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
+                              int64_t n_cell_faces, int32_t precision);
+
+/* ---- states ----
+ * sfx_state_upload_W: primitive variables [n_cells][S]; conserved ones are
+ * derived as in Simulation::initialize (Q = solver->get_Q(V, W),
+ * src/Simulation.cpp:1231-1251).  sfx_state_upload_WQ sets both.       */
+int sfx_state_upload_W(sfx_mesh* mesh, const double* W);
+int sfx_state_upload_WQ(sfx_mesh* mesh, const double* W, const double* Q);
+int sfx_state_download(sfx_mesh* mesh, double* W, double* Q);
+
+/* ---- the pass ----
+ * sfx_step: nsteps of gradients -> face fluxes -> update_Q -> get_W with a
+ * global time step dt (every cell active).  Stops at the first error and
+ * reports it in stats (may be NULL).  Asynchronous unless stats != NULL. */
+int sfx_step(sfx_mesh* mesh, double dt, int32_t nsteps, sfx_stats* stats);
+
+/* sfx_step with CUDA events around every launch: kernel_ms[0..2] receive
+ * the summed device time (ms) of the gradient, face and update kernels over
+ * the nsteps, *launches the number of kernels launched.  For profiling. */
+int sfx_step_timed(sfx_mesh* mesh, double dt, int32_t nsteps, float* kernel_ms,
+                   int32_t* launches);
+
+/* one pass for parity checks: gradients and per-face limited dQ (the amount
+ * the left cell receives; a real right cell receives its negation) without
+ * updating the state.  Outputs are host arrays, each may be NULL:
+ * grad [n_cells][dim][S], dQ_face [n_faces][S], branch [n_faces]. */
+int sfx_flux_pass(sfx_mesh* mesh, double dt, double* grad, double* dQ_face,
+                  int32_t* branch, sfx_stats* stats);
+
+/* Riemann solver on n independent state pairs (host arrays), interface at
+ * rest: RiemannSolver::solve (exact only) and solve_for_flux
+ * (ExactRiemannSolver.cpp:108-290, 858-880; HLLCRiemannSolver.cpp:258-403).
+ * half/flux/branch are [n][S], [n][S], [n]; half may be NULL. */
+int sfx_riemann_eval(sfx_ctx* ctx, int32_t n, const double* WL, const double* WR,
+                     const double* normal, int32_t reflective, double* half,
+                     double* flux, int32_t* branch);
+
+/* conserved totals sum_i Q_i (m, p[dim], e), deterministic FP64 */
+int sfx_mesh_totals(sfx_mesh* mesh, double* totals);
+
+/* ---- host Voronoi face-list builder (inputs for the pass) ---- */
+typedef struct sfx_voronoi sfx_voronoi;
+int sfx_voronoi_build(int dim, int64_t n, const double* pos, int periodic,
+                      int nthreads, sfx_voronoi** out);
+int sfx_voronoi_counts(const sfx_voronoi* v, int64_t* n_cells,
+                       int64_t* n_faces, int64_t* n_cell_faces);
+int sfx_voronoi_export(const sfx_voronoi* v, double* cell_centroid,
+                       double* cell_volume, double* cell_total_area,
+                       int32_t* cell_face_offset, int32_t* cell_face_index,
+                       double* face_area, double* face_midpoint,
+                       int32_t* face_left, int32_t* face_right,
+                       int32_t* face_kind, double* face_right_pos);
+void sfx_voronoi_free(sfx_voronoi* v);
+
+/* library version string */
+const char* sfx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

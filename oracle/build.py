@@ -1,0 +1,104 @@
+"""Build the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+* ``oracle/libsfxoracle.so`` - the C restatement of the flux pass
+  (sfx_oracle.c), compiled with gcc from this directory.
+* ``oracle/_ref/refharness_{2,3}d_{libm,sfxpow}`` - the reference Shadowfax
+  flux-pass sources compiled UNMODIFIED from the reference tree
+  (``$SFX_REFERENCE_SRC``, default /root/reference/src) together with
+  oracle/refharness (single-rank MPI stand-in, version header, TimeLine
+  constructor, driver).  Built only where the reference tree exists; the
+  binaries then travel with the repository.  "libm" keeps glibc's pow,
+  "sfxpow" routes pow() to sfx_pow (refharness/pow_interpose.c).
+
+Nothing here is linked into or called by the product library.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF_SRC = Path(os.environ.get("SFX_REFERENCE_SRC", "/root/reference/src"))
+OUT = HERE / "_ref"
+ORACLE_SO = HERE / "libsfxoracle.so"
+
+# reference translation units of the hot path and the support code they link
+REF_UNITS = [
+    "riemann/RiemannSolver.cpp", "riemann/ExactRiemannSolver.cpp",
+    "riemann/HLLCRiemannSolver.cpp", "VorFace.cpp", "VorCell.cpp", "VorGen.cpp",
+    "utilities/GasParticle.cpp", "utilities/Particle.cpp", "utilities/Timer.cpp",
+    "utilities/HelperFunctions.cpp", "utilities/Hilbert.cpp", "ColorMap.cpp", "MPIGlobal.cpp", "ProgramLog.cpp", "RestartFile.cpp",
+]
+# the reference's release flags plus: no FMA contraction (matches x86-64 default
+# code generation on every host), no builtin pow folding (so the sfxpow build
+# can interpose pow), <array> pre-included (src/RestartFile.hpp uses std::array)
+REF_FLAGS = ["-O2", "-ffp-contract=off", "-fno-builtin-pow", "-std=c++11",
+             "-include", "array", "-DSTATIC", "-w"]
+
+
+def _newer(out: Path, deps: list[Path]) -> bool:
+    return out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps)
+
+
+def build_oracle(force: bool = False) -> Path:
+    deps = [HERE / "sfx_oracle.c", HERE / "sfx_oracle.h", HERE / "sfx_oracle_dim.h",
+            HERE.parent / "shadowfax_b200" / "csrc" / "sfx_pow.h"]
+    if not force and _newer(ORACLE_SO, deps):
+        return ORACLE_SO
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fno-builtin", "-std=c99", "-shared",
+                    "-fPIC", str(HERE / "sfx_oracle.c"), "-o", str(ORACLE_SO), "-lm"],
+                   check=True)
+    return ORACLE_SO
+
+
+def ref_binary(dim: int, pow_kind: str) -> Path:
+    return OUT / f"refharness_{dim}d_{pow_kind}"
+
+
+def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
+    """Compile the reference harness binaries; returns [] if the reference
+    tree is absent (the prebuilt binaries are used instead)."""
+    if not (REF_SRC / "VorFace.cpp").exists():
+        return []
+    OUT.mkdir(exist_ok=True)
+    obj = OUT / "obj"
+    obj.mkdir(exist_ok=True)
+    inc = ["-I", str(HERE / "refharness" / "shim"), "-I", str(HERE / "refharness"),
+           "-I", str(REF_SRC), "-I", str(REF_SRC / "utilities")]
+    harness = HERE / "refharness" / "harness.cpp"
+    interpose = HERE / "refharness" / "pow_interpose.c"
+    outs = [ref_binary(d, k) for d in (2, 3) for k in ("libm", "sfxpow")]
+    deps = [harness, interpose, HERE / "refharness" / "shim" / "mpi.h", Path(__file__)]
+    if not force and all(_newer(o, deps) for o in outs):
+        return outs
+    tasks = []
+    for d in (2, 3):
+        for u in REF_UNITS:
+            o = obj / (u.replace("/", "_") + f".{d}d.o")
+            tasks.append(["g++", *REF_FLAGS, f"-Dndim_={d}", *inc, "-c", str(REF_SRC / u),
+                          "-o", str(o)])
+        tasks.append(["g++", *REF_FLAGS, f"-Dndim_={d}", *inc, "-c", str(harness), "-o",
+                      str(obj / f"harness.{d}d.o")])
+    tasks.append(["gcc", "-O2", "-ffp-contract=off", "-std=c99", "-c", str(interpose), "-o",
+                  str(obj / "pow_interpose.o")])
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), tasks):
+            if r.returncode:
+                raise RuntimeError(f"reference build failed: {' '.join(r.args)}\n{r.stderr}")
+    for d in (2, 3):
+        objs = [str(obj / (u.replace("/", "_") + f".{d}d.o")) for u in REF_UNITS]
+        objs.append(str(obj / f"harness.{d}d.o"))
+        for k in ("libm", "sfxpow"):
+            extra = [str(obj / "pow_interpose.o")] if k == "sfxpow" else []
+            subprocess.run(["g++", "-o", str(ref_binary(d, k)), *objs, *extra, "-lm"],
+                           check=True)
+    return outs
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    for p in build_reference(force="--force" in sys.argv):
+        print(p)

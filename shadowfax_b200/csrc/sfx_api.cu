@@ -1,0 +1,465 @@
+/*
+ * C-ABI front end of the sfxflux library: contexts, mesh upload (VorTess
+ * face-list contract -> device structure-of-arrays), state transfer, the
+ * step driver and the parity entry points.  See include/sfxflux.h.
+ */
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "sfx_internal.h"
+
+struct sfx_ctx {
+    sfx_config cfg;
+    sfx_solver_params sp;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+struct sfx_mesh {
+    sfx_ctx* ctx = nullptr;
+    sfx_dmesh d;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+int cuda_ok(cudaError_t e) {
+    return e == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+}
+
+#define SFX_TRY(x)                       \
+    do {                                 \
+        int _rc = (x);                   \
+        if(_rc != SFX_OK) return _rc;    \
+    } while(0)
+
+template <typename T>
+int dalloc(sfx_mesh* m, T** p, size_t count) {
+    *p = nullptr;
+    if(count == 0) count = 1;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if(e != cudaSuccess) {
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? SFX_ERR_NOMEM : SFX_ERR_CUDA;
+    }
+    m->allocs.push_back(q);
+    *p = (T*)q;
+    return SFX_OK;
+}
+
+template <typename T>
+int h2d(T* dst, const T* src, size_t count, cudaStream_t s) {
+    if(count == 0) return SFX_OK;
+    return cuda_ok(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+/* [n][w] row-major host -> [w][n] field-major host buffer */
+void transpose_in(const double* src, int64_t n, int w, std::vector<double>& out) {
+    out.resize((size_t)n * w);
+    for(int64_t i = 0; i < n; ++i)
+        for(int k = 0; k < w; ++k) out[(size_t)k * n + i] = src[(size_t)i * w + k];
+}
+
+void transpose_out(const std::vector<double>& src, int64_t n, int w, double* out) {
+    for(int64_t i = 0; i < n; ++i)
+        for(int k = 0; k < w; ++k) out[(size_t)i * w + k] = src[(size_t)k * n + i];
+}
+
+int check_err(sfx_mesh* m, sfx_stats* st) {
+    sfx_dev_error e;
+    cudaStream_t s = m->ctx->stream;
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(&e, m->d.err, sizeof e, cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+    int status = SFX_OK;
+    if(st) {
+        st->bad_face = -1;
+        st->bad_cell = -1;
+    }
+    if(e.face_key != ~0ull) {
+        status = (int)(e.face_key & 0xff);
+        if(st) st->bad_face = (int32_t)(e.face_key >> 8);
+    } else if(e.cell_key != ~0ull) {
+        status = (int)(e.cell_key & 0xff);
+        if(st) st->bad_cell = (int32_t)(e.cell_key >> 8);
+    }
+    if(st) st->status = status;
+    return status;
+}
+
+int reset_err(sfx_mesh* m) {
+    sfx_dev_error e;
+    e.face_key = ~0ull;
+    e.cell_key = ~0ull;
+    return cuda_ok(cudaMemcpyAsync(m->d.err, &e, sizeof e, cudaMemcpyHostToDevice,
+                                   m->ctx->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sfx_version(void) {
+    return "sfxflux 0.1 (sm_100a)";
+}
+
+int sfx_ctx_create(const sfx_config* cfg, sfx_ctx** out) {
+    if(!cfg || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    if(cfg->dim != 2 && cfg->dim != 3) return SFX_ERR_INVALID;
+    if(cfg->solver != SFX_SOLVER_EXACT && cfg->solver != SFX_SOLVER_HLLC)
+        return SFX_ERR_UNSUPPORTED;
+    if(cfg->precision != SFX_PREC_FP64 && cfg->precision != SFX_PREC_SPLIT)
+        return SFX_ERR_INVALID;
+    if(!(cfg->gamma > 1.)) return SFX_ERR_INVALID;
+    int ndev = 0;
+    if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SFX_ERR_CUDA;
+    }
+    if(cfg->device < 0 || cfg->device >= ndev) return SFX_ERR_INVALID;
+    SFX_TRY(cuda_ok(cudaSetDevice(cfg->device)));
+    sfx_ctx* c = new(std::nothrow) sfx_ctx;
+    if(!c) return SFX_ERR_NOMEM;
+    c->cfg = *cfg;
+    sfx_solver_params_init(&c->sp, cfg->solver, cfg->gamma, cfg->tolerance, cfg->cutoff);
+    if(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return SFX_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return SFX_OK;
+}
+
+int sfx_ctx_destroy(sfx_ctx* ctx) {
+    if(!ctx) return SFX_ERR_INVALID;
+    cudaSetDevice(ctx->cfg.device);
+    if(ctx->own_stream) {
+        cudaStreamSynchronize(ctx->own_stream);
+        cudaStreamDestroy(ctx->own_stream);
+    }
+    delete ctx;
+    return SFX_OK;
+}
+
+int sfx_ctx_set_stream(sfx_ctx* ctx, void* stream) {
+    if(!ctx) return SFX_ERR_INVALID;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return SFX_OK;
+}
+
+int sfx_ctx_synchronize(sfx_ctx* ctx) {
+    if(!ctx) return SFX_ERR_INVALID;
+    return cuda_ok(cudaStreamSynchronize(ctx->stream));
+}
+
+int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
+                              int64_t nnz, int32_t precision) {
+    (void)precision;
+    const int64_t S = dim + 2, n = n_cells, F = n_faces;
+    int64_t cells = n * (8 * (2 * dim + 2 + 2 * S + dim * S) + 4) + 4;
+    int64_t faces = F * (8 * (1 + 3 * dim + S) + 4 * 4);
+    return cells + faces + nnz * 4 + 8 * 8 * 1024 + 4096;
+}
+
+int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
+    if(!ctx || !desc || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    const int dim = desc->dim;
+    if(dim != ctx->cfg.dim) return SFX_ERR_INVALID;
+    const int64_t n = desc->n_cells, F = desc->n_faces;
+    if(n <= 0 || F < 0) return SFX_ERR_INVALID;
+    if(!desc->cell_pos || !desc->cell_centroid || !desc->cell_volume ||
+       !desc->cell_total_area || !desc->cell_face_offset || !desc->cell_face_index ||
+       (F && (!desc->face_area || !desc->face_midpoint || !desc->face_left ||
+              !desc->face_right || !desc->face_kind || !desc->face_right_pos)))
+        return SFX_ERR_INVALID;
+    /* validate every index the kernels will dereference */
+    const int32_t* off = desc->cell_face_offset;
+    if(off[0] != 0) return SFX_ERR_BOUNDS;
+    for(int64_t i = 0; i < n; ++i)
+        if(off[i + 1] < off[i]) return SFX_ERR_BOUNDS;
+    const int64_t nnz = off[n];
+    for(int64_t f = 0; f < F; ++f) {
+        int L = desc->face_left[f], R = desc->face_right[f], k = desc->face_kind[f];
+        if(L < 0 || L >= n) return SFX_ERR_BOUNDS;
+        if(k == SFX_FACE_REAL || k == SFX_FACE_PERIODIC) {
+            if(R < 0 || R >= n) return SFX_ERR_BOUNDS;
+        } else if(k != SFX_FACE_MIRROR) {
+            return SFX_ERR_BOUNDS;
+        }
+    }
+    std::vector<int32_t> idx(nnz);
+    for(int64_t i = 0; i < n; ++i) {
+        for(int64_t j = off[i]; j < off[i + 1]; ++j) {
+            int32_t f = desc->cell_face_index[j];
+            if(f < 0 || f >= F) return SFX_ERR_BOUNDS;
+            if(desc->face_left[f] == i) {
+                idx[j] = f;
+            } else if(desc->face_right[f] == i && desc->face_kind[f] == SFX_FACE_REAL) {
+                idx[j] = (int32_t)((uint32_t)f | 0x80000000u);
+            } else {
+                return SFX_ERR_BOUNDS;
+            }
+        }
+    }
+    SFX_TRY(cuda_ok(cudaSetDevice(ctx->cfg.device)));
+    sfx_mesh* m = new(std::nothrow) sfx_mesh;
+    if(!m) return SFX_ERR_NOMEM;
+    m->ctx = ctx;
+    sfx_dmesh& d = m->d;
+    std::memset(&d, 0, sizeof d);
+    d.dim = dim;
+    d.S = dim + 2;
+    d.n_cells = (int32_t)n;
+    d.n_faces = (int32_t)F;
+    d.nnz = nnz;
+    d.has_velocity = desc->face_velocity != nullptr;
+    const int S = d.S;
+    int rc = SFX_OK;
+    auto A = [&](auto** p, size_t c) {
+        if(rc == SFX_OK) rc = dalloc(m, p, c);
+    };
+    A(&d.pos, n * dim);
+    A(&d.cen, n * dim);
+    A(&d.vol, n);
+    A(&d.tarea, n);
+    A(&d.off, n + 1);
+    A(&d.idx, nnz);
+    A(&d.W, n * S);
+    A(&d.Q, n * S);
+    A(&d.grad, n * dim * S);
+    A(&d.area, F);
+    A(&d.mid, F * dim);
+    A(&d.left, F);
+    A(&d.right, F);
+    A(&d.kind, F);
+    A(&d.rpos, F * dim);
+    if(d.has_velocity) A(&d.vel, F * dim);
+    A(&d.dQf, F * S);
+    A(&d.branch, F);
+    A(&d.err, 1);
+    A(&d.totals_scratch, (size_t)(S + 1) * 1024);
+    if(rc != SFX_OK) {
+        sfx_mesh_free(m);
+        return rc;
+    }
+    cudaStream_t s = ctx->stream;
+    std::vector<double> t1, t2, t3, t4, t5;
+    transpose_in(desc->cell_pos, n, dim, t1);
+    transpose_in(desc->cell_centroid, n, dim, t2);
+    transpose_in(desc->face_midpoint, F, dim, t3);
+    transpose_in(desc->face_right_pos, F, dim, t4);
+    if(d.has_velocity) transpose_in(desc->face_velocity, F, dim, t5);
+    rc = h2d(d.pos, t1.data(), t1.size(), s);
+    if(!rc) rc = h2d(d.cen, t2.data(), t2.size(), s);
+    if(!rc) rc = h2d(d.vol, desc->cell_volume, n, s);
+    if(!rc) rc = h2d(d.tarea, desc->cell_total_area, n, s);
+    if(!rc) rc = h2d(d.off, off, n + 1, s);
+    if(!rc) rc = h2d(d.idx, idx.data(), nnz, s);
+    if(!rc) rc = h2d(d.area, desc->face_area, F, s);
+    if(!rc) rc = h2d(d.mid, t3.data(), t3.size(), s);
+    if(!rc) rc = h2d(d.left, desc->face_left, F, s);
+    if(!rc) rc = h2d(d.right, desc->face_right, F, s);
+    if(!rc) rc = h2d(d.kind, desc->face_kind, F, s);
+    if(!rc) rc = h2d(d.rpos, t4.data(), t4.size(), s);
+    if(!rc && d.has_velocity) rc = h2d(d.vel, t5.data(), t5.size(), s);
+    if(!rc) rc = cuda_ok(cudaMemsetAsync(d.W, 0, sizeof(double) * n * S, s));
+    if(!rc) rc = cuda_ok(cudaMemsetAsync(d.Q, 0, sizeof(double) * n * S, s));
+    if(!rc) rc = reset_err(m);
+    /* host staging buffers go out of scope: wait for the copies */
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    if(rc != SFX_OK) {
+        sfx_mesh_free(m);
+        return rc;
+    }
+    *out = m;
+    return SFX_OK;
+}
+
+int sfx_mesh_free(sfx_mesh* m) {
+    if(!m) return SFX_ERR_INVALID;
+    if(m->ctx) {
+        cudaSetDevice(m->ctx->cfg.device);
+        cudaStreamSynchronize(m->ctx->stream);
+    }
+    for(void* p : m->allocs) cudaFree(p);
+    delete m;
+    return SFX_OK;
+}
+
+int sfx_state_upload_W(sfx_mesh* m, const double* W) {
+    if(!m || !W) return SFX_ERR_INVALID;
+    const int64_t n = m->d.n_cells;
+    cudaStream_t s = m->ctx->stream;
+    std::vector<double> t;
+    transpose_in(W, n, m->d.S, t);
+    SFX_TRY(reset_err(m));
+    SFX_TRY(h2d(m->d.W, t.data(), t.size(), s));
+    SFX_TRY(sfx_fp64_init_Q(&m->d, &m->ctx->sp, s));
+    return check_err(m, nullptr);
+}
+
+int sfx_state_upload_WQ(sfx_mesh* m, const double* W, const double* Q) {
+    if(!m || !W || !Q) return SFX_ERR_INVALID;
+    const int64_t n = m->d.n_cells;
+    cudaStream_t s = m->ctx->stream;
+    std::vector<double> t1, t2;
+    transpose_in(W, n, m->d.S, t1);
+    transpose_in(Q, n, m->d.S, t2);
+    SFX_TRY(reset_err(m));
+    SFX_TRY(h2d(m->d.W, t1.data(), t1.size(), s));
+    SFX_TRY(h2d(m->d.Q, t2.data(), t2.size(), s));
+    return cuda_ok(cudaStreamSynchronize(s));
+}
+
+int sfx_state_download(sfx_mesh* m, double* W, double* Q) {
+    if(!m) return SFX_ERR_INVALID;
+    const int64_t n = m->d.n_cells;
+    const int S = m->d.S;
+    cudaStream_t s = m->ctx->stream;
+    std::vector<double> t1(W ? n * S : 0), t2(Q ? n * S : 0);
+    if(W)
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(t1.data(), m->d.W, sizeof(double) * n * S,
+                                        cudaMemcpyDeviceToHost, s)));
+    if(Q)
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(t2.data(), m->d.Q, sizeof(double) * n * S,
+                                        cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+    if(W) transpose_out(t1, n, S, W);
+    if(Q) transpose_out(t2, n, S, Q);
+    return SFX_OK;
+}
+
+int sfx_step(sfx_mesh* m, double dt, int32_t nsteps, sfx_stats* st) {
+    if(!m || nsteps < 0 || !(dt > 0.)) return SFX_ERR_INVALID;
+    sfx_ctx* c = m->ctx;
+    if(c->cfg.precision != SFX_PREC_FP64) return SFX_ERR_UNSUPPORTED;
+    cudaStream_t s = c->stream;
+    SFX_TRY(reset_err(m));
+    for(int t = 0; t < nsteps; ++t) {
+        SFX_TRY(sfx_fp64_gradients(&m->d, s));
+        SFX_TRY(sfx_fp64_faces(&m->d, &c->sp, dt, 0, s));
+        SFX_TRY(sfx_fp64_apply(&m->d, &c->sp, s));
+    }
+    if(!st) return SFX_OK;
+    std::memset(st, 0, sizeof *st);
+    int rc = check_err(m, st);
+    st->steps_done = rc == SFX_OK ? nsteps : -1;
+    int rt = sfx_fp64_totals(&m->d, st->totals, s);
+    return rc != SFX_OK ? rc : rt;
+}
+
+int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
+                   int32_t* launches) {
+    if(!m || nsteps < 0 || !(dt > 0.) || !kernel_ms) return SFX_ERR_INVALID;
+    sfx_ctx* c = m->ctx;
+    if(c->cfg.precision != SFX_PREC_FP64) return SFX_ERR_UNSUPPORTED;
+    cudaStream_t s = c->stream;
+    cudaEvent_t ev[4];
+    for(auto& e : ev)
+        if(cudaEventCreate(&e) != cudaSuccess) return SFX_ERR_CUDA;
+    double acc[3] = {0., 0., 0.};
+    int rc = reset_err(m);
+    int nl = 0;
+    for(int t = 0; t < nsteps && rc == SFX_OK; ++t) {
+        cudaEventRecord(ev[0], s);
+        rc = sfx_fp64_gradients(&m->d, s);
+        cudaEventRecord(ev[1], s);
+        if(!rc) rc = sfx_fp64_faces(&m->d, &c->sp, dt, 0, s);
+        cudaEventRecord(ev[2], s);
+        if(!rc) rc = sfx_fp64_apply(&m->d, &c->sp, s);
+        cudaEventRecord(ev[3], s);
+        nl += 3;
+        if(!rc) rc = cuda_ok(cudaEventSynchronize(ev[3]));
+        for(int k = 0; k < 3 && !rc; ++k) {
+            float ms = 0.f;
+            rc = cuda_ok(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[k] += ms;
+        }
+    }
+    for(auto& e : ev) cudaEventDestroy(e);
+    for(int k = 0; k < 3; ++k) kernel_ms[k] = (float)acc[k];
+    if(launches) *launches = nl;
+    if(rc) return rc;
+    return check_err(m, nullptr);
+}
+
+int sfx_flux_pass(sfx_mesh* m, double dt, double* grad, double* dQ_face,
+                  int32_t* branch, sfx_stats* st) {
+    if(!m || !(dt > 0.)) return SFX_ERR_INVALID;
+    sfx_ctx* c = m->ctx;
+    cudaStream_t s = c->stream;
+    const int64_t n = m->d.n_cells, F = m->d.n_faces;
+    const int S = m->d.S, D = m->d.dim;
+    SFX_TRY(reset_err(m));
+    SFX_TRY(sfx_fp64_gradients(&m->d, s));
+    SFX_TRY(sfx_fp64_faces(&m->d, &c->sp, dt, 1, s));
+    std::vector<double> tg(grad ? n * D * S : 0), tq(dQ_face ? F * S : 0);
+    if(grad)
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(tg.data(), m->d.grad, sizeof(double) * tg.size(),
+                                        cudaMemcpyDeviceToHost, s)));
+    if(dQ_face)
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(tq.data(), m->d.dQf, sizeof(double) * tq.size(),
+                                        cudaMemcpyDeviceToHost, s)));
+    if(branch && F)
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(branch, m->d.branch, sizeof(int32_t) * F,
+                                        cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+    if(grad) transpose_out(tg, n, D * S, grad);
+    if(dQ_face) transpose_out(tq, F, S, dQ_face);
+    sfx_stats local;
+    return check_err(m, st ? st : &local);
+}
+
+int sfx_riemann_eval(sfx_ctx* c, int32_t n, const double* WL, const double* WR,
+                     const double* normal, int32_t reflective, double* half,
+                     double* flux, int32_t* branch) {
+    if(!c || n < 0 || (n && (!WL || !WR || !normal || !flux || !branch)))
+        return SFX_ERR_INVALID;
+    if(n == 0) return SFX_OK;
+    const int D = c->cfg.dim, S = D + 2;
+    cudaStream_t s = c->stream;
+    double *dWL = nullptr, *dWR = nullptr, *dn = nullptr, *dh = nullptr, *df = nullptr;
+    int32_t* dc = nullptr;
+    int rc = SFX_OK;
+    auto al = [&](auto** p, size_t bytes) {
+        if(rc == SFX_OK && cudaMalloc((void**)p, bytes) != cudaSuccess) rc = SFX_ERR_CUDA;
+    };
+    al(&dWL, sizeof(double) * n * S);
+    al(&dWR, sizeof(double) * n * S);
+    al(&dn, sizeof(double) * n * D);
+    al(&dh, sizeof(double) * n * S);
+    al(&df, sizeof(double) * n * S);
+    al(&dc, sizeof(int32_t) * n);
+    if(!rc) rc = h2d(dWL, WL, (size_t)n * S, s);
+    if(!rc) rc = h2d(dWR, WR, (size_t)n * S, s);
+    if(!rc) rc = h2d(dn, normal, (size_t)n * D, s);
+    if(!rc) rc = sfx_fp64_riemann(D, &c->sp, n, dWL, dWR, dn, reflective, dh, df, dc, s);
+    if(!rc && half)
+        rc = cuda_ok(cudaMemcpyAsync(half, dh, sizeof(double) * n * S, cudaMemcpyDeviceToHost, s));
+    if(!rc)
+        rc = cuda_ok(cudaMemcpyAsync(flux, df, sizeof(double) * n * S, cudaMemcpyDeviceToHost, s));
+    if(!rc)
+        rc = cuda_ok(cudaMemcpyAsync(branch, dc, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    cudaFree(dWL);
+    cudaFree(dWR);
+    cudaFree(dn);
+    cudaFree(dh);
+    cudaFree(df);
+    cudaFree(dc);
+    return rc;
+}
+
+int sfx_mesh_totals(sfx_mesh* m, double* totals) {
+    if(!m || !totals) return SFX_ERR_INVALID;
+    return sfx_fp64_totals(&m->d, totals, m->ctx->stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+/*
+ * Internal declarations of the sfxflux library (not part of the C ABI).
+ */
+#ifndef SFX_INTERNAL_H
+#define SFX_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/sfxflux.h"
+
+/* hard cap on Newton and Brent iterations of the exact solver (the reference
+ * has none; a face that reaches it reports SFX_ERR_NOCONV) */
+#define SFX_MAX_ITER 1000
+
+/* device error record.  Each key packs (index << 8) | status, and the
+ * kernels take the minimum, so the record names the lowest failing face or
+ * cell -- the one at which the reference's loops would have thrown. */
+struct sfx_dev_error {
+    unsigned long long face_key; /* ~0ull when no face failed */
+    unsigned long long cell_key; /* ~0ull when no cell failed */
+};
+
+/* device-resident mesh in structure-of-arrays layout.  Field-major arrays:
+ * W[k * n_cells + i] etc.  All pointers are device pointers. */
+struct sfx_dmesh {
+    int32_t dim, S;
+    int32_t n_cells, n_faces;
+    int64_t nnz;
+    int32_t has_velocity;
+    /* cells */
+    double* pos;    /* [dim][n]  */
+    double* cen;    /* [dim][n]  */
+    double* vol;    /* [n]       */
+    double* tarea;  /* [n]       */
+    int32_t* off;   /* [n+1]     */
+    int32_t* idx;   /* [nnz] face id | (1u << 31 if the cell is the right) */
+    double* W;      /* [S][n]    */
+    double* Q;      /* [S][n]    */
+    double* grad;   /* [dim*S][n]: grad[(l*S + k)*n + i] = dW_k/dx_l       */
+    /* faces */
+    double* area;   /* [F]       */
+    double* mid;    /* [dim][F]  */
+    int32_t* left;  /* [F]       */
+    int32_t* right; /* [F]       */
+    int32_t* kind;  /* [F]       */
+    double* rpos;   /* [dim][F]  */
+    double* vel;    /* [dim][F] or NULL */
+    double* dQf;    /* [S][F] scratch: limited dQ received by the left cell */
+    int32_t* branch; /* [F] scratch or NULL */
+    sfx_dev_error* err;
+    double* totals_scratch; /* [S * 1024] */
+};
+
+struct sfx_solver_params {
+    int32_t kind;
+    double gamma, tol, cutoff;
+    double gp1d2g, gm1d2g, gm1dgp1, tdgp1, tdgm1, gm1d2, tgdgm1, ginv;
+};
+
+void sfx_solver_params_init(sfx_solver_params* p, int kind, double gamma,
+                            double tol, double cutoff);
+
+/* FP64 kernels (sfx_fp64.cu) */
+int sfx_fp64_gradients(const sfx_dmesh* m, void* stream);
+int sfx_fp64_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
+                   int write_branch, void* stream);
+int sfx_fp64_apply(const sfx_dmesh* m, const sfx_solver_params* sp,
+                   void* stream);
+int sfx_fp64_init_Q(const sfx_dmesh* m, const sfx_solver_params* sp,
+                    void* stream);
+int sfx_fp64_totals(const sfx_dmesh* m, double* host_out, void* stream);
+int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n,
+                     const double* dWL, const double* dWR, const double* dn,
+                     int reflective, double* dhalf, double* dflux,
+                     int32_t* dcode, void* stream);
+
+#endif

@@ -1,0 +1,210 @@
+"""Host-side mirror of Shadowfax's flux-pass interface over the C ABI.
+
+* :class:`RiemannSolver` and :class:`RiemannSolverFactory` mirror the
+  reference plugin selection (src/riemann/RiemannSolver.hpp:37-155,
+  src/riemann/RiemannSolverFactory.hpp): ``tag()`` "EXAC"/"HLLC",
+  ``get_gamma()``, tolerance and cutoff.  Unsupported solver names raise, as
+  the factory's ``my_exit()`` does.
+* :class:`FluxPass` is the device-side replacement of the gradient loop +
+  ``VorTessManager::hydro`` + ``update_Q``/``get_W`` (src/Simulation.cpp:
+  414-483, 791-836) for one uploaded mesh.
+
+Errors map onto :class:`shadowfax_b200._lib.SfxError`, whose ``status`` is one
+of the SFX_ERR_* codes (RiemannSolverException -> SFX_ERR_RIEMANN,
+FluxCalculationException -> SFX_ERR_NAN_FLUX, UpdateQException ->
+SFX_ERR_NEG_STATE).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .mesh import Mesh
+
+DEFAULT_GAMMA = 5.0 / 3.0      # RIEMANNSOLVERFACTORY_DEFAULT_GAMMA
+DEFAULT_TOLERANCE = 1e-8       # RIEMANNSOLVERFACTORY_DEFAULT_TOLERANCE
+DEFAULT_CUTOFF = -5.0          # RIEMANNSOLVERFACTORY_DEFAULT_CUTOFF
+
+
+class RiemannSolver:
+    """Selection of the Riemann solver for the flux pass."""
+
+    kind: int = -1
+    _tag: str = ""
+
+    def __init__(self, gamma: float = DEFAULT_GAMMA, tolerance: float = DEFAULT_TOLERANCE,
+                 cutoff: float = DEFAULT_CUTOFF):
+        self.gamma = float(gamma)
+        self.tolerance = float(tolerance)
+        self.cutoff = float(cutoff)
+
+    def tag(self) -> str:
+        return self._tag
+
+    def get_gamma(self) -> float:
+        return self.gamma
+
+    def __repr__(self):
+        return f"{type(self).__name__}(gamma={self.gamma!r})"
+
+
+class ExactRiemannSolver(RiemannSolver):
+    """src/riemann/ExactRiemannSolver.cpp"""
+    kind = L.SOLVER_EXACT
+    _tag = "EXAC"
+
+
+class HLLCRiemannSolver(RiemannSolver):
+    """src/riemann/HLLCRiemannSolver.cpp"""
+    kind = L.SOLVER_HLLC
+    _tag = "HLLC"
+
+
+class RiemannSolverFactory:
+    """Name / tag -> solver (src/riemann/RiemannSolverFactory.hpp)."""
+
+    @staticmethod
+    def generate(name: str, gamma: float = DEFAULT_GAMMA, tolerance: float = DEFAULT_TOLERANCE,
+                 cutoff: float = DEFAULT_CUTOFF) -> RiemannSolver:
+        if name == "Exact":
+            return ExactRiemannSolver(gamma, tolerance, cutoff)
+        if name == "HLLC":
+            return HLLCRiemannSolver(gamma)
+        if name in ("TRRS", "NoPressure", "Advection"):
+            raise L.SfxError(L.SFX_ERR_UNSUPPORTED, f"Riemann solver {name!r}")
+        raise ValueError(f"Unknown Riemann solver type: {name}!")
+
+    @staticmethod
+    def from_tag(tag: str, gamma: float = DEFAULT_GAMMA, tolerance: float = DEFAULT_TOLERANCE,
+                 cutoff: float = DEFAULT_CUTOFF) -> RiemannSolver:
+        if tag == "EXAC":
+            return ExactRiemannSolver(gamma, tolerance, cutoff)
+        if tag == "HLLC":
+            return HLLCRiemannSolver(gamma)
+        raise L.SfxError(L.SFX_ERR_UNSUPPORTED, f"Riemann solver tag {tag!r}")
+
+
+class Context:
+    """One device + solver configuration (sfx_ctx)."""
+
+    def __init__(self, dim: int, solver: RiemannSolver, precision: int = L.PREC_FP64,
+                 device: int = 0):
+        self.dim = dim
+        self.solver = solver
+        self.precision = precision
+        cfg = L.sfx_config(dim, solver.kind, solver.gamma, solver.tolerance, solver.cutoff,
+                           precision, device)
+        h = C.c_void_p()
+        L.check(L.lib().sfx_ctx_create(C.byref(cfg), C.byref(h)), "sfx_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            L.lib().sfx_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        L.check(L.lib().sfx_ctx_set_stream(self.h, C.c_void_p(stream_handle or 0)))
+
+    def synchronize(self):
+        L.check(L.lib().sfx_ctx_synchronize(self.h))
+
+    def riemann(self, WL, WR, normal, reflective: bool = False):
+        """RiemannSolver::solve (exact) and solve_for_flux on the GPU for n
+        state pairs with the interface at rest; returns (half, flux, branch)."""
+        WL = np.ascontiguousarray(WL, np.float64)
+        WR = np.ascontiguousarray(WR, np.float64)
+        normal = np.ascontiguousarray(normal, np.float64)
+        n = WL.shape[0]
+        half = np.zeros_like(WL)
+        flux = np.zeros_like(WL)
+        code = np.zeros(n, np.int32)
+        L.check(L.lib().sfx_riemann_eval(self.h, n, L.dptr(WL), L.dptr(WR), L.dptr(normal),
+                                         int(reflective), L.dptr(half), L.dptr(flux),
+                                         L.iptr(code)), "sfx_riemann_eval")
+        return half, flux, code
+
+
+class FluxPass:
+    """A mesh resident on the device with its hydro state."""
+
+    def __init__(self, ctx: Context, mesh: Mesh):
+        if mesh.dim != ctx.dim:
+            raise ValueError("mesh dimension does not match the context")
+        self.ctx = ctx
+        self.mesh = mesh
+        h = C.c_void_p()
+        d = mesh.desc()
+        L.check(L.lib().sfx_mesh_upload(ctx.h, C.byref(d), C.byref(h)), "sfx_mesh_upload")
+        self.h = h
+        self.S = mesh.dim + 2
+
+    def close(self):
+        if self.h:
+            L.lib().sfx_mesh_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_primitive(self, W: np.ndarray):
+        """W per cell; Q = get_Q(V, W) on the device (Simulation::initialize)."""
+        W = np.ascontiguousarray(W, np.float64)
+        assert W.shape == (self.mesh.n_cells, self.S)
+        L.check(L.lib().sfx_state_upload_W(self.h, L.dptr(W)), "sfx_state_upload_W")
+
+    def set_state(self, W: np.ndarray, Q: np.ndarray):
+        W = np.ascontiguousarray(W, np.float64)
+        Q = np.ascontiguousarray(Q, np.float64)
+        L.check(L.lib().sfx_state_upload_WQ(self.h, L.dptr(W), L.dptr(Q)), "sfx_state_upload_WQ")
+
+    def state(self) -> tuple[np.ndarray, np.ndarray]:
+        W = np.empty((self.mesh.n_cells, self.S))
+        Q = np.empty((self.mesh.n_cells, self.S))
+        L.check(L.lib().sfx_state_download(self.h, L.dptr(W), L.dptr(Q)), "sfx_state_download")
+        return W, Q
+
+    def step(self, dt: float, nsteps: int = 1, stats: bool = True) -> L.sfx_stats | None:
+        st = L.sfx_stats() if stats else None
+        rc = L.lib().sfx_step(self.h, dt, nsteps, C.byref(st) if stats else None)
+        if rc:
+            idx = None
+            if st is not None:
+                idx = st.bad_face if st.bad_face >= 0 else st.bad_cell
+            raise L.SfxError(rc, "sfx_step", idx)
+        return st
+
+    def step_timed(self, dt: float, nsteps: int) -> tuple[np.ndarray, int]:
+        """nsteps with per-kernel device times: (ms[gradients, faces, update],
+        launches)"""
+        ms = (C.c_float * 3)()
+        nl = C.c_int32(0)
+        L.check(L.lib().sfx_step_timed(self.h, dt, nsteps, ms, C.byref(nl)), "sfx_step_timed")
+        return np.array(list(ms), dtype=np.float64), nl.value
+
+    def flux_pass(self, dt: float):
+        """gradients [n, dim, S], per-face dQ of the left cell [F, S], branch
+        codes [F] of one pass without updating the state."""
+        n, F, D, S = self.mesh.n_cells, self.mesh.n_faces, self.mesh.dim, self.S
+        grad = np.empty((n, D, S))
+        dQ = np.empty((F, S))
+        br = np.empty(F, np.int32)
+        st = L.sfx_stats()
+        rc = L.lib().sfx_flux_pass(self.h, dt, L.dptr(grad), L.dptr(dQ), L.iptr(br), C.byref(st))
+        return grad, dQ, br, rc, (st.bad_face if st.bad_face >= 0 else st.bad_cell)
+
+    def totals(self) -> np.ndarray:
+        out = np.zeros(5)
+        L.check(L.lib().sfx_mesh_totals(self.h, L.dptr(out)), "sfx_mesh_totals")
+        return out[: self.S]

@@ -1,0 +1,108 @@
+"""Synthetic workloads: the five configurations the flux pass is measured on.
+
+Inputs are seeded synthetic stand-ins (numpy PCG64 streams): generators
+uniform in the unit square/cube, tessellated by the host face-list builder,
+with the initial states of each configuration.  Nothing here reads files.
+
+  c1  2D Sod tube, reflective unit square, exact solver, dt = 1e-4, 100 steps
+  c2  3D Sedov-type blast, reflective unit cube, HLLC, global CFL 0.4, 50 steps
+  c3  3D supersonic random field, periodic unit cube, exact solver, one pass
+  c4  1,024 independent 2D step-state meshes, HLLC, 20 steps at own CFL dt
+  c5  Poisson request stream of static meshes (serving)
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mesh import Mesh, build_voronoi, random_generators
+
+GAMMA = 5.0 / 3.0
+
+
+@dataclass
+class Problem:
+    name: str
+    mesh: Mesh
+    W0: np.ndarray      # [n, S] primitive variables
+    solver: str          # "Exact" or "HLLC"
+    dt: float
+    nsteps: int
+    gamma: float = GAMMA
+
+
+def cell_h(mesh: Mesh) -> np.ndarray:
+    """VorCell::get_h (src/VorCell.cpp:948-956)"""
+    V = mesh.cell_volume
+    if mesh.dim == 3:
+        return np.cbrt(V * 3.0 / 4.0 / math.pi)
+    return np.sqrt(V / math.pi)
+
+
+def cfl_dt(mesh: Mesh, W: np.ndarray, gamma: float = GAMMA, cfl: float = 0.4) -> float:
+    """Global CFL time step 0.4 min h / (|v| + c) (the per-cell criterion of
+    src/TimeLine.cpp:254-274, taken as one global value without power-of-two
+    binning)."""
+    D = mesh.dim
+    rho, p = W[:, 0], W[:, D + 1]
+    c = np.sqrt(gamma * p / np.where(rho > 0, rho, 1.0)) * (rho > 0)
+    v = np.sqrt((W[:, 1:D + 1] ** 2).sum(1))
+    return float(cfl * np.min(cell_h(mesh) / (v + c)))
+
+
+def sod2d(n: int = 10_000, seed: int = 1, nsteps: int = 100, dt: float = 1e-4,
+          solver: str = "Exact") -> Problem:
+    pos = random_generators(n, 2, seed)
+    mesh = build_voronoi(pos, periodic=False)
+    W = np.zeros((n, 4))
+    left = pos[:, 0] < 0.5
+    W[:, 0] = np.where(left, 1.0, 0.125)
+    W[:, 3] = np.where(left, 1.0, 0.1)
+    return Problem("sod2d", mesh, W, solver, dt, nsteps)
+
+
+def sedov3d(n: int = 262_144, seed: int = 2, nsteps: int = 50, solver: str = "HLLC",
+            n_hot: int = 32, energy: float = 1.0) -> Problem:
+    pos = random_generators(n, 3, seed)
+    mesh = build_voronoi(pos, periodic=False)
+    W = np.zeros((n, 5))
+    W[:, 0] = 1.0
+    W[:, 4] = 1e-6
+    d2 = ((pos - 0.5) ** 2).sum(1)
+    hot = np.argsort(d2, kind="stable")[:n_hot]
+    W[hot, 4] = (GAMMA - 1.0) * (energy / n_hot) / mesh.cell_volume[hot]
+    return Problem("sedov3d", mesh, W, solver, cfl_dt(mesh, W), nsteps)
+
+
+def random_field3d(n: int = 2_097_152, seed: int = 3, solver: str = "Exact",
+                   nsteps: int = 1) -> Problem:
+    pos = random_generators(n, 3, seed)
+    mesh = build_voronoi(pos, periodic=True)
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    W = np.zeros((n, 5))
+    W[:, 0] = np.exp(rng.normal(-0.5, 1.0, n))
+    W[:, 1:4] = rng.normal(0.0, 1.0, (n, 3))
+    W[:, 4] = 1.0
+    return Problem("random3d", mesh, W, solver, cfl_dt(mesh, W), nsteps)
+
+
+def step_state2d(n: int, seed: int, solver: str = "HLLC", nsteps: int = 20) -> Problem:
+    """one c4 mesh: left/right constant states split by a line through the
+    centre with a random normal angle"""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pos = random_generators(n, 2, int(rng.integers(1 << 62)))
+    mesh = build_voronoi(pos, periodic=False)
+    rhoL, pL, rhoR, pR = rng.uniform(0.1, 1.0, 4)
+    th = rng.uniform(0.0, 2 * math.pi)
+    side = (pos - 0.5) @ np.array([math.cos(th), math.sin(th)]) < 0
+    W = np.zeros((n, 4))
+    W[:, 0] = np.where(side, rhoL, rhoR)
+    W[:, 3] = np.where(side, pL, rhoR * 0 + pR)
+    return Problem(f"step2d_{n}", mesh, W, solver, cfl_dt(mesh, W), nsteps)
+
+
+def batch_sizes(count: int = 1024, lo: int = 1_000, hi: int = 100_000, seed: int = 4) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.exp(rng.uniform(math.log(lo), math.log(hi), count)).astype(np.int64)

@@ -1,0 +1,66 @@
+"""The CPU oracle against the reference's own results (golden fixtures made
+by running the unmodified reference flux pass, tests/golden/make_golden.py)
+and against the reference's Riemann-solver unit-test vectors."""
+import numpy as np
+import pytest
+
+from golden_util import MESH_CASES, TORO_HALF_STATES, assert_values_equal, load_case, \
+    load_riemann, toro_pairs
+from oracle.oracle import Params
+
+
+@pytest.mark.parametrize("name", MESH_CASES)
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_matches_reference_bitwise(oracle, name, powk):
+    mesh, meta, ref = load_case(name)
+    p = Params(solver=meta["solver"], gamma=meta["gamma"], use_libm_pow=(powk == "libm"))
+    out = oracle.run(mesh, p, meta["dt"], meta["nsteps"], meta["W0"])
+    assert out["status"] == 0 and out["steps"] == meta["nsteps"]
+    for key in ("W", "Q", "grad", "dQ"):
+        np.testing.assert_array_equal(out[key], ref[f"ref_{powk}_{key}"], err_msg=key)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("solver", ["Exact", "HLLC"])
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_riemann_matches_reference(oracle, dim, solver, powk):
+    z = load_riemann(dim)
+    p = Params(solver=solver, use_libm_pow=(powk == "libm"))
+    half, flux, code = oracle.riemann(dim, p, z["WL"], z["WR"], z["normal"])
+    assert np.all(code >= 0)
+    np.testing.assert_array_equal(flux, z[f"{solver}_{powk}_flux"])
+    if solver == "Exact":
+        np.testing.assert_array_equal(half, z[f"{solver}_{powk}_half"])
+    half, flux, code = oracle.riemann(dim, Params(solver=solver), z["WL"], z["WR"], z["normal"],
+                                      reflective=True)
+    np.testing.assert_array_equal(flux, z[f"{solver}_reflective_flux"])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_toro_half_states(oracle, dim):
+    WL, WR, nrm, exp = toro_pairs(dim)
+    half, flux, code = oracle.riemann(dim, Params(solver="Exact", gamma=1.66667), WL, WR, nrm)
+    assert np.all(code >= 0)
+    for i in range(len(TORO_HALF_STATES)):
+        assert_values_equal(half[i, 0], exp[i, 0])
+        assert_values_equal(half[i, 1], exp[i, 1])
+        assert_values_equal(half[i, dim + 1], exp[i, 2])
+
+
+def test_branch_coverage_of_riemann_fixture(oracle):
+    """the fixture exercises vacuum, Newton-only, Newton, Brent and every
+    sampled region"""
+    seen = set()
+    for dim in (2, 3):
+        z = load_riemann(dim)
+        _, _, code = oracle.riemann(dim, Params(solver="Exact"), z["WL"], z["WR"], z["normal"])
+        for c in code:
+            seen.add(("vac", int(c) & 7))
+            seen.add(("it", (int(c) >> 3) & 3))
+            seen.add(("s", (int(c) >> 5) & 15))
+    for v in range(1, 5):
+        assert ("vac", v) in seen
+    for it in (1, 2, 3):
+        assert ("it", it) in seen
+    for s in (1, 3, 4, 6, 8, 9, 11):
+        assert ("s", s) in seen, s
