@@ -48,7 +48,7 @@ UNIT = "face-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
@@ -67,7 +67,7 @@ def dist_env():
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region"""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -79,8 +79,8 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                ["stdbuf", "-oL", "nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -90,7 +90,10 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, which: str):
+        setattr(self, which, time.time())
 
     def __exit__(self, *a):
         if self.proc:
@@ -101,9 +104,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        """samples read between the marks t0 and t1 (widened by 0.25 s on each
+        side when the timed region is shorter than the sampling period)"""
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", 1e300)
+        pad = 0.0 if t1 - t0 > 0.5 else 0.25
+        for ts, ln in self.lines:
+            if not (t0 - pad <= ts <= t1 + pad):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -118,7 +127,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window_s": round(t1 - t0, 4), "pad_s": pad}
 
 
 def peaks():
@@ -220,7 +229,7 @@ def main():
     faces = mesh.n_active_faces
     dt = pr.dt
 
-    with torch.cuda.stream(stream):
+    with torch.cuda.stream(stream), ClockSampler(local) as clk:
         for _ in range(args.warmup):
             fp.step(dt, 1, stats=False)
         torch.cuda.synchronize()
@@ -229,12 +238,14 @@ def main():
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local) as clk:
-            e0.record(stream)
-            for _ in range(args.steps):
-                fp.step(dt, 1, stats=False)
-            e1.record(stream)
-            torch.cuda.synchronize()
+        clk.mark("t0")
+        e0.record(stream)
+        for _ in range(args.steps):
+            fp.step(dt, 1, stats=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk.mark("t1")
+        time.sleep(0.3)
         ms = e0.elapsed_time(e1)
         if world > 1:
             dist.barrier()

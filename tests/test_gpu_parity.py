@@ -23,8 +23,16 @@ def _pass(mesh, meta):
     return ctx, fp
 
 
-def rel_err(a, b):
-    return np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
+def assert_close_per_field(a, b, rtol=1e-12, atol_scale=1e-15):
+    """per conserved field and per cell: |a - b| <= rtol |b| + atol_scale *
+    max|b| over the field.  The absolute term only matters for values at the
+    round-off level of their field (e.g. a y-momentum that is zero in exact
+    arithmetic in a 1D problem)."""
+    for k in range(b.shape[1]):
+        scale = np.max(np.abs(b[:, k]))
+        err = np.abs(a[:, k] - b[:, k])
+        lim = rtol * np.abs(b[:, k]) + atol_scale * scale
+        assert np.all(err <= lim), (k, float(np.max(err / np.maximum(lim, 1e-300))))
 
 
 @pytest.mark.parametrize("name", MESH_CASES)
@@ -55,8 +63,7 @@ def test_steps_bitwise_vs_reference(cuda_ok, name):
     W, Q = fp.state()
     np.testing.assert_array_equal(Q, ref["ref_sfxpow_Q"])
     np.testing.assert_array_equal(W, ref["ref_sfxpow_W"])
-    for k in range(mesh.dim + 2):
-        assert rel_err(Q[:, k], ref["ref_libm_Q"][:, k]) <= 1e-12
+    assert_close_per_field(Q, ref["ref_libm_Q"])
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -102,8 +109,7 @@ def test_sod2d_c1_full_config_vs_oracle(cuda_ok, oracle):
     np.testing.assert_array_equal(Q, o["Q"])
     np.testing.assert_array_equal(W, o["W"])
     ol = oracle.run(pr.mesh, Params(solver="Exact", use_libm_pow=True), pr.dt, pr.nsteps, pr.W0)
-    for k in range(4):
-        assert rel_err(Q[:, k], ol["Q"][:, k]) <= 1e-12
+    assert_close_per_field(Q, ol["Q"])
     # mass is conserved to round-off in the reflective box
     m0 = oracle.init_Q(pr.mesh, Params(solver="Exact"), pr.W0)[:, 0].sum()
     assert abs(st.totals[0] - m0) <= 1e-13 * m0
