@@ -91,6 +91,21 @@ int check_err(sfx_mesh* m, sfx_stats* st) {
     return status;
 }
 
+/* one phase of a step: 0 gradients, 1 face fluxes, 2 update */
+int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t s) {
+    sfx_ctx* c = m->ctx;
+    const bool split = c->cfg.precision == SFX_PREC_SPLIT;
+    switch(phase) {
+    case 0:
+        return split ? sfx_split_gradients(&m->d, s) : sfx_fp64_gradients(&m->d, s);
+    case 1:
+        return split ? sfx_split_faces(&m->d, &c->sp, dt, s)
+                     : sfx_fp64_faces(&m->d, &c->sp, dt, write_branch, s);
+    default:
+        return split ? sfx_split_apply(&m->d, &c->sp, s) : sfx_fp64_apply(&m->d, &c->sp, s);
+    }
+}
+
 int reset_err(sfx_mesh* m) {
     sfx_dev_error e;
     e.face_key = ~0ull;
@@ -245,6 +260,21 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     A(&d.branch, F);
     A(&d.err, 1);
     A(&d.totals_scratch, (size_t)(S + 1) * 1024);
+    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
+    if(split) {
+        if(d.has_velocity) {
+            sfx_mesh_free(m);
+            return SFX_ERR_UNSUPPORTED; /* the split pass is for static meshes */
+        }
+        A(&d.fg, 2 * F);
+        A(&d.fi, F);
+        A(&d.fsh, F);
+        A(&d.cw, 2 * n);
+        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
+        A(&d.cx, n);
+        A(&d.dq4, F);
+        A(&d.dq1, F);
+    }
     if(rc != SFX_OK) {
         sfx_mesh_free(m);
         return rc;
@@ -272,6 +302,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     if(!rc) rc = cuda_ok(cudaMemsetAsync(d.W, 0, sizeof(double) * n * S, s));
     if(!rc) rc = cuda_ok(cudaMemsetAsync(d.Q, 0, sizeof(double) * n * S, s));
     if(!rc) rc = reset_err(m);
+    if(!rc && split) rc = sfx_split_prepare(&d, s);
     /* host staging buffers go out of scope: wait for the copies */
     if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
     if(rc != SFX_OK) {
@@ -302,6 +333,7 @@ int sfx_state_upload_W(sfx_mesh* m, const double* W) {
     SFX_TRY(reset_err(m));
     SFX_TRY(h2d(m->d.W, t.data(), t.size(), s));
     SFX_TRY(sfx_fp64_init_Q(&m->d, &m->ctx->sp, s));
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_load_state(&m->d, s));
     return check_err(m, nullptr);
 }
 
@@ -315,6 +347,7 @@ int sfx_state_upload_WQ(sfx_mesh* m, const double* W, const double* Q) {
     SFX_TRY(reset_err(m));
     SFX_TRY(h2d(m->d.W, t1.data(), t1.size(), s));
     SFX_TRY(h2d(m->d.Q, t2.data(), t2.size(), s));
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_load_state(&m->d, s));
     return cuda_ok(cudaStreamSynchronize(s));
 }
 
@@ -324,6 +357,7 @@ int sfx_state_download(sfx_mesh* m, double* W, double* Q) {
     const int S = m->d.S;
     cudaStream_t s = m->ctx->stream;
     std::vector<double> t1(W ? n * S : 0), t2(Q ? n * S : 0);
+    if(W && m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_export_W(&m->d, s));
     if(W)
         SFX_TRY(cuda_ok(cudaMemcpyAsync(t1.data(), m->d.W, sizeof(double) * n * S,
                                         cudaMemcpyDeviceToHost, s)));
@@ -339,14 +373,10 @@ int sfx_state_download(sfx_mesh* m, double* W, double* Q) {
 int sfx_step(sfx_mesh* m, double dt, int32_t nsteps, sfx_stats* st) {
     if(!m || nsteps < 0 || !(dt > 0.)) return SFX_ERR_INVALID;
     sfx_ctx* c = m->ctx;
-    if(c->cfg.precision != SFX_PREC_FP64) return SFX_ERR_UNSUPPORTED;
     cudaStream_t s = c->stream;
     SFX_TRY(reset_err(m));
-    for(int t = 0; t < nsteps; ++t) {
-        SFX_TRY(sfx_fp64_gradients(&m->d, s));
-        SFX_TRY(sfx_fp64_faces(&m->d, &c->sp, dt, 0, s));
-        SFX_TRY(sfx_fp64_apply(&m->d, &c->sp, s));
-    }
+    for(int t = 0; t < nsteps; ++t)
+        for(int ph = 0; ph < 3; ++ph) SFX_TRY(run_phase(m, ph, dt, 0, s));
     if(!st) return SFX_OK;
     std::memset(st, 0, sizeof *st);
     int rc = check_err(m, st);
@@ -359,7 +389,6 @@ int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
                    int32_t* launches) {
     if(!m || nsteps < 0 || !(dt > 0.) || !kernel_ms) return SFX_ERR_INVALID;
     sfx_ctx* c = m->ctx;
-    if(c->cfg.precision != SFX_PREC_FP64) return SFX_ERR_UNSUPPORTED;
     cudaStream_t s = c->stream;
     cudaEvent_t ev[4];
     for(auto& e : ev)
@@ -369,11 +398,11 @@ int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
     int nl = 0;
     for(int t = 0; t < nsteps && rc == SFX_OK; ++t) {
         cudaEventRecord(ev[0], s);
-        rc = sfx_fp64_gradients(&m->d, s);
+        rc = run_phase(m, 0, dt, 0, s);
         cudaEventRecord(ev[1], s);
-        if(!rc) rc = sfx_fp64_faces(&m->d, &c->sp, dt, 0, s);
+        if(!rc) rc = run_phase(m, 1, dt, 0, s);
         cudaEventRecord(ev[2], s);
-        if(!rc) rc = sfx_fp64_apply(&m->d, &c->sp, s);
+        if(!rc) rc = run_phase(m, 2, dt, 0, s);
         cudaEventRecord(ev[3], s);
         nl += 3;
         if(!rc) rc = cuda_ok(cudaEventSynchronize(ev[3]));
@@ -397,13 +426,26 @@ int sfx_flux_pass(sfx_mesh* m, double dt, double* grad, double* dQ_face,
     cudaStream_t s = c->stream;
     const int64_t n = m->d.n_cells, F = m->d.n_faces;
     const int S = m->d.S, D = m->d.dim;
+    const bool split = c->cfg.precision == SFX_PREC_SPLIT;
     SFX_TRY(reset_err(m));
-    SFX_TRY(sfx_fp64_gradients(&m->d, s));
-    SFX_TRY(sfx_fp64_faces(&m->d, &c->sp, dt, 1, s));
+    SFX_TRY(run_phase(m, 0, dt, 1, s));
+    SFX_TRY(run_phase(m, 1, dt, 1, s));
+    if(split) SFX_TRY(sfx_split_export_dQ(&m->d, s));
     std::vector<double> tg(grad ? n * D * S : 0), tq(dQ_face ? F * S : 0);
-    if(grad)
+    if(grad && split) {
+        /* FP32 gradient records [n][G float4] -> [D*S][n] */
+        const int G = (D * S + 3) / 4;
+        std::vector<float> tf((size_t)n * G * 4);
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(tf.data(), m->d.cg, sizeof(float) * tf.size(),
+                                        cudaMemcpyDeviceToHost, s)));
+        SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+        for(int64_t i = 0; i < n; ++i)
+            for(int q = 0; q < D * S; ++q) tg[(size_t)q * n + i] = tf[(size_t)i * G * 4 + q];
+    } else if(grad) {
         SFX_TRY(cuda_ok(cudaMemcpyAsync(tg.data(), m->d.grad, sizeof(double) * tg.size(),
                                         cudaMemcpyDeviceToHost, s)));
+    }
+    if(branch && split && F) SFX_TRY(cuda_ok(cudaMemsetAsync(m->d.branch, 0, 4 * F, s)));
     if(dQ_face)
         SFX_TRY(cuda_ok(cudaMemcpyAsync(tq.data(), m->d.dQf, sizeof(double) * tq.size(),
                                         cudaMemcpyDeviceToHost, s)));

@@ -50,6 +50,25 @@ struct sfx_dmesh {
     int32_t* branch; /* [F] scratch or NULL */
     sfx_dev_error* err;
     double* totals_scratch; /* [S * 1024] */
+    /* ---- FP32/FP64-split arrays (precision SFX_PREC_SPLIT only) ----
+     * fg [2F] float4: {A, c0, c1, c2}, {r0, r1, r2, |r|} (2D: {A, c0, c1, r0},
+     *     {r1, |r|, 0, 0}) with c = midpoint - (x_L + x_R)/2 and
+     *     r = x_L - x_R (right generator at its image/mirror position),
+     *     computed in FP64 and rounded once;
+     * fi [F] int2: {L, R}; R = -1 mirror, R | 1<<30 periodic image;
+     * fsh [F]: periodic image shift, 2 bits per axis (0, +1, -1 box);
+     * cw [2n] float4 cell record {rho, v.., p | Q.m, total area ..};
+     * cg [G*n] float4 gradients (G = 4 in 3D, 2 in 2D);
+     * cx [n] float4 {x - centroid, volume};
+     * dq4/dq1 [F]: per-face limited dQ of the left cell (float4 + float). */
+    float4* fg;
+    int2* fi;
+    uint8_t* fsh;
+    float4* cw;
+    float4* cg;
+    float4* cx;
+    float4* dq4;
+    float* dq1;
 };
 
 struct sfx_solver_params {
@@ -74,5 +93,17 @@ int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n,
                      const double* dWL, const double* dWR, const double* dn,
                      int reflective, double* dhalf, double* dflux,
                      int32_t* dcode, void* stream);
+
+/* FP32/FP64-split kernels (sfx_split.cu) */
+int sfx_split_prepare(const sfx_dmesh* m, void* stream);
+int sfx_split_load_state(const sfx_dmesh* m, void* stream);
+int sfx_split_gradients(const sfx_dmesh* m, void* stream);
+int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
+                    void* stream);
+int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream);
+/* W (FP64 SoA) from the FP32 cell records, for downloads */
+int sfx_split_export_W(const sfx_dmesh* m, void* stream);
+/* per-face dQ (FP32) widened into dQf (FP64 SoA), for parity checks */
+int sfx_split_export_dQ(const sfx_dmesh* m, void* stream);
 
 #endif

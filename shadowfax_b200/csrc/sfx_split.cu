@@ -1,0 +1,1056 @@
+/*
+ * FP32/FP64-split flux pass for sm_100a.
+ *
+ * Same algorithm as the plain-FP64 pass (VorCell::estimate_gradient,
+ * VorFace::calculate_flux, update_Q/get_W; src/VorCell.cpp:464-530,
+ * src/VorFace.cpp:670-1024, src/Simulation.cpp:473-483, 791-836), with the
+ * precision chosen per step:
+ *   FP32  gradients, slope limiters, reconstruction, MUSCL-Hancock prediction,
+ *         HLLC fluxes, per-face dQ
+ *   FP64  the exact solver's pressure iteration and wave sampling (pressure
+ *         ratio powers lose digits near vacuum and strong shocks), the
+ *         per-cell accumulation of dQ and Q -= dQ, get_W, the conservation
+ *         totals.
+ * Geometry is precomputed once per mesh in FP64 and rounded once to FP32 as
+ * differences (c = midpoint - (x_L + x_R)/2, r = x_L - x_R, x - centroid), so
+ * no FP32 subtraction of nearby absolute positions happens per step.
+ *
+ * Memory layout (one 32-byte cell record, 64-byte gradient record, 32-byte
+ * face geometry record, 8-byte face index record) keeps every gather a pair
+ * of 16-byte vector loads.  No floating-point atomics: each cell sums its own
+ * faces in ascending face order in FP64, so reruns are bitwise identical and
+ * the face flux leaving one cell enters the other exactly.
+ */
+#include <cuda_runtime.h>
+
+#include "sfx_internal.h"
+
+namespace {
+
+constexpr unsigned kRightBit = 0x80000000u;
+constexpr int kPeriodicBit = 1 << 30;
+constexpr int kIndexMask = (1 << 30) - 1;
+
+__device__ __forceinline__ void report_face(sfx_dev_error* e, int f, int st) {
+    atomicMin(&e->face_key, ((unsigned long long)(unsigned)f << 8) | (unsigned)st);
+}
+__device__ __forceinline__ void report_cell(sfx_dev_error* e, int i, int st) {
+    atomicMin(&e->cell_key, ((unsigned long long)(unsigned)i << 8) | (unsigned)st);
+}
+__device__ __forceinline__ bool failed(const sfx_dev_error* e) {
+    return (*(volatile const unsigned long long*)&e->face_key != ~0ull) ||
+           (*(volatile const unsigned long long*)&e->cell_key != ~0ull);
+}
+
+template <int D>
+struct Cell {
+    static constexpr int S = D + 2;
+    float W[S];
+    float Qm, tarea;
+};
+
+template <int D>
+__device__ __forceinline__ Cell<D> load_cell(const float4* __restrict__ cw, int i) {
+    const float4 a = __ldg(cw + 2 * i);
+    const float4 b = __ldg(cw + 2 * i + 1);
+    Cell<D> c;
+    c.W[0] = a.x;
+    c.W[1] = a.y;
+    c.W[2] = a.z;
+    c.W[3] = a.w;
+    if(D == 3) {
+        c.W[D + 1] = b.x;
+        c.Qm = b.y;
+        c.tarea = b.z;
+    } else {
+        c.Qm = b.x;
+        c.tarea = b.y;
+    }
+    return c;
+}
+
+template <int D>
+__device__ __forceinline__ void store_cell(float4* cw, int i, const float* W, float Qm,
+                                           float tarea) {
+    if(D == 3) {
+        cw[2 * i] = make_float4(W[0], W[1], W[2], W[3]);
+        cw[2 * i + 1] = make_float4(W[4], Qm, tarea, 0.f);
+    } else {
+        cw[2 * i] = make_float4(W[0], W[1], W[2], W[3]);
+        cw[2 * i + 1] = make_float4(Qm, tarea, 0.f, 0.f);
+    }
+}
+
+/* gradient record: g[l][k] at flat l*S+k, padded to float4s */
+template <int D>
+__device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i,
+                                          float (*g)[D + 2]) {
+    constexpr int S = D + 2, G = (D * S + 3) / 4;
+    float t[4 * G];
+#pragma unroll
+    for(int q = 0; q < G; ++q) {
+        const float4 v = __ldg(cg + (size_t)G * i + q);
+        t[4 * q] = v.x;
+        t[4 * q + 1] = v.y;
+        t[4 * q + 2] = v.z;
+        t[4 * q + 3] = v.w;
+    }
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+#pragma unroll
+        for(int k = 0; k < S; ++k) g[l][k] = t[l * S + k];
+}
+
+template <int D>
+__device__ __forceinline__ void geom(const float4* __restrict__ fg, int f, float& A, float* c,
+                                     float* r, float& rn) {
+    const float4 g0 = __ldg(fg + 2 * f);
+    const float4 g1 = __ldg(fg + 2 * f + 1);
+    A = g0.x;
+    c[0] = g0.y;
+    c[1] = g0.z;
+    if(D == 3) {
+        c[2] = g0.w;
+        r[0] = g1.x;
+        r[1] = g1.y;
+        r[2] = g1.z;
+        rn = g1.w;
+    } else {
+        r[0] = g0.w;
+        r[1] = g1.x;
+        rn = g1.y;
+    }
+}
+
+/* ------------------------------- prepare ------------------------------- */
+template <int D>
+__global__ void k_prep_faces(sfx_dmesh m) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= m.n_faces) return;
+    const int n = m.n_cells, F = m.n_faces;
+    const int L = m.left[f];
+    double c[D], r[D], xl[D], xr[D];
+    for(int l = 0; l < D; ++l) {
+        xl[l] = m.pos[(size_t)l * n + L];
+        xr[l] = m.rpos[(size_t)l * F + f];
+        c[l] = m.mid[(size_t)l * F + f] - 0.5 * (xl[l] + xr[l]);
+        r[l] = xl[l] - xr[l];
+    }
+    double rn2 = 0.;
+    for(int l = 0; l < D; ++l) rn2 += r[l] * r[l];
+    const float A = (float)m.area[f];
+    const float rn = (float)sqrt(rn2);
+    if(D == 3) {
+        m.fg[2 * f] = make_float4(A, (float)c[0], (float)c[1], (float)c[2]);
+        m.fg[2 * f + 1] = make_float4((float)r[0], (float)r[1], (float)r[2], rn);
+    } else {
+        m.fg[2 * f] = make_float4(A, (float)c[0], (float)c[1], (float)r[0]);
+        m.fg[2 * f + 1] = make_float4((float)r[1], rn, 0.f, 0.f);
+    }
+    const int kind = m.kind[f];
+    int R = -1;
+    uint8_t sh = 0;
+    if(kind == SFX_FACE_REAL) {
+        R = m.right[f];
+    } else if(kind == SFX_FACE_PERIODIC) {
+        R = m.right[f] | kPeriodicBit;
+        for(int l = 0; l < D; ++l) {
+            const double s = xr[l] - m.pos[(size_t)l * n + m.right[f]];
+            const int code = s > 0.5 ? 1 : (s < -0.5 ? 2 : 0);
+            sh |= (uint8_t)(code << (2 * l));
+        }
+    }
+    m.fi[f] = make_int2(L, R);
+    m.fsh[f] = sh;
+}
+
+template <int D>
+__global__ void k_prep_cells(sfx_dmesh m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    const int n = m.n_cells;
+    float v[3] = {0.f, 0.f, 0.f};
+    for(int l = 0; l < D; ++l)
+        v[l] = (float)(m.pos[(size_t)l * n + i] - m.cen[(size_t)l * n + i]);
+    m.cx[i] = make_float4(v[0], v[1], v[2], (float)m.vol[i]);
+}
+
+/* W (FP64 SoA) and Q (FP64 SoA) -> FP32 cell records */
+template <int D>
+__global__ void k_load_state(sfx_dmesh m) {
+    constexpr int S = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    const int n = m.n_cells;
+    float W[S];
+    for(int k = 0; k < S; ++k) W[k] = (float)m.W[(size_t)k * n + i];
+    store_cell<D>(m.cw, i, W, (float)m.Q[i], (float)m.tarea[i]);
+}
+
+template <int D>
+__global__ void k_export_W(sfx_dmesh m) {
+    constexpr int S = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    const int n = m.n_cells;
+    const Cell<D> c = load_cell<D>(m.cw, i);
+    for(int k = 0; k < S; ++k) m.W[(size_t)k * n + i] = c.W[k];
+}
+
+template <int D>
+__global__ void k_export_dQ(sfx_dmesh m) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= m.n_faces) return;
+    const int F = m.n_faces;
+    const float4 a = m.dq4[f];
+    m.dQf[f] = a.x;
+    m.dQf[(size_t)F + f] = a.y;
+    m.dQf[(size_t)2 * F + f] = a.z;
+    m.dQf[(size_t)3 * F + f] = a.w;
+    if(D == 3) m.dQf[(size_t)4 * F + f] = m.dq1[f];
+}
+
+/* ------------------------------ gradients ------------------------------ */
+template <int D>
+__global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
+    constexpr int S = D + 2, G = (D * S + 3) / 4;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells || failed(m.err)) return;
+    const Cell<D> own = load_cell<D>(m.cw, i);
+    const float4 xv = __ldg(m.cx + i);
+    const float xmc[3] = {xv.x, xv.y, xv.z};
+    float W[S], Wmax[S], Wmin[S], delta[D][S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) {
+        W[k] = own.W[k];
+        Wmax[k] = W[k];
+        Wmin[k] = W[k];
+#pragma unroll
+        for(int l = 0; l < D; ++l) delta[l][k] = 0.f;
+    }
+    const int beg = __ldg(m.off + i), end = __ldg(m.off + i + 1);
+    for(int j = beg; j < end; ++j) {
+        const unsigned e = (unsigned)__ldg(m.idx + j);
+        const int f = (int)(e & ~kRightBit);
+        const bool right = e & kRightBit;
+        float A, c[D], r[D], rn;
+        geom<D>(m.fg, f, A, c, r, rn);
+        if(A == 0.f) continue;
+        if(right) {
+#pragma unroll
+            for(int l = 0; l < D; ++l) r[l] = -r[l];
+        }
+        const int2 fi = __ldg(m.fi + f);
+        float Wj[S];
+        if(!right && fi.y < 0) {
+            /* reflective mirror: flip the velocity component along the face
+             * normal (VorFace::transform / invtransform, VorFace.cpp:417-542) */
+            float vn = 0.f;
+#pragma unroll
+            for(int l = 0; l < D; ++l) vn += W[1 + l] * r[l];
+            vn = 2.f * vn / (rn * rn);
+#pragma unroll
+            for(int k = 0; k < S; ++k) Wj[k] = W[k];
+#pragma unroll
+            for(int l = 0; l < D; ++l) Wj[1 + l] = W[1 + l] - vn * r[l];
+        } else {
+            const int nb = right ? fi.x : (fi.y & kIndexMask);
+            const Cell<D> cn = load_cell<D>(m.cw, nb);
+#pragma unroll
+            for(int k = 0; k < S; ++k) Wj[k] = cn.W[k];
+        }
+        const float s = A / rn;
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            const float dW = Wj[k] - W[k];
+            const float sW = 0.5f * (W[k] + Wj[k]);
+#pragma unroll
+            for(int l = 0; l < D; ++l) delta[l][k] += s * (dW * c[l] - sW * r[l]);
+            Wmax[k] = fmaxf(Wmax[k], Wj[k]);
+            Wmin[k] = fminf(Wmin[k], Wj[k]);
+        }
+    }
+    const float iv = 1.f / xv.w;
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+#pragma unroll
+        for(int k = 0; k < S; ++k) delta[l][k] *= iv;
+    float alpha[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) alpha[k] = 1.f;
+    for(int j = beg; j < end; ++j) {
+        const unsigned e = (unsigned)__ldg(m.idx + j);
+        const int f = (int)(e & ~kRightBit);
+        const bool right = e & kRightBit;
+        float A, c[D], r[D], rn;
+        geom<D>(m.fg, f, A, c, r, rn);
+        if(A == 0.f) continue;
+        /* midpoint - centroid = c + (x - centroid) - r_cell / 2 */
+        float d[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) d[l] = c[l] + xmc[l] + (right ? 0.5f : -0.5f) * r[l];
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            float dp = 0.f;
+#pragma unroll
+            for(int l = 0; l < D; ++l) dp += delta[l][k] * d[l];
+            float mx = 1.f;
+            if(dp != 0.f) {
+                const float id = 1.f / dp;
+                mx = fmaxf((Wmax[k] - W[k]) * id, (Wmin[k] - W[k]) * id);
+            }
+            alpha[k] = fminf(alpha[k], mx);
+        }
+    }
+    float out[4 * G];
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+#pragma unroll
+        for(int k = 0; k < S; ++k) out[l * S + k] = delta[l][k] * alpha[k];
+#pragma unroll
+    for(int q = D * S; q < 4 * G; ++q) out[q] = 0.f;
+#pragma unroll
+    for(int q = 0; q < G; ++q)
+        m.cg[(size_t)G * i + q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2],
+                                              out[4 * q + 3]);
+}
+
+/* ----------------------------- face physics ----------------------------- */
+template <int D>
+__device__ __forceinline__ void sdwdt(float gamma, const float* W, const float (*g)[D + 2],
+                                      float* dW) {
+    const float ir = 1.f / W[0];
+    if(D == 3) {
+        const float div = g[0][1] + g[1][2] + g[2][3];
+        dW[0] = -W[0] * div - W[1] * g[0][0] - W[2] * g[1][0] - W[3] * g[2][0];
+        dW[1] = -W[1] * g[0][1] - W[2] * g[1][1] - W[3] * g[2][1] - g[0][4] * ir;
+        dW[2] = -W[1] * g[0][2] - W[2] * g[1][2] - W[3] * g[2][2] - g[1][4] * ir;
+        dW[3] = -W[1] * g[0][3] - W[2] * g[1][3] - W[3] * g[2][3] - g[2][4] * ir;
+        dW[4] = -gamma * W[4] * div - W[1] * g[0][4] - W[2] * g[1][4] - W[3] * g[2][4];
+    } else {
+        dW[0] = -W[1] * g[0][0] - W[2] * g[1][0] - W[0] * (g[0][1] + g[1][2]);
+        dW[1] = -W[1] * g[0][1] - W[2] * g[1][1] - g[0][3] * ir;
+        /* the reference's 2D row uses d(vy)/dy twice (ExactRiemannSolver.cpp:920) */
+        dW[2] = -W[1] * g[1][2] - W[2] * g[1][2] - g[1][3] * ir;
+        dW[3] = -gamma * W[3] * (g[0][1] + g[1][2]) - W[1] * g[0][3] - W[2] * g[1][3];
+    }
+}
+
+/* VorFace.hpp:92-137 in FP32 */
+__device__ __forceinline__ float slimit(float phimid0, float phiL, float phiR, float dr) {
+    const float delta1 = 0.5f * fabsf(phiL - phiR);
+    const float delta2 = 0.25f * fabsf(phiL - phiR);
+    const float phimin = fminf(phiL, phiR);
+    const float phimax = fmaxf(phiL, phiR);
+    const float phibar = phiL + dr * (phiR - phiL);
+    if(phiL == phiR) return phiL;
+    if(phiL < phiR) {
+        const float phiminus = (phimin - delta1) * phimin > 0.f
+                                   ? phimin - delta1
+                                   : phimin / (1.f + delta1 / fabsf(phimin));
+        return fmaxf(phiminus, fminf(phibar + delta2, phimid0));
+    }
+    const float phiplus = (phimax + delta1) * phimax > 0.f ? phimax + delta1
+                                                           : phimax / (1.f + delta1 / fabsf(phimax));
+    return fminf(phiplus, fmaxf(phibar - delta2, phimid0));
+}
+
+template <int D>
+__device__ __forceinline__ void spredict(float gamma, float hdt, float* Wt, const float* Wself,
+                                         const float* Wother, const float (*g)[D + 2],
+                                         const float* d, bool do_limit, float r) {
+    constexpr int S = D + 2;
+    float dW[S];
+    sdwdt<D>(gamma, Wt, g, dW);
+#pragma unroll
+    for(int k = 0; k < S; ++k) {
+        float s = 0.f;
+#pragma unroll
+        for(int l = 0; l < D; ++l) s += g[l][k] * d[l];
+        Wt[k] += s;
+    }
+    if(do_limit) {
+        float dn = 0.f;
+#pragma unroll
+        for(int l = 0; l < D; ++l) dn += d[l] * d[l];
+        const float dr = sqrtf(dn) / r;
+#pragma unroll
+        for(int k = 0; k < S; ++k) Wt[k] = slimit(Wt[k], Wself[k], Wother[k], dr);
+    }
+    if(Wt[0] < 0.f || Wt[D + 1] < 0.f) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) Wt[k] = Wself[k];
+    }
+    bool neg = false;
+#pragma unroll
+    for(int k = 0; k < S; ++k) dW[k] *= hdt;
+    float t0 = Wt[0] + dW[0], tp = Wt[D + 1] + dW[D + 1];
+    neg = t0 < 0.f || tp < 0.f;
+    if(!neg) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) Wt[k] += dW[k];
+    }
+}
+
+/* HLLC (HLLCRiemannSolver.cpp:258-403) in FP32; the vacuum branch
+ * (HLLCRiemannSolver.cpp:44-209) samples the exact vacuum solution */
+template <int D>
+__device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflective,
+                      float* flux) {
+    constexpr int S = D + 2;
+#pragma unroll
+    for(int k = 0; k < S; ++k) flux[k] = 0.f;
+    if(WL[0] == 0.f && (reflective || WR[0] == 0.f)) return;
+    float uL = 0.f, uR = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        uL += WL[1 + l] * n[l];
+        uR += WR[1 + l] * n[l];
+    }
+    if(reflective) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) WR[k] = WL[k];
+        uR = -uL;
+    }
+    const float gm1 = g - 1.f;
+    const float aL = WL[0] != 0.f ? sqrtf(g * WL[D + 1] / WL[0]) : 0.f;
+    const float aR = WR[0] != 0.f ? sqrtf(g * WR[D + 1] / WR[0]) : 0.f;
+    if(WL[0] == 0.f || WR[0] == 0.f || 2.f * (aL + aR) / gm1 <= uR - uL) {
+        /* exact vacuum solution at x/t = 0 */
+        float sol[S], vhalf = 0.f;
+        const float tdgp1 = 2.f / (g + 1.f), gm1dgp1 = gm1 / (g + 1.f);
+        bool vac = false, fan = false;
+        const float* Ws = WL;
+        if(WR[0] == 0.f) {
+            Ws = WL;
+            if(aL > uL) {
+                if(uL + 2.f * aL / gm1 > 0.f) {
+                    const float base = tdgp1 + gm1dgp1 / aL * uL;
+                    vhalf = tdgp1 * (aL + 0.5f * gm1 * uL) - uL;
+#pragma unroll
+                    for(int k = 0; k < S; ++k) sol[k] = WL[k];
+                    sol[0] = WL[0] * powf(base, 2.f / gm1);
+                    sol[D + 1] = WL[D + 1] * powf(base, 2.f * g / gm1);
+                    fan = true;
+                } else {
+                    vac = true;
+                }
+            }
+        } else if(WL[0] == 0.f) {
+            Ws = WR;
+            if(-uR < aR) {
+                if(uR - 2.f * aR / gm1 >= 0.f) {
+                    vac = true;
+                } else {
+                    const float base = tdgp1 - gm1dgp1 / aR * uR;
+                    vhalf = tdgp1 * (-aR + 0.5f * gm1 * uR) - uR;
+#pragma unroll
+                    for(int k = 0; k < S; ++k) sol[k] = WR[k];
+                    sol[0] = WR[0] * powf(base, 2.f / gm1);
+                    sol[D + 1] = WR[D + 1] * powf(base, 2.f * g / gm1);
+                    fan = true;
+                }
+            }
+        } else {
+            const float SR = uR - 2.f * aR / gm1, SL = uL + 2.f * aL / gm1;
+            if(SR > 0.f && SL < 0.f) {
+                vac = true;
+            } else if(SL >= 0.f) {
+                Ws = WL;
+                if(aL > uL) {
+                    const float base = tdgp1 + gm1dgp1 / aL * uL;
+                    vhalf = tdgp1 * (aL + 0.5f * gm1 * uL) - uL;
+#pragma unroll
+                    for(int k = 0; k < S; ++k) sol[k] = WL[k];
+                    sol[0] = WL[0] * powf(base, 2.f / gm1);
+                    sol[D + 1] = WL[D + 1] * powf(base, 2.f * g / gm1);
+                    fan = true;
+                }
+            } else {
+                Ws = WR;
+                if(-uR < aR) {
+                    const float base = tdgp1 - gm1dgp1 / aR * uR;
+                    vhalf = tdgp1 * (-aR + 0.5f * gm1 * uR) - uR;
+#pragma unroll
+                    for(int k = 0; k < S; ++k) sol[k] = WR[k];
+                    sol[0] = WR[0] * powf(base, 2.f / gm1);
+                    sol[D + 1] = WR[D + 1] * powf(base, 2.f * g / gm1);
+                    fan = true;
+                }
+            }
+        }
+        if(vac) return;
+        if(!fan) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) sol[k] = Ws[k];
+        }
+#pragma unroll
+        for(int l = 0; l < D; ++l) sol[1 + l] += vhalf * n[l];
+        if(sol[0] == 0.f) return;
+        float vsol = 0.f, v2 = 0.f;
+#pragma unroll
+        for(int l = 0; l < D; ++l) {
+            vsol += sol[1 + l] * n[l];
+            v2 += sol[1 + l] * sol[1 + l];
+        }
+        flux[0] = sol[0] * vsol;
+#pragma unroll
+        for(int l = 0; l < D; ++l) flux[1 + l] = sol[0] * sol[1 + l] * vsol + sol[D + 1] * n[l];
+        const float e = sol[D + 1] / gm1 / sol[0] + 0.5f * v2;
+        flux[D + 1] = (sol[0] * e + sol[D + 1]) * vsol;
+        return;
+    }
+    const float rhobar = 0.5f * (WL[0] + WR[0]);
+    const float abar = 0.5f * (aL + aR);
+    const float pstar = fmaxf(0.f, 0.5f * (WL[D + 1] + WR[D + 1]) - 0.5f * (uR - uL) * rhobar * abar);
+    const float gp = 0.5f * (g + 1.f) / g;
+    const float qL = pstar > WL[D + 1] ? sqrtf(1.f + gp * (pstar / WL[D + 1] - 1.f)) : 1.f;
+    const float qR = pstar > WR[D + 1] ? sqrtf(1.f + gp * (pstar / WR[D + 1] - 1.f)) : 1.f;
+    const float SL = uL - aL * qL;
+    const float SR = uR + aR * qR;
+    const float Sstar = (WR[D + 1] - WL[D + 1] + WL[0] * uL * (SL - uL) - WR[0] * uR * (SR - uR)) /
+                        (WL[0] * (SL - uL) - WR[0] * (SR - uR));
+    const bool left = Sstar >= 0.f;
+    const float* Wk = left ? WL : WR;
+    const float uk = left ? uL : uR;
+    const float Sk = left ? SL : SR;
+    float v2 = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) v2 += Wk[1 + l] * Wk[1 + l];
+    const float ek = Wk[D + 1] / gm1 / Wk[0] + 0.5f * v2;
+    flux[0] = Wk[0] * uk;
+#pragma unroll
+    for(int l = 0; l < D; ++l) flux[1 + l] = Wk[0] * Wk[1 + l] * uk + Wk[D + 1] * n[l];
+    flux[D + 1] = (Wk[0] * ek + Wk[D + 1]) * uk;
+    if(left ? (SL < 0.f) : (SR > 0.f)) {
+        const float fac = Wk[0] * (Sk - uk) / (Sk - Sstar);
+        const float ds = Sstar - uk;
+        flux[0] += Sk * (fac - Wk[0]);
+#pragma unroll
+        for(int l = 0; l < D; ++l)
+            flux[1 + l] += Sk * ((Wk[1 + l] + ds * n[l]) * fac - Wk[0] * Wk[1 + l]);
+        const float Ue = ek + ds * (Sstar + Wk[D + 1] / (Wk[0] * (Sk - uk)));
+        flux[D + 1] += Sk * (Ue * fac - Wk[0] * ek);
+    }
+}
+
+/* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
+ * 462-546) with the device pow; returns 0 or SFX_ERR_* */
+template <int D>
+struct XS {
+    const sfx_solver_params& s;
+    __device__ double fb(double p, const double* Wb, double a) const {
+        if(p > Wb[D + 1]) {
+            const double A = s.tdgp1 / Wb[0], B = s.gm1dgp1 * Wb[D + 1];
+            return (p - Wb[D + 1]) * sqrt(A / (p + B));
+        }
+        return s.tdgm1 * a * (pow(p / Wb[D + 1], s.gm1d2g) - 1.);
+    }
+    __device__ double fpb(double p, const double* Wb, double a) const {
+        if(p > Wb[D + 1]) {
+            const double A = s.tdgp1 / Wb[0], B = s.gm1dgp1 * Wb[D + 1];
+            return (1. - 0.5 * (p - Wb[D + 1]) / (B + p)) * sqrt(A / (p + B));
+        }
+        return 1. / (Wb[0] * a) * pow(p / Wb[D + 1], -s.gp1d2g);
+    }
+};
+
+template <int D>
+__device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const double* n,
+                      bool reflective, double* sol) {
+    constexpr int S = D + 2;
+    double vL = 0., vR = 0.;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        vL += WL[1 + l] * n[l];
+        vR += WR[1 + l] * n[l];
+    }
+    if(reflective) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) WR[k] = WL[k];
+        vR = -vL;
+    }
+    const double g = s.gamma;
+    const double aL = WL[0] != 0. ? sqrt(g * WL[D + 1] / WL[0]) : 0.;
+    const double aR = WR[0] != 0. ? sqrt(g * WR[D + 1] / WR[0]) : 0.;
+    double vhalf = 0.;
+    if(WL[0] == 0. || WR[0] == 0. || s.tdgm1 * (aL + aR) <= vR - vL) {
+        /* vacuum cases (ExactRiemannSolver.cpp:304-446) */
+#pragma unroll
+        for(int k = 0; k < S; ++k) sol[k] = 0.;
+        if(WL[0] == 0. && WR[0] == 0.) return SFX_OK;
+        const double SR = vR - s.tdgm1 * aR, SL = vL + s.tdgm1 * aL;
+        int side; /* 0 vacuum, 1 left state, 2 left fan, 3 right state, 4 right fan */
+        if(WR[0] == 0.)
+            side = vL < aL ? (SL > 0. ? 2 : 0) : 1;
+        else if(WL[0] == 0.)
+            side = -aR < vR ? (SR >= 0. ? 0 : 4) : 3;
+        else if(SR > 0. && SL < 0.)
+            side = 0;
+        else if(SL >= 0.)
+            side = aL > vL ? 2 : 1;
+        else
+            side = -aR < vR ? 4 : 3;
+        if(side == 0) return SFX_OK;
+        const double* Ws = side <= 2 ? WL : WR;
+#pragma unroll
+        for(int k = 0; k < S; ++k) sol[k] = Ws[k];
+        if(side == 2) {
+            const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
+            sol[0] = WL[0] * pow(base, s.tdgm1);
+            vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
+            sol[D + 1] = WL[D + 1] * pow(base, s.tgdgm1);
+        } else if(side == 4) {
+            const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
+            sol[0] = WR[0] * pow(base, s.tdgm1);
+            vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
+            sol[D + 1] = WR[D + 1] * pow(base, s.tgdgm1);
+        }
+    } else {
+        XS<D> x{s};
+        const double pL = WL[D + 1], pR = WR[D + 1];
+        const double pmin = fmin(pL, pR), pmax = fmax(pL, pR);
+        double ppv = 0.5 * (pL + pR) - 0.125 * (vR - vL) * (WL[0] + WR[0]) * (aL + aR);
+        const double floorp = s.tol * 0.5 * (pL + pR);
+        ppv = fmax(floorp, ppv);
+        double pg;
+        if(pmax / pmin <= 2. && pmin <= ppv && ppv <= pmax) {
+            pg = ppv;
+        } else if(ppv < pmin) {
+            pg = pow((aL + aR - s.gm1d2 * (vR - vL)) /
+                         (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
+                     s.tgdgm1);
+        } else {
+            const double gL = sqrt(s.tdgp1 / WL[0] / (ppv + s.gm1dgp1 * pL));
+            const double gR = sqrt(s.tdgp1 / WR[0] / (ppv + s.gm1dgp1 * pR));
+            pg = (gL * pL + gR * pR - vR + vL) / (gL + gR);
+        }
+        pg = fmax(floorp, pg);
+        auto f = [&](double p) { return x.fb(p, WL, aL) + x.fb(p, WR, aR) + (vR - vL); };
+        auto fp = [&](double p) { return x.fpb(p, WL, aL) + x.fpb(p, WR, aR); };
+        double p = 0.;
+        const double f0 = f(0.);
+        double fg = f(pg);
+        int it = 0;
+        if(f0 < s.cutoff) {
+            while(fabs(p - pg) > s.tol * 0.5 * (p + pg)) {
+                if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
+                p = pg;
+                pg = fmax(0., pg - fg / fp(pg));
+                fg = f(pg);
+            }
+            p = pg;
+        } else {
+            if(f0 * fg >= 0.) {
+                while(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg < 0.) {
+                    if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
+                    p = pg;
+                    pg = pg - fg / fp(pg);
+                    fg = f(pg);
+                }
+            }
+            if(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg > 0.) {
+                /* Brent on [0, pg] */
+                double a = 0., b = pg, c, d = 1e230, fa = f(a), fbv = fg, fc, sv;
+                if(fa * fbv >= 0.) {
+                    p = fa < fbv ? a : b;
+                } else {
+                    if(fabs(fa) < fabs(fbv)) {
+                        double t = a; a = b; b = t;
+                        t = fa; fa = fbv; fbv = t;
+                    }
+                    c = a;
+                    fc = fa;
+                    bool mflag = true;
+                    const double tol = s.tol;
+                    while(fbv != 0. && fabs(a - b) > tol * (a + b) * 0.5) {
+                        if(++it > 2 * SFX_MAX_ITER) return SFX_ERR_NOCONV;
+                        if(fa != fc && fbv != fc)
+                            sv = a * fbv * fc / (fa - fbv) / (fa - fc) +
+                                 b * fa * fc / (fbv - fa) / (fbv - fc) +
+                                 c * fa * fbv / (fc - fa) / (fc - fbv);
+                        else
+                            sv = b - fbv * (b - a) / (fbv - fa);
+                        const double t2 = (3. * a + b) / 4.;
+                        if(!((sv > t2 && sv < b) || (sv < t2 && sv > b)) ||
+                           (mflag && fabs(sv - b) >= fabs(b - c) / 2.) ||
+                           (!mflag && fabs(sv - b) >= fabs(c - d) / 2.) ||
+                           (mflag && fabs(b - c) < tol * (b + c) * 0.5) ||
+                           (!mflag && fabs(c - d) < tol * (c + d) * 0.5)) {
+                            sv = (a + b) / 2.;
+                            mflag = true;
+                        } else {
+                            mflag = false;
+                        }
+                        const double fs = f(sv);
+                        d = c;
+                        c = b;
+                        fc = fbv;
+                        if(fa * fs < 0.) {
+                            b = sv;
+                            fbv = fs;
+                        } else {
+                            a = sv;
+                            fa = fs;
+                        }
+                        if(fabs(fa) < fabs(fbv)) {
+                            double t = a; a = b; b = t;
+                            t = fa; fa = fbv; fbv = t;
+                        }
+                    }
+                    p = b;
+                }
+            } else {
+                p = pg;
+            }
+        }
+        const double u = 0.5 * (vL + vR) + 0.5 * (x.fb(p, WR, aR) - x.fb(p, WL, aL));
+        if(u < 0.) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) sol[k] = WR[k];
+            const double r = p / pR;
+            if(p > pR) {
+                if(vR + aR * sqrt(s.gp1d2g * r + s.gm1d2g) > 0.) {
+                    sol[0] = WR[0] * (r + s.gm1dgp1) / (s.gm1dgp1 * r + 1.);
+                    sol[D + 1] = p;
+                    vhalf = u - vR;
+                }
+            } else if(vR + aR > 0.) {
+                if(u + aR * pow(r, s.gm1d2g) <= 0.) {
+                    const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
+                    sol[0] = WR[0] * pow(base, s.tdgm1);
+                    vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
+                    sol[D + 1] = pR * pow(base, s.tgdgm1);
+                } else {
+                    sol[0] = WR[0] * pow(r, s.ginv);
+                    sol[D + 1] = p;
+                    vhalf = u - vR;
+                }
+            }
+        } else {
+#pragma unroll
+            for(int k = 0; k < S; ++k) sol[k] = WL[k];
+            const double r = p / pL;
+            if(p > pL) {
+                if(vL - aL * sqrt(s.gp1d2g * r + s.gm1d2g) < 0.) {
+                    sol[0] = WL[0] * (r + s.gm1dgp1) / (s.gm1dgp1 * r + 1.);
+                    sol[D + 1] = p;
+                    vhalf = u - vL;
+                }
+            } else if(vL - aL < 0.) {
+                if(u - aL * pow(r, s.gm1d2g) > 0.) {
+                    const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
+                    sol[0] = WL[0] * pow(base, s.tdgm1);
+                    vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
+                    sol[D + 1] = pL * pow(base, s.tgdgm1);
+                } else {
+                    sol[0] = WL[0] * pow(r, s.ginv);
+                    sol[D + 1] = p;
+                    vhalf = u - vL;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for(int l = 0; l < D; ++l) sol[1 + l] += vhalf * n[l];
+    bool bad = !(sol[0] >= 0.) || !(sol[D + 1] >= 0.);
+#pragma unroll
+    for(int l = 0; l < D; ++l) bad |= sol[1 + l] != sol[1 + l];
+    return bad ? SFX_ERR_RIEMANN : SFX_OK;
+}
+
+template <int D, int SOLVER>
+__global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
+    constexpr int S = D + 2;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= m.n_faces || failed(m.err)) return;
+    float A, c[D], r[D], rn;
+    geom<D>(m.fg, f, A, c, r, rn);
+    if(A == 0.f) {
+        m.dq4[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+        m.dq1[f] = 0.f;
+        return;
+    }
+    const int2 fi = __ldg(m.fi + f);
+    const int iL = fi.x;
+    const bool mirror = fi.y < 0;
+    const int iR = mirror ? 0 : (fi.y & kIndexMask);
+    const float g = (float)sp.gamma;
+    const float hdt = 0.5f * dt;
+    float nrm[D];
+    const float irn = 1.f / rn;
+#pragma unroll
+    for(int l = 0; l < D; ++l) nrm[l] = -r[l] * irn;
+    const Cell<D> cL = load_cell<D>(m.cw, iL);
+    const float4 xL = __ldg(m.cx + iL);
+    const float xmcL[3] = {xL.x, xL.y, xL.z};
+    float WL[S], WR[S], WLr[S], WRr[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) {
+        WL[k] = cL.W[k];
+        WR[k] = 0.f;
+        WRr[k] = 0.f;
+    }
+    float QmR = 0.f, taR = 1.f, rr = 1.f;
+    if(!mirror) {
+        const Cell<D> cR = load_cell<D>(m.cw, iR);
+        const float4 xR = __ldg(m.cx + iR);
+        const float xmcR[3] = {xR.x, xR.y, xR.z};
+#pragma unroll
+        for(int k = 0; k < S; ++k) WR[k] = cR.W[k];
+        QmR = cR.Qm;
+        taR = cR.tarea;
+        /* centroid difference (unshifted centroids, as the reference) */
+        float sh[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) sh[l] = 0.f;
+        if(fi.y & kPeriodicBit) {
+            const unsigned code = __ldg(m.fsh + f);
+#pragma unroll
+            for(int l = 0; l < D; ++l) {
+                const unsigned cc = (code >> (2 * l)) & 3u;
+                sh[l] = cc == 1u ? 1.f : (cc == 2u ? -1.f : 0.f);
+            }
+        }
+        float cd2 = 0.f, dR[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) {
+            const float cd = r[l] + sh[l] - xmcL[l] + xmcR[l];
+            cd2 += cd * cd;
+            dR[l] = c[l] + xmcR[l] + 0.5f * r[l];
+        }
+        rr = sqrtf(cd2);
+        float gR[D][S];
+        load_grad<D>(m.cg, iR, gR);
+#pragma unroll
+        for(int k = 0; k < S; ++k) WRr[k] = WR[k];
+        spredict<D>(g, hdt, WRr, WR, WL, gR, dR, true, rr);
+    }
+    {
+        float dL[D], gL[D][S];
+#pragma unroll
+        for(int l = 0; l < D; ++l) dL[l] = c[l] + xmcL[l] - 0.5f * r[l];
+        load_grad<D>(m.cg, iL, gL);
+#pragma unroll
+        for(int k = 0; k < S; ++k) WLr[k] = WL[k];
+        spredict<D>(g, hdt, WLr, WL, WR, gL, dL, !mirror, rr);
+    }
+    if(WL[0] != 0.f) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) WL[k] = WLr[k];
+    }
+    if(WR[0] != 0.f) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) WR[k] = WRr[k];
+    }
+    float flux[S];
+    int status = SFX_OK;
+    if(SOLVER == SFX_SOLVER_HLLC) {
+        shllc<D>(g, WL, WR, nrm, mirror, flux);
+    } else {
+        double dWL[S], dWR[S], dn[D], h[S];
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            dWL[k] = WL[k];
+            dWR[k] = WR[k];
+        }
+#pragma unroll
+        for(int l = 0; l < D; ++l) dn[l] = nrm[l];
+        status = sexact<D>(sp, dWL, dWR, dn, mirror, h);
+#pragma unroll
+        for(int k = 0; k < S; ++k) flux[k] = 0.f;
+        if(h[0] != 0.) {
+            double un = 0., v2 = 0.;
+#pragma unroll
+            for(int l = 0; l < D; ++l) {
+                un += h[1 + l] * dn[l];
+                v2 += h[1 + l] * h[1 + l];
+            }
+            const double e = 0.5 * h[0] * v2 + h[D + 1] / (sp.gamma - 1.);
+            flux[0] = (float)(h[0] * un);
+#pragma unroll
+            for(int l = 0; l < D; ++l) flux[1 + l] = (float)(h[0] * un * h[1 + l] + h[D + 1] * dn[l]);
+            flux[D + 1] = (float)((e + h[D + 1]) * un);
+        }
+    }
+    const float dtA = dt * A;
+    float dQ[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) dQ[k] = dtA * flux[k];
+    /* over-flux limiter (VorFace.cpp:837-866) */
+    const float afL = A / cL.tarea;
+    if(dQ[0] > afL * cL.Qm) {
+        const float cf = fabsf(afL * cL.Qm / dQ[0]);
+#pragma unroll
+        for(int k = 0; k < S; ++k) dQ[k] *= cf;
+    }
+    if(!mirror) {
+        const float afR = A / taR;
+        if(-dQ[0] > afR * QmR) {
+            const float cf = fabsf(afR * QmR / dQ[0]);
+#pragma unroll
+            for(int k = 0; k < S; ++k) dQ[k] *= cf;
+        }
+    }
+    m.dq4[f] = make_float4(dQ[0], dQ[1], dQ[2], dQ[3]);
+    m.dq1[f] = D == 3 ? dQ[4] : 0.f;
+    if(status == SFX_OK && flux[0] != flux[0]) status = SFX_ERR_NAN_FLUX;
+    if(status != SFX_OK) report_face(m.err, f, status);
+}
+
+/* ------------------------------- update ------------------------------- */
+template <int D>
+__global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
+    constexpr int S = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells || failed(m.err)) return;
+    const int n = m.n_cells;
+    double dQ[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) dQ[k] = 0.;
+    const int beg = __ldg(m.off + i), end = __ldg(m.off + i + 1);
+    for(int j = beg; j < end; ++j) {
+        const unsigned e = (unsigned)__ldg(m.idx + j);
+        const int f = (int)(e & ~kRightBit);
+        const float4 a = __ldg(m.dq4 + f);
+        double v[S];
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = a.z;
+        v[3] = a.w;
+        if(D == 3) v[4] = __ldg(m.dq1 + f);
+        if(e & kRightBit) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) dQ[k] -= v[k];
+        } else {
+#pragma unroll
+            for(int k = 0; k < S; ++k) dQ[k] += v[k];
+        }
+    }
+    double Q[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) Q[k] = m.Q[(size_t)k * n + i] - dQ[k];
+    if(Q[0] < 0. || Q[D + 1] < 0.) {
+        report_cell(m.err, i, SFX_ERR_NEG_STATE);
+        return;
+    }
+    /* get_W (ExactRiemannSolver.cpp:716-766 / HLLCRiemannSolver.cpp:495-535) */
+    const double V = m.vol[i];
+    double W[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) W[k] = 0.;
+    if(Q[0] != 0.) {
+        const double im = 1. / Q[0];
+        double p2 = 0.;
+        W[0] = Q[0] / V;
+#pragma unroll
+        for(int l = 0; l < D; ++l) {
+            W[1 + l] = Q[1 + l] * im;
+            p2 += Q[1 + l] * Q[1 + l];
+        }
+        W[D + 1] = (gamma - 1.) * (Q[D + 1] - 0.5 * p2 * im) / V;
+        if(W[D + 1] < 1e-30) {
+            W[D + 1] = 1e-30;
+            Q[D + 1] = 0.5 * p2 * im + W[D + 1] * V / (gamma - 1.);
+        }
+        if(W[0] < 1e-30) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) W[k] = 0.;
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < S; ++k) m.Q[(size_t)k * n + i] = Q[k];
+    float Wf[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) Wf[k] = (float)W[k];
+    store_cell<D>(m.cw, i, Wf, (float)Q[0], (float)m.tarea[i]);
+}
+
+inline int grid_for(long long n, int b) {
+    return (int)((n + b - 1) / b);
+}
+inline int cuda_status(cudaError_t e) {
+    return e == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+}
+
+}  // namespace
+
+int sfx_split_prepare(const sfx_dmesh* m, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->n_faces) {
+        if(m->dim == 3)
+            k_prep_faces<3><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
+        else
+            k_prep_faces<2><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
+    }
+    if(m->dim == 3)
+        k_prep_cells<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    else
+        k_prep_cells<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_load_state(const sfx_dmesh* m, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_load_state<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    else
+        k_load_state<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_export_W(const sfx_dmesh* m, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_export_W<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    else
+        k_export_W<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
+    if(!m->n_faces) return SFX_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_export_dQ<3><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
+    else
+        k_export_dQ<2><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_gradients(const sfx_dmesh* m, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_sgrad<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    else
+        k_sgrad<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, void* stream) {
+    if(!m->n_faces) return SFX_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int G = grid_for(m->n_faces, 256);
+    const float fdt = (float)dt;
+    if(m->dim == 3) {
+        if(sp->kind == SFX_SOLVER_EXACT)
+            k_sfaces<3, SFX_SOLVER_EXACT><<<G, 256, 0, s>>>(*m, *sp, fdt);
+        else
+            k_sfaces<3, SFX_SOLVER_HLLC><<<G, 256, 0, s>>>(*m, *sp, fdt);
+    } else {
+        if(sp->kind == SFX_SOLVER_EXACT)
+            k_sfaces<2, SFX_SOLVER_EXACT><<<G, 256, 0, s>>>(*m, *sp, fdt);
+        else
+            k_sfaces<2, SFX_SOLVER_HLLC><<<G, 256, 0, s>>>(*m, *sp, fdt);
+    }
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_sapply<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m, sp->gamma);
+    else
+        k_sapply<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m, sp->gamma);
+    return cuda_status(cudaGetLastError());
+}

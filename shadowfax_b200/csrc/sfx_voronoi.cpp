@@ -38,7 +38,7 @@
 #include <thread>
 #include <vector>
 
-#include "sfx_internal.h"
+#include "../../include/sfxflux.h"
 
 namespace {
 

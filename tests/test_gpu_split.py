@@ -1,0 +1,81 @@
+"""FP32/FP64-split flux pass against the plain-FP64 pass: <= 1e-6 relative L1
+per conserved field, mass and energy conserved to round-off, bitwise
+identical reruns."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_L1 = 1e-6
+
+
+def _run(pr, precision, nsteps=None):
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    ctx = Context(pr.mesh.dim, RiemannSolverFactory.generate(pr.solver, pr.gamma), precision)
+    fp = FluxPass(ctx, pr.mesh)
+    fp.set_primitive(pr.W0)
+    t0 = fp.totals()
+    st = fp.step(pr.dt, pr.nsteps if nsteps is None else nsteps)
+    W, Q = fp.state()
+    return W, Q, t0, np.array(st.totals[: pr.mesh.dim + 2])
+
+
+def l1_rel(a, b):
+    return np.abs(a - b).sum(0) / np.abs(b).sum(0)
+
+
+@pytest.mark.parametrize("case", ["sod2d", "sod2d_hllc", "sedov3d", "random3d_exact",
+                                  "random3d_hllc"])
+def test_split_within_tolerance_of_fp64(cuda_ok, case):
+    from shadowfax_b200 import workloads as wl
+    pr = {
+        "sod2d": lambda: wl.sod2d(n=10_000, nsteps=100),
+        "sod2d_hllc": lambda: wl.sod2d(n=10_000, nsteps=100, solver="HLLC"),
+        "sedov3d": lambda: wl.sedov3d(n=40_000, nsteps=20),
+        "random3d_exact": lambda: wl.random_field3d(n=40_000, nsteps=3),
+        "random3d_hllc": lambda: wl.random_field3d(n=40_000, nsteps=3, solver="HLLC"),
+    }[case]()
+    W64, Q64, _, _ = _run(pr, 0)
+    W32, Q32, t0, t1 = _run(pr, 1)
+    err = l1_rel(Q32, Q64)
+    print(case, "L1 rel per field", err)
+    assert np.all(err <= TOL_L1), err
+    # mass is conserved to round-off (the reflective/periodic box is closed)
+    assert abs(t1[0] - t0[0]) <= 1e-12 * abs(t0[0])
+    # energy too (the flux leaving one cell enters its neighbour exactly)
+    assert abs(t1[-1] - t0[-1]) <= 1e-12 * abs(t0[-1])
+
+
+def test_split_reruns_are_bitwise_identical(cuda_ok):
+    from shadowfax_b200 import workloads as wl
+    pr = wl.sedov3d(n=20_000, nsteps=10)
+    a = _run(pr, 1)[1]
+    b = _run(pr, 1)[1]
+    np.testing.assert_array_equal(a, b)
+
+
+def test_split_single_pass_face_flux_error_by_branch(cuda_ok):
+    """config-3 style: per-face flux error of the split pass vs FP64 for the
+    exact solver, grouped by the FP64 branch (shock / rarefaction / vacuum)"""
+    from shadowfax_b200 import workloads as wl
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    pr = wl.random_field3d(n=40_000)
+    out = {}
+    for prec in (0, 1):
+        ctx = Context(3, RiemannSolverFactory.generate("Exact"), prec)
+        fp = FluxPass(ctx, pr.mesh)
+        fp.set_primitive(pr.W0)
+        grad, dQ, br, rc, _ = fp.flux_pass(pr.dt)
+        assert rc == 0
+        out[prec] = (dQ, br)
+    dQ64, br = out[0]
+    dQ32 = out[1][0]
+    region = (br >> 5) & 15
+    shock = np.isin(region, [1, 6])
+    raref = np.isin(region, [3, 4, 8, 9])
+    scale = np.abs(dQ64).sum(0)
+    for mask in (shock, raref):
+        if mask.any():
+            e = np.abs(dQ32[mask] - dQ64[mask]).sum(0) / np.maximum(np.abs(dQ64[mask]).sum(0), 1e-300)
+            assert np.all(e <= 1e-5), e
+    assert np.all(np.abs(dQ32 - dQ64).sum(0) / scale <= 1e-5)
