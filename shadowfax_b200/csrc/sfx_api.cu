@@ -12,11 +12,16 @@
 
 #include "sfx_internal.h"
 
+/* A context outlives its meshes: sfx_ctx_destroy on a context that still has
+ * meshes only marks it, and the last sfx_mesh_free releases it.  Callers that
+ * free in any order (garbage-collected bindings) stay safe. */
 struct sfx_ctx {
     sfx_config cfg;
     sfx_solver_params sp;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    int live_meshes = 0;
+    bool closing = false;
 };
 
 struct sfx_mesh {
@@ -151,14 +156,20 @@ int sfx_ctx_create(const sfx_config* cfg, sfx_ctx** out) {
     return SFX_OK;
 }
 
-int sfx_ctx_destroy(sfx_ctx* ctx) {
-    if(!ctx) return SFX_ERR_INVALID;
+static void ctx_release(sfx_ctx* ctx) {
     cudaSetDevice(ctx->cfg.device);
     if(ctx->own_stream) {
         cudaStreamSynchronize(ctx->own_stream);
         cudaStreamDestroy(ctx->own_stream);
     }
     delete ctx;
+}
+
+int sfx_ctx_destroy(sfx_ctx* ctx) {
+    if(!ctx || ctx->closing) return SFX_ERR_INVALID;
+    ctx->closing = true;
+    if(ctx->live_meshes > 0) return SFX_OK; /* released with the last mesh */
+    ctx_release(ctx);
     return SFX_OK;
 }
 
@@ -224,9 +235,11 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         }
     }
     SFX_TRY(cuda_ok(cudaSetDevice(ctx->cfg.device)));
+    if(ctx->closing) return SFX_ERR_INVALID;
     sfx_mesh* m = new(std::nothrow) sfx_mesh;
     if(!m) return SFX_ERR_NOMEM;
     m->ctx = ctx;
+    ctx->live_meshes++;
     sfx_dmesh& d = m->d;
     std::memset(&d, 0, sizeof d);
     d.dim = dim;
@@ -272,8 +285,9 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         A(&d.cw, 2 * n);
         A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
         A(&d.cx, n);
-        A(&d.dq4, F);
-        A(&d.dq1, F);
+        A(&d.an, (size_t)dim * F);
+        A(&d.dqm, F);
+        A(&d.dqv, (size_t)dim * F);
     }
     if(rc != SFX_OK) {
         sfx_mesh_free(m);
@@ -315,12 +329,15 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
 
 int sfx_mesh_free(sfx_mesh* m) {
     if(!m) return SFX_ERR_INVALID;
-    if(m->ctx) {
-        cudaSetDevice(m->ctx->cfg.device);
-        cudaStreamSynchronize(m->ctx->stream);
+    sfx_ctx* ctx = m->ctx;
+    if(ctx) {
+        cudaSetDevice(ctx->cfg.device);
+        /* cudaFree waits for the device; a caller stream may already be gone */
+        cudaStreamSynchronize(ctx->own_stream);
     }
     for(void* p : m->allocs) cudaFree(p);
     delete m;
+    if(ctx && --ctx->live_meshes == 0 && ctx->closing) ctx_release(ctx);
     return SFX_OK;
 }
 

@@ -60,15 +60,20 @@ struct sfx_dmesh {
      * cw [2n] float4 cell record {rho, v.., p | Q.m, total area ..};
      * cg [G*n] float4 gradients (G = 4 in 3D, 2 in 2D);
      * cx [n] float4 {x - centroid, volume};
-     * dq4/dq1 [F]: per-face limited dQ of the left cell (float4 + float). */
+     * an [dim][F] FP64 area vector A n (n from x_L to x_R), for the pressure
+     *     force, so that the forces on a cell cancel to FP64 round-off in a
+     *     uniform region;
+     * dqm [F] float2 {mass, energy} and dqv [dim][F] FP64 momentum: the
+     *     limited dQ received by the left cell. */
     float4* fg;
     int2* fi;
     uint8_t* fsh;
     float4* cw;
     float4* cg;
     float4* cx;
-    float4* dq4;
-    float* dq1;
+    double* an;
+    float2* dqm;
+    double* dqv;
 };
 
 struct sfx_solver_params {

@@ -138,8 +138,10 @@ __global__ void k_prep_faces(sfx_dmesh m) {
     }
     double rn2 = 0.;
     for(int l = 0; l < D; ++l) rn2 += r[l] * r[l];
+    const double rn64 = sqrt(rn2);
+    for(int l = 0; l < D; ++l) m.an[(size_t)l * F + f] = m.area[f] * (-r[l] / rn64);
     const float A = (float)m.area[f];
-    const float rn = (float)sqrt(rn2);
+    const float rn = (float)rn64;
     if(D == 3) {
         m.fg[2 * f] = make_float4(A, (float)c[0], (float)c[1], (float)c[2]);
         m.fg[2 * f + 1] = make_float4((float)r[0], (float)r[1], (float)r[2], rn);
@@ -202,13 +204,18 @@ __global__ void k_export_dQ(sfx_dmesh m) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if(f >= m.n_faces) return;
     const int F = m.n_faces;
-    const float4 a = m.dq4[f];
-    m.dQf[f] = a.x;
-    m.dQf[(size_t)F + f] = a.y;
-    m.dQf[(size_t)2 * F + f] = a.z;
-    m.dQf[(size_t)3 * F + f] = a.w;
-    if(D == 3) m.dQf[(size_t)4 * F + f] = m.dq1[f];
+    const float2 me = m.dqm[f];
+    m.dQf[f] = me.x;
+    for(int l = 0; l < D; ++l) m.dQf[(size_t)(1 + l) * F + f] = m.dqv[(size_t)l * F + f];
+    m.dQf[(size_t)(D + 1) * F + f] = me.y;
 }
+
+/* face flux split as: mass m, momentum m v + P n, energy E (the momentum's
+ * pressure part P n is assembled in FP64 with the FP64 area vector) */
+template <int D>
+struct SFlux {
+    float m, mv[D], P, E;
+};
 
 /* ------------------------------ gradients ------------------------------ */
 template <int D>
@@ -396,10 +403,13 @@ __device__ __forceinline__ void spredict(float gamma, float hdt, float* Wt, cons
  * (HLLCRiemannSolver.cpp:44-209) samples the exact vacuum solution */
 template <int D>
 __device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflective,
-                      float* flux) {
+                      SFlux<D>& F) {
     constexpr int S = D + 2;
+    F.m = 0.f;
+    F.P = 0.f;
+    F.E = 0.f;
 #pragma unroll
-    for(int k = 0; k < S; ++k) flux[k] = 0.f;
+    for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
     if(WL[0] == 0.f && (reflective || WR[0] == 0.f)) return;
     float uL = 0.f, uR = 0.f;
 #pragma unroll
@@ -493,11 +503,12 @@ __device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflec
             vsol += sol[1 + l] * n[l];
             v2 += sol[1 + l] * sol[1 + l];
         }
-        flux[0] = sol[0] * vsol;
+        F.m = sol[0] * vsol;
 #pragma unroll
-        for(int l = 0; l < D; ++l) flux[1 + l] = sol[0] * sol[1 + l] * vsol + sol[D + 1] * n[l];
+        for(int l = 0; l < D; ++l) F.mv[l] = F.m * sol[1 + l];
+        F.P = sol[D + 1];
         const float e = sol[D + 1] / gm1 / sol[0] + 0.5f * v2;
-        flux[D + 1] = (sol[0] * e + sol[D + 1]) * vsol;
+        F.E = (sol[0] * e + sol[D + 1]) * vsol;
         return;
     }
     const float rhobar = 0.5f * (WL[0] + WR[0]);
@@ -518,20 +529,22 @@ __device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflec
 #pragma unroll
     for(int l = 0; l < D; ++l) v2 += Wk[1 + l] * Wk[1 + l];
     const float ek = Wk[D + 1] / gm1 / Wk[0] + 0.5f * v2;
-    flux[0] = Wk[0] * uk;
-#pragma unroll
-    for(int l = 0; l < D; ++l) flux[1 + l] = Wk[0] * Wk[1 + l] * uk + Wk[D + 1] * n[l];
-    flux[D + 1] = (Wk[0] * ek + Wk[D + 1]) * uk;
+    /* momentum flux = (mass flux) v + P n with P the star pressure
+     * p_K + S_K fac (S* - u_K) when the star state is used */
+    float mk = Wk[0] * uk;
+    F.P = Wk[D + 1];
+    F.E = (Wk[0] * ek + Wk[D + 1]) * uk;
     if(left ? (SL < 0.f) : (SR > 0.f)) {
         const float fac = Wk[0] * (Sk - uk) / (Sk - Sstar);
         const float ds = Sstar - uk;
-        flux[0] += Sk * (fac - Wk[0]);
-#pragma unroll
-        for(int l = 0; l < D; ++l)
-            flux[1 + l] += Sk * ((Wk[1 + l] + ds * n[l]) * fac - Wk[0] * Wk[1 + l]);
+        mk += Sk * (fac - Wk[0]);
+        F.P += Sk * fac * ds;
         const float Ue = ek + ds * (Sstar + Wk[D + 1] / (Wk[0] * (Sk - uk)));
-        flux[D + 1] += Sk * (Ue * fac - Wk[0] * ek);
+        F.E += Sk * (Ue * fac - Wk[0] * ek);
     }
+    F.m = mk;
+#pragma unroll
+    for(int l = 0; l < D; ++l) F.mv[l] = mk * Wk[1 + l];
 }
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
@@ -767,8 +780,9 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
     float A, c[D], r[D], rn;
     geom<D>(m.fg, f, A, c, r, rn);
     if(A == 0.f) {
-        m.dq4[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-        m.dq1[f] = 0.f;
+        m.dqm[f] = make_float2(0.f, 0.f);
+#pragma unroll
+        for(int l = 0; l < D; ++l) m.dqv[(size_t)l * m.n_faces + f] = 0.;
         return;
     }
     const int2 fi = __ldg(m.fi + f);
@@ -843,10 +857,10 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
 #pragma unroll
         for(int k = 0; k < S; ++k) WR[k] = WRr[k];
     }
-    float flux[S];
+    SFlux<D> F;
     int status = SFX_OK;
     if(SOLVER == SFX_SOLVER_HLLC) {
-        shllc<D>(g, WL, WR, nrm, mirror, flux);
+        shllc<D>(g, WL, WR, nrm, mirror, F);
     } else {
         double dWL[S], dWR[S], dn[D], h[S];
 #pragma unroll
@@ -857,9 +871,13 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
 #pragma unroll
         for(int l = 0; l < D; ++l) dn[l] = nrm[l];
         status = sexact<D>(sp, dWL, dWR, dn, mirror, h);
+        F.m = 0.f;
+        F.P = 0.f;
+        F.E = 0.f;
 #pragma unroll
-        for(int k = 0; k < S; ++k) flux[k] = 0.f;
+        for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
         if(h[0] != 0.) {
+            /* ExactRiemannSolver::get_flux contracted with n (:815-880) */
             double un = 0., v2 = 0.;
 #pragma unroll
             for(int l = 0; l < D; ++l) {
@@ -867,34 +885,46 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
                 v2 += h[1 + l] * h[1 + l];
             }
             const double e = 0.5 * h[0] * v2 + h[D + 1] / (sp.gamma - 1.);
-            flux[0] = (float)(h[0] * un);
+            const double mf = h[0] * un;
+            F.m = (float)mf;
 #pragma unroll
-            for(int l = 0; l < D; ++l) flux[1 + l] = (float)(h[0] * un * h[1 + l] + h[D + 1] * dn[l]);
-            flux[D + 1] = (float)((e + h[D + 1]) * un);
+            for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * h[1 + l]);
+            F.P = (float)h[D + 1];
+            F.E = (float)((e + h[D + 1]) * un);
         }
     }
     const float dtA = dt * A;
-    float dQ[S];
+    float dm = dtA * F.m, dE = dtA * F.E;
+    /* momentum: advective part in FP32, pressure force dt P (A n) in FP64 */
+    double dv[D];
+    const double dtP = (double)dt * (double)F.P;
+    const int FF = m.n_faces;
 #pragma unroll
-    for(int k = 0; k < S; ++k) dQ[k] = dtA * flux[k];
+    for(int l = 0; l < D; ++l)
+        dv[l] = (double)(dtA * F.mv[l]) + dtP * __ldg(m.an + (size_t)l * FF + f);
     /* over-flux limiter (VorFace.cpp:837-866) */
     const float afL = A / cL.tarea;
-    if(dQ[0] > afL * cL.Qm) {
-        const float cf = fabsf(afL * cL.Qm / dQ[0]);
+    if(dm > afL * cL.Qm) {
+        const float cf = fabsf(afL * cL.Qm / dm);
+        dm *= cf;
+        dE *= cf;
 #pragma unroll
-        for(int k = 0; k < S; ++k) dQ[k] *= cf;
+        for(int l = 0; l < D; ++l) dv[l] *= (double)cf;
     }
     if(!mirror) {
         const float afR = A / taR;
-        if(-dQ[0] > afR * QmR) {
-            const float cf = fabsf(afR * QmR / dQ[0]);
+        if(-dm > afR * QmR) {
+            const float cf = fabsf(afR * QmR / dm);
+            dm *= cf;
+            dE *= cf;
 #pragma unroll
-            for(int k = 0; k < S; ++k) dQ[k] *= cf;
+            for(int l = 0; l < D; ++l) dv[l] *= (double)cf;
         }
     }
-    m.dq4[f] = make_float4(dQ[0], dQ[1], dQ[2], dQ[3]);
-    m.dq1[f] = D == 3 ? dQ[4] : 0.f;
-    if(status == SFX_OK && flux[0] != flux[0]) status = SFX_ERR_NAN_FLUX;
+    m.dqm[f] = make_float2(dm, dE);
+#pragma unroll
+    for(int l = 0; l < D; ++l) m.dqv[(size_t)l * FF + f] = dv[l];
+    if(status == SFX_OK && F.m != F.m) status = SFX_ERR_NAN_FLUX;
     if(status != SFX_OK) report_face(m.err, f, status);
 }
 
@@ -904,7 +934,7 @@ __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
     constexpr int S = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= m.n_cells || failed(m.err)) return;
-    const int n = m.n_cells;
+    const int n = m.n_cells, F = m.n_faces;
     double dQ[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) dQ[k] = 0.;
@@ -912,13 +942,12 @@ __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
     for(int j = beg; j < end; ++j) {
         const unsigned e = (unsigned)__ldg(m.idx + j);
         const int f = (int)(e & ~kRightBit);
-        const float4 a = __ldg(m.dq4 + f);
+        const float2 me = __ldg(m.dqm + f);
         double v[S];
-        v[0] = a.x;
-        v[1] = a.y;
-        v[2] = a.z;
-        v[3] = a.w;
-        if(D == 3) v[4] = __ldg(m.dq1 + f);
+        v[0] = me.x;
+#pragma unroll
+        for(int l = 0; l < D; ++l) v[1 + l] = __ldg(m.dqv + (size_t)l * F + f);
+        v[D + 1] = me.y;
         if(e & kRightBit) {
 #pragma unroll
             for(int k = 0; k < S; ++k) dQ[k] -= v[k];
