@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <unordered_map>
 #include <vector>
 
 #include "sfx_internal.h"
@@ -234,6 +235,67 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
             }
         }
     }
+    /* Split pass only: a face across a periodic boundary is listed twice, once
+     * owned by each cell (the reference computes it twice and lets each copy
+     * update only its owner, src/VorFace.cpp:913-955).  The split pass
+     * computes such a pair once: the copy with the higher index is dropped and
+     * its owner takes the negated flux of the twin, so mass and energy leave
+     * one cell exactly as they enter the other. */
+    std::vector<uint8_t> skip;
+    std::vector<int32_t> idx_split;
+    if(ctx->cfg.precision == SFX_PREC_SPLIT) {
+        skip.assign(F, 0);
+        idx_split = idx;
+        auto shcode = [&](int64_t f) {
+            int code = 0;
+            for(int l = 0; l < dim; ++l) {
+                double s = desc->face_right_pos[f * dim + l] -
+                           desc->cell_pos[(int64_t)desc->face_right[f] * dim + l];
+                int c = s > 0.5 ? 1 : (s < -0.5 ? 2 : 0);
+                code = code * 3 + c;
+            }
+            return code;
+        };
+        auto negcode = [&](int code) {
+            int out = 0, mul = 1;
+            for(int l = 0; l < dim; ++l) {
+                int c = code % 3;
+                code /= 3;
+                out += (c == 1 ? 2 : (c == 2 ? 1 : 0)) * mul;
+                mul *= 3;
+            }
+            return out;
+        };
+        auto key = [](int64_t L, int64_t R, int code) {
+            return ((uint64_t)L * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)R << 20) ^ (uint64_t)code;
+        };
+        std::unordered_multimap<uint64_t, int64_t> per;
+        for(int64_t f = 0; f < F; ++f)
+            if(desc->face_kind[f] == SFX_FACE_PERIODIC)
+                per.emplace(key(desc->face_left[f], desc->face_right[f], shcode(f)), f);
+        std::vector<int32_t> twin(F, -1);
+        for(int64_t g = 0; g < F; ++g) {
+            if(desc->face_kind[g] != SFX_FACE_PERIODIC) continue;
+            const int64_t L = desc->face_left[g], R = desc->face_right[g];
+            const int want = negcode(shcode(g));
+            auto rng = per.equal_range(key(R, L, want));
+            for(auto it = rng.first; it != rng.second; ++it) {
+                const int64_t f = it->second;
+                if(desc->face_left[f] == R && desc->face_right[f] == L && shcode(f) == want &&
+                   f < g && twin[f] < 0) {
+                    twin[f] = (int32_t)g;
+                    twin[g] = (int32_t)f;
+                    skip[g] = 1;
+                    break;
+                }
+            }
+        }
+        for(int64_t i = 0; i < n; ++i)
+            for(int64_t j = off[i]; j < off[i + 1]; ++j) {
+                const int32_t g = desc->cell_face_index[j];
+                if(skip[g]) idx_split[j] = (int32_t)((uint32_t)twin[g] | 0x80000000u);
+            }
+    }
     SFX_TRY(cuda_ok(cudaSetDevice(ctx->cfg.device)));
     if(ctx->closing) return SFX_ERR_INVALID;
     sfx_mesh* m = new(std::nothrow) sfx_mesh;
@@ -305,7 +367,8 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     if(!rc) rc = h2d(d.vol, desc->cell_volume, n, s);
     if(!rc) rc = h2d(d.tarea, desc->cell_total_area, n, s);
     if(!rc) rc = h2d(d.off, off, n + 1, s);
-    if(!rc) rc = h2d(d.idx, idx.data(), nnz, s);
+    if(!rc) rc = h2d(d.idx, split ? idx_split.data() : idx.data(), nnz, s);
+    if(!rc && split) rc = h2d(d.fsh, skip.data(), F, s);
     if(!rc) rc = h2d(d.area, desc->face_area, F, s);
     if(!rc) rc = h2d(d.mid, t3.data(), t3.size(), s);
     if(!rc) rc = h2d(d.left, desc->face_left, F, s);

@@ -140,7 +140,10 @@ __global__ void k_prep_faces(sfx_dmesh m) {
     for(int l = 0; l < D; ++l) rn2 += r[l] * r[l];
     const double rn64 = sqrt(rn2);
     for(int l = 0; l < D; ++l) m.an[(size_t)l * F + f] = m.area[f] * (-r[l] / rn64);
-    const float A = (float)m.area[f];
+    /* a periodic copy whose twin carries the flux (marked by the host in
+     * fsh bit 7) is switched off by a zero area */
+    const bool twin_skip = m.fsh[f] & 0x80;
+    const float A = twin_skip ? 0.f : (float)m.area[f];
     const float rn = (float)rn64;
     if(D == 3) {
         m.fg[2 * f] = make_float4(A, (float)c[0], (float)c[1], (float)c[2]);
@@ -892,6 +895,15 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
             F.P = (float)h[D + 1];
             F.E = (float)((e + h[D + 1]) * un);
         }
+    }
+    if(mirror) {
+        /* the reflective Riemann problem has zero normal velocity at the wall:
+         * no mass, energy or advected momentum crosses it, only the pressure
+         * force (the FP32 solver would leave a round-off-sized leak) */
+        F.m = 0.f;
+        F.E = 0.f;
+#pragma unroll
+        for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
     }
     const float dtA = dt * A;
     float dm = dtA * F.m, dE = dtA * F.E;

@@ -149,23 +149,35 @@ def test_reruns_are_bitwise_identical(cuda_ok):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
-def test_errors_match_the_oracle(cuda_ok, oracle):
-    """an absurd time step drives a cell negative: same status and the same
-    first failing index as the reference's exception would name"""
-    mesh, meta, _ = load_case("sod2d_exact")
-    dt = 2.0
+@pytest.mark.parametrize("name", ["sod2d_exact", "sod2d_hllc", "sedov3d_hllc"])
+def test_errors_match_the_oracle(cuda_ok, oracle, name):
+    """a corrupted (NaN) cell state makes the pass fail with the same status
+    (RiemannSolverException -> SFX_ERR_RIEMANN for the exact solver,
+    FluxCalculationException -> SFX_ERR_NAN_FLUX for HLLC) at the same first
+    face as the reference's face loop would throw at"""
+    from shadowfax_b200 import _lib as L
+    mesh, meta, _ = load_case(name)
+    W0 = meta["W0"].copy()
+    W0[mesh.n_cells // 3, 0] = np.nan
+    meta = dict(meta, W0=W0)
     ctx, fp = _pass(mesh, meta)
     p = Params(solver=meta["solver"], gamma=meta["gamma"])
-    Q0 = oracle.init_Q(mesh, p, meta["W0"])
-    og, odQ, ocode, orc, obad = oracle.flux_pass(mesh, p, dt, meta["W0"], Q0)
-    from shadowfax_b200 import _lib as L
-    if orc == 0:
-        _, _, arc, abad = oracle.apply(mesh, p, odQ, meta["W0"], Q0)
-        assert arc == L.SFX_ERR_NEG_STATE
-        with pytest.raises(L.SfxError) as ei:
-            fp.step(dt, 1)
-        assert ei.value.status == arc and ei.value.index == abad
-    else:
-        with pytest.raises(L.SfxError) as ei:
-            fp.step(dt, 1)
-        assert ei.value.status == orc and ei.value.index == obad
+    Q0 = oracle.init_Q(mesh, p, W0)
+    _, _, _, orc, obad = oracle.flux_pass(mesh, p, meta["dt"], W0, Q0)
+    assert orc in (L.SFX_ERR_RIEMANN, L.SFX_ERR_NAN_FLUX)
+    with pytest.raises(L.SfxError) as ei:
+        fp.step(meta["dt"], 1)
+    assert ei.value.status == orc and ei.value.index == obad
+    # a negative mass after the update is reported per cell (UpdateQException)
+    W1 = meta["W0"].copy()
+    ctx2, fp2 = _pass(mesh, dict(meta, W0=W1))
+    Q1 = oracle.init_Q(mesh, p, W1)
+    Q1[:, -1] = 1e-300  # every cell that loses energy goes negative
+    fp2.set_state(W1, Q1)
+    g, dQ, _, rc, _ = oracle.flux_pass(mesh, p, meta["dt"], W1, Q1)
+    assert rc == 0
+    _, _, arc, abad = oracle.apply(mesh, p, dQ, W1, Q1)
+    assert arc == L.SFX_ERR_NEG_STATE
+    with pytest.raises(L.SfxError) as ei:
+        fp2.step(meta["dt"], 1)
+    assert ei.value.status == arc and ei.value.index == abad
