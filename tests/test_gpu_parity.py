@@ -157,6 +157,7 @@ def test_errors_match_the_oracle(cuda_ok, oracle, name):
     face as the reference's face loop would throw at"""
     from shadowfax_b200 import _lib as L
     mesh, meta, _ = load_case(name)
+    W_clean = meta["W0"].copy()
     W0 = meta["W0"].copy()
     W0[mesh.n_cells // 3, 0] = np.nan
     meta = dict(meta, W0=W0)
@@ -169,7 +170,7 @@ def test_errors_match_the_oracle(cuda_ok, oracle, name):
         fp.step(meta["dt"], 1)
     assert ei.value.status == orc and ei.value.index == obad
     # a negative mass after the update is reported per cell (UpdateQException)
-    W1 = meta["W0"].copy()
+    W1 = W_clean
     ctx2, fp2 = _pass(mesh, dict(meta, W0=W1))
     Q1 = oracle.init_Q(mesh, p, W1)
     Q1[:, -1] = 1e-300  # every cell that loses energy goes negative
