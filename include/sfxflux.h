@@ -225,6 +225,51 @@ int sfx_voronoi_export(const sfx_voronoi* v, double* cell_centroid,
                        int32_t* face_kind, double* face_right_pos);
 void sfx_voronoi_free(sfx_voronoi* v);
 
+/* ---- one FP64 flux pass that allocates nothing ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory through the library: applications that hand out all device memory
+ * from their own pools or reserve it up front, or that must not allocate
+ * while requests are in flight.  The caller owns every input and output
+ * array (device pointers, field-major layout below); the gradient scratch is
+ * a fixed file-scope device array of SFX_NOALLOC_MAX_CELLS cells (7.5 MiB on
+ * every GPU that loads the library, held until the process exits), so
+ * meshes with more cells are rejected with SFX_ERR_TOO_LARGE.
+ *
+ * Same arithmetic as sfx_flux_pass in SFX_PREC_FP64: gradients, then the
+ * limited dQ each face gives its left cell.  Runs on the current device and
+ * on `cuda_stream` (NULL = legacy default stream), and waits for it before
+ * returning the status.  The first call on a device looks up the scratch
+ * array's device address; make that first call before any stream capture.
+ * All calls share the scratch array: calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller.
+ * Mesh indices are not range-checked on the device: they must be valid. */
+#define SFX_ERR_TOO_LARGE 13
+#define SFX_NOALLOC_MAX_CELLS 65536
+
+typedef struct sfx_device_mesh {
+    int32_t dim;
+    int32_t n_cells;
+    int32_t n_faces;
+    const double* cell_pos;          /* [dim][n_cells]                      */
+    const double* cell_centroid;     /* [dim][n_cells]                      */
+    const double* cell_volume;       /* [n_cells]                           */
+    const double* cell_total_area;   /* [n_cells]                           */
+    const int32_t* cell_face_offset; /* [n_cells + 1]                       */
+    const int32_t* cell_face_entry;  /* face id, bit 31 set when the cell is
+                                        the face's (real) right cell         */
+    const double* face_area;         /* [n_faces]                           */
+    const double* face_midpoint;     /* [dim][n_faces]                      */
+    const int32_t* face_left;        /* [n_faces]                           */
+    const int32_t* face_right;       /* [n_faces]                           */
+    const int32_t* face_kind;        /* [n_faces] SFX_FACE_*                */
+    const double* face_right_pos;    /* [dim][n_faces]                      */
+} sfx_device_mesh;
+
+/* W, Q: [S][n_cells] device (S = dim + 2); dQ_face: [S][n_faces] device out */
+int sfx_flux_pass_noalloc(const sfx_device_mesh* mesh, const sfx_config* cfg, double dt,
+                          const double* W, const double* Q, double* dQ_face,
+                          void* cuda_stream);
+
 /* library version string */
 const char* sfx_version(void);
 

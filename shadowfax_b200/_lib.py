@@ -62,6 +62,17 @@ class sfx_mesh_desc(C.Structure):
                 ("face_right_pos", _dp), ("face_velocity", _dp)]
 
 
+class sfx_device_mesh(C.Structure):
+    """device-pointer face list of sfx_flux_pass_noalloc (field-major)"""
+    _fields_ = [("dim", C.c_int32), ("n_cells", C.c_int32), ("n_faces", C.c_int32),
+                ("cell_pos", C.c_void_p), ("cell_centroid", C.c_void_p),
+                ("cell_volume", C.c_void_p), ("cell_total_area", C.c_void_p),
+                ("cell_face_offset", C.c_void_p), ("cell_face_entry", C.c_void_p),
+                ("face_area", C.c_void_p), ("face_midpoint", C.c_void_p),
+                ("face_left", C.c_void_p), ("face_right", C.c_void_p),
+                ("face_kind", C.c_void_p), ("face_right_pos", C.c_void_p)]
+
+
 class sfx_stats(C.Structure):
     _fields_ = [("status", C.c_int32), ("bad_face", C.c_int32), ("bad_cell", C.c_int32),
                 ("steps_done", C.c_int32), ("totals", C.c_double * 5)]
@@ -94,6 +105,9 @@ PROTOTYPES = {
     "sfx_voronoi_export": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip,
                                      _ip, _dp]),
     "sfx_voronoi_free": (None, [C.c_void_p]),
+    "sfx_flux_pass_noalloc": (C.c_int, [C.POINTER(sfx_device_mesh), C.POINTER(sfx_config),
+                                        C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
 }
 
 

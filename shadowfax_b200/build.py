@@ -35,6 +35,7 @@ UNITS = {
     "sfx_fp64.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "sfx_split.cu": ["-fmad=true"],
     "sfx_api.cu": [],
+    "sfx_noalloc.cu": [],
     "sfx_voronoi.cpp": [],
 }
 
