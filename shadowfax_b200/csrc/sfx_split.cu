@@ -221,13 +221,50 @@ struct SFlux {
 };
 
 /* ------------------------------ gradients ------------------------------ */
+/* Lanes per cell: a group of LPC lanes of one warp shares a cell, each lane
+ * takes every LPC-th of the cell's faces, and the group combines its partial
+ * sums / maxima / minima with shuffles.  All loads of a group are independent,
+ * so a warp keeps 32 face gathers in flight instead of one. */
+template <int D>
+struct Lanes {
+    static constexpr int value = D == 3 ? 16 : 8;
+};
+
+template <int LPC>
+__device__ __forceinline__ float seg_sum(float v) {
+#pragma unroll
+    for(int o = LPC / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, LPC);
+    return v;
+}
+template <int LPC>
+__device__ __forceinline__ float seg_max(float v) {
+#pragma unroll
+    for(int o = LPC / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o, LPC));
+    return v;
+}
+template <int LPC>
+__device__ __forceinline__ float seg_min(float v) {
+#pragma unroll
+    for(int o = LPC / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o, LPC));
+    return v;
+}
+template <int LPC>
+__device__ __forceinline__ double seg_sum(double v) {
+#pragma unroll
+    for(int o = LPC / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, LPC);
+    return v;
+}
+
 template <int D>
 __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
-    constexpr int S = D + 2, G = (D * S + 3) / 4;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= m.n_cells || failed(m.err)) return;
-    const Cell<D> own = load_cell<D>(m.cw, i);
-    const float4 xv = __ldg(m.cx + i);
+    constexpr int S = D + 2, G = (D * S + 3) / 4, LPC = Lanes<D>::value;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / LPC, lane = t % LPC;
+    /* whole warps stay alive for the shuffles; lanes past the end idle */
+    const bool live = i < m.n_cells && !failed(m.err);
+    const int ic = live ? i : 0;
+    const Cell<D> own = load_cell<D>(m.cw, ic);
+    const float4 xv = __ldg(m.cx + ic);
     const float xmc[3] = {xv.x, xv.y, xv.z};
     float W[S], Wmax[S], Wmin[S], delta[D][S];
 #pragma unroll
@@ -238,8 +275,9 @@ __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
 #pragma unroll
         for(int l = 0; l < D; ++l) delta[l][k] = 0.f;
     }
-    const int beg = __ldg(m.off + i), end = __ldg(m.off + i + 1);
-    for(int j = beg; j < end; ++j) {
+    const int beg = live ? __ldg(m.off + ic) : 0;
+    const int end = live ? __ldg(m.off + ic + 1) : 0;
+    for(int j = beg + lane; j < end; j += LPC) {
         const unsigned e = (unsigned)__ldg(m.idx + j);
         const int f = (int)(e & ~kRightBit);
         const bool right = e & kRightBit;
@@ -282,13 +320,16 @@ __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
     }
     const float iv = 1.f / xv.w;
 #pragma unroll
-    for(int l = 0; l < D; ++l)
+    for(int k = 0; k < S; ++k) {
 #pragma unroll
-        for(int k = 0; k < S; ++k) delta[l][k] *= iv;
+        for(int l = 0; l < D; ++l) delta[l][k] = seg_sum<LPC>(delta[l][k]) * iv;
+        Wmax[k] = seg_max<LPC>(Wmax[k]);
+        Wmin[k] = seg_min<LPC>(Wmin[k]);
+    }
     float alpha[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) alpha[k] = 1.f;
-    for(int j = beg; j < end; ++j) {
+    for(int j = beg + lane; j < end; j += LPC) {
         const unsigned e = (unsigned)__ldg(m.idx + j);
         const int f = (int)(e & ~kRightBit);
         const bool right = e & kRightBit;
@@ -312,6 +353,10 @@ __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
             alpha[k] = fminf(alpha[k], mx);
         }
     }
+#pragma unroll
+    for(int k = 0; k < S; ++k) alpha[k] = seg_min<LPC>(alpha[k]);
+    if(!live) return;
+    /* lane q < G writes float4 q of the gradient record */
     float out[4 * G];
 #pragma unroll
     for(int l = 0; l < D; ++l)
@@ -321,8 +366,9 @@ __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
     for(int q = D * S; q < 4 * G; ++q) out[q] = 0.f;
 #pragma unroll
     for(int q = 0; q < G; ++q)
-        m.cg[(size_t)G * i + q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2],
-                                              out[4 * q + 3]);
+        if(lane == q)
+            m.cg[(size_t)G * i + q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2],
+                                                  out[4 * q + 3]);
 }
 
 /* ----------------------------- face physics ----------------------------- */
@@ -776,7 +822,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
 }
 
 template <int D, int SOLVER>
-__global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
+__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
+        k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
     constexpr int S = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if(f >= m.n_faces || failed(m.err)) return;
@@ -943,15 +990,19 @@ __global__ void __launch_bounds__(256) k_sfaces(sfx_dmesh m, sfx_solver_params s
 /* ------------------------------- update ------------------------------- */
 template <int D>
 __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
-    constexpr int S = D + 2;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= m.n_cells || failed(m.err)) return;
+    constexpr int S = D + 2, LPC = Lanes<D>::value;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / LPC, lane = t % LPC;
+    const bool live = i < m.n_cells && !failed(m.err);
     const int n = m.n_cells, F = m.n_faces;
     double dQ[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) dQ[k] = 0.;
-    const int beg = __ldg(m.off + i), end = __ldg(m.off + i + 1);
-    for(int j = beg; j < end; ++j) {
+    const int beg = live ? __ldg(m.off + i) : 0;
+    const int end = live ? __ldg(m.off + i + 1) : 0;
+    /* each lane sums every LPC-th face in FP64; the group then adds the lanes'
+     * partial sums in a fixed tree, so reruns are bitwise identical */
+    for(int j = beg + lane; j < end; j += LPC) {
         const unsigned e = (unsigned)__ldg(m.idx + j);
         const int f = (int)(e & ~kRightBit);
         const float2 me = __ldg(m.dqm + f);
@@ -968,6 +1019,9 @@ __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
             for(int k = 0; k < S; ++k) dQ[k] += v[k];
         }
     }
+#pragma unroll
+    for(int k = 0; k < S; ++k) dQ[k] = seg_sum<LPC>(dQ[k]);
+    if(!live || lane != 0) return;
     double Q[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) Q[k] = m.Q[(size_t)k * n + i] - dQ[k];
@@ -1062,9 +1116,9 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
 int sfx_split_gradients(const sfx_dmesh* m, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if(m->dim == 3)
-        k_sgrad<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+        k_sgrad<3><<<grid_for((long long)m->n_cells * Lanes<3>::value, 256), 256, 0, s>>>(*m);
     else
-        k_sgrad<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
+        k_sgrad<2><<<grid_for((long long)m->n_cells * Lanes<2>::value, 256), 256, 0, s>>>(*m);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1090,8 +1144,10 @@ int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, 
 int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if(m->dim == 3)
-        k_sapply<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m, sp->gamma);
+        k_sapply<3><<<grid_for((long long)m->n_cells * Lanes<3>::value, 256), 256, 0, s>>>(
+                *m, sp->gamma);
     else
-        k_sapply<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m, sp->gamma);
+        k_sapply<2><<<grid_for((long long)m->n_cells * Lanes<2>::value, 256), 256, 0, s>>>(
+                *m, sp->gamma);
     return cuda_status(cudaGetLastError());
 }
