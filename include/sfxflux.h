@@ -211,6 +211,28 @@ int sfx_riemann_eval(sfx_ctx* ctx, int32_t n, const double* WL, const double* WR
 /* conserved totals sum_i Q_i (m, p[dim], e), deterministic FP64 */
 int sfx_mesh_totals(sfx_mesh* mesh, double* totals);
 
+/* ---- launch groups: many meshes per launch (SFX_PREC_SPLIT) ----
+ * A group runs one step of every member mesh with one launch per phase
+ * (gradients, faces, update): block b of a launch works on the mesh whose
+ * block range contains b.  Each mesh keeps its own time step, state and error
+ * record (a failing mesh stops only itself).  The member meshes must belong
+ * to `ctx` and stay alive while the group exists; their states are set and
+ * read with the per-mesh sfx_state_* calls.  With use_graph != 0 the nsteps
+ * steps are captured once in a CUDA graph and replayed on later calls with
+ * the same nsteps.  mesh_status (may be NULL) receives one status per mesh. */
+typedef struct sfx_group sfx_group;
+int sfx_group_create(sfx_ctx* ctx, int32_t n_meshes, sfx_mesh* const* meshes,
+                     const double* dt, sfx_group** out);
+int sfx_group_set_dt(sfx_group* group, const double* dt);
+int sfx_group_step(sfx_group* group, int32_t nsteps, int32_t use_graph,
+                   int32_t* mesh_status);
+/* time each lanes-per-cell variant (4, 8, 16) of the gradient kernel on this
+ * group (reads the states, changes none) and keep the fastest for the
+ * gradient and update kernels; *lanes receives it */
+int sfx_group_tune(sfx_group* group, int32_t reps, int32_t* lanes);
+int sfx_group_set_lanes(sfx_group* group, int32_t lanes);
+int sfx_group_free(sfx_group* group);
+
 /* ---- host Voronoi face-list builder (inputs for the pass) ---- */
 typedef struct sfx_voronoi sfx_voronoi;
 int sfx_voronoi_build(int dim, int64_t n, const double* pos, int periodic,

@@ -36,6 +36,7 @@ UNITS = {
     "sfx_split.cu": ["-fmad=true"],
     "sfx_api.cu": [],
     "sfx_noalloc.cu": [],
+    "sfx_group.cu": [],
     "sfx_voronoi.cpp": [],
 }
 

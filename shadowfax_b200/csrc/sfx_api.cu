@@ -122,6 +122,22 @@ int reset_err(sfx_mesh* m) {
 
 }  // namespace
 
+sfx_dmesh* sfx_mesh_dev(sfx_mesh* m) {
+    return &m->d;
+}
+sfx_ctx* sfx_mesh_ctx(sfx_mesh* m) {
+    return m->ctx;
+}
+void* sfx_ctx_stream(sfx_ctx* c) {
+    return (void*)c->stream;
+}
+const sfx_config* sfx_ctx_config(sfx_ctx* c) {
+    return &c->cfg;
+}
+const sfx_solver_params* sfx_ctx_params(sfx_ctx* c) {
+    return &c->sp;
+}
+
 extern "C" {
 
 const char* sfx_version(void) {

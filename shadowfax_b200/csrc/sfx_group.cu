@@ -1,0 +1,229 @@
+/*
+ * Launch groups: many independent meshes advanced with one launch per phase.
+ *
+ * The group keeps, in device memory, a table with each member mesh's device
+ * view and time step, and per phase the prefix sum of thread blocks over the
+ * members.  A step is three launches (gradients, faces, update) for all
+ * members together, optionally captured in a CUDA graph, so small meshes share
+ * the GPU instead of each paying its own launch latency and leaving most SMs
+ * idle.  The per-mesh error records stay separate: a failing member stops
+ * only itself, and its status is reported per mesh.
+ */
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "sfx_internal.h"
+
+struct sfx_group {
+    sfx_ctx* ctx = nullptr;
+    std::vector<sfx_mesh*> meshes;
+    std::vector<sfx_group_entry> host_tab;
+    sfx_group_dev dev{};
+    sfx_dev_error* d_err_out = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = -1;
+};
+
+namespace {
+
+int cuda_ok(cudaError_t e) {
+    if(e == cudaSuccess) return SFX_OK;
+    cudaGetLastError();
+    return SFX_ERR_CUDA;
+}
+
+void drop_graph(sfx_group* g) {
+    if(g->graph) cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+    g->graph_steps = -1;
+}
+
+/* block prefix sums for the current lanes-per-cell and upload of the table */
+int upload_layout(sfx_group* g) {
+    const int nm = (int)g->meshes.size();
+    std::vector<int32_t> pre(3 * (nm + 1), 0);
+    for(int mi = 0; mi < nm; ++mi) {
+        const sfx_dmesh& d = g->host_tab[mi].m;
+        int32_t b[3];
+        sfx_split_blocks(d.dim, g->dev.lanes, d.n_cells, d.n_faces, b);
+        for(int p = 0; p < 3; ++p) {
+            const long long next = (long long)pre[p * (nm + 1) + mi] + b[p];
+            if(next > 0x7fffffffLL) return SFX_ERR_TOO_LARGE;
+            pre[p * (nm + 1) + mi + 1] = (int32_t)next;
+        }
+    }
+    for(int p = 0; p < 3; ++p) g->dev.blocks[p] = pre[p * (nm + 1) + nm];
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    int rc = cuda_ok(cudaMemcpyAsync(g->dev.pre, pre.data(), sizeof(int32_t) * pre.size(),
+                                     cudaMemcpyHostToDevice, s));
+    if(!rc)
+        rc = cuda_ok(cudaMemcpyAsync(g->dev.tab, g->host_tab.data(),
+                                     sizeof(sfx_group_entry) * nm, cudaMemcpyHostToDevice, s));
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    drop_graph(g);
+    return rc;
+}
+
+int run_steps(sfx_group* g, int nsteps, cudaStream_t s) {
+    const sfx_solver_params* sp = sfx_ctx_params(g->ctx);
+    for(int t = 0; t < nsteps; ++t)
+        for(int ph = 0; ph < 3; ++ph) {
+            int rc = sfx_split_group_phase(&g->dev, ph, sp, s);
+            if(rc) return rc;
+        }
+    return SFX_OK;
+}
+
+}  // namespace
+
+extern "C" int sfx_group_create(sfx_ctx* ctx, int32_t n, sfx_mesh* const* meshes,
+                                const double* dt, sfx_group** out) {
+    if(!ctx || !meshes || !dt || !out || n <= 0) return SFX_ERR_INVALID;
+    *out = nullptr;
+    const sfx_config* cfg = sfx_ctx_config(ctx);
+    if(cfg->precision != SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    for(int i = 0; i < n; ++i) {
+        if(!meshes[i] || sfx_mesh_ctx(meshes[i]) != ctx || !(dt[i] > 0.)) return SFX_ERR_INVALID;
+    }
+    sfx_group* g = new(std::nothrow) sfx_group;
+    if(!g) return SFX_ERR_NOMEM;
+    g->ctx = ctx;
+    g->meshes.assign(meshes, meshes + n);
+    g->host_tab.resize(n);
+    for(int i = 0; i < n; ++i) {
+        std::memset(&g->host_tab[i], 0, sizeof(sfx_group_entry));
+        g->host_tab[i].m = *sfx_mesh_dev(meshes[i]);
+        g->host_tab[i].dt = (float)dt[i];
+    }
+    g->dev.n_meshes = n;
+    g->dev.dim = cfg->dim;
+    g->dev.lanes = cfg->dim == 3 ? 16 : 8;
+    int rc = cuda_ok(cudaSetDevice(cfg->device));
+    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.tab, sizeof(sfx_group_entry) * n));
+    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.pre, sizeof(int32_t) * 3 * (n + 1)));
+    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->d_err_out, sizeof(sfx_dev_error) * n));
+    if(!rc) rc = upload_layout(g);
+    if(rc) {
+        sfx_group_free(g);
+        return rc;
+    }
+    *out = g;
+    return SFX_OK;
+}
+
+extern "C" int sfx_group_set_dt(sfx_group* g, const double* dt) {
+    if(!g || !dt) return SFX_ERR_INVALID;
+    for(size_t i = 0; i < g->meshes.size(); ++i) {
+        if(!(dt[i] > 0.)) return SFX_ERR_INVALID;
+        g->host_tab[i].dt = (float)dt[i];
+    }
+    return upload_layout(g);
+}
+
+extern "C" int sfx_group_set_lanes(sfx_group* g, int32_t lanes) {
+    if(!g || (lanes != 4 && lanes != 8 && lanes != 16)) return SFX_ERR_INVALID;
+    g->dev.lanes = lanes;
+    return upload_layout(g);
+}
+
+extern "C" int sfx_group_step(sfx_group* g, int32_t nsteps, int32_t use_graph,
+                              int32_t* mesh_status) {
+    if(!g || nsteps < 0) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    int rc = sfx_split_group_reset(&g->dev, s);
+    if(rc) return rc;
+    if(use_graph && nsteps > 0) {
+        if(!g->graph || g->graph_steps != nsteps) {
+            drop_graph(g);
+            cudaGraph_t graph = nullptr;
+            rc = cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            if(rc) return rc;
+            const int rr = run_steps(g, nsteps, s);
+            rc = cuda_ok(cudaStreamEndCapture(s, &graph));
+            if(!rc && rr) rc = rr;
+            if(!rc) rc = cuda_ok(cudaGraphInstantiate(&g->graph, graph, 0));
+            if(graph) cudaGraphDestroy(graph);
+            if(rc) {
+                drop_graph(g);
+                return rc;
+            }
+            g->graph_steps = nsteps;
+        }
+        rc = cuda_ok(cudaGraphLaunch(g->graph, s));
+    } else {
+        rc = run_steps(g, nsteps, s);
+    }
+    if(rc) return rc;
+    if(!mesh_status) return SFX_OK;
+    const int nm = g->dev.n_meshes;
+    std::vector<sfx_dev_error> e(nm);
+    rc = sfx_split_group_collect(&g->dev, g->d_err_out, s);
+    if(!rc)
+        rc = cuda_ok(cudaMemcpyAsync(e.data(), g->d_err_out, sizeof(sfx_dev_error) * nm,
+                                     cudaMemcpyDeviceToHost, s));
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    if(rc) return rc;
+    int first = SFX_OK;
+    for(int i = 0; i < nm; ++i) {
+        int st = SFX_OK;
+        if(e[i].face_key != ~0ull)
+            st = (int)(e[i].face_key & 0xff);
+        else if(e[i].cell_key != ~0ull)
+            st = (int)(e[i].cell_key & 0xff);
+        mesh_status[i] = st;
+        if(st && !first) first = st;
+    }
+    return first;
+}
+
+extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
+    if(!g || reps <= 0) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    const sfx_solver_params* sp = sfx_ctx_params(g->ctx);
+    cudaEvent_t e0, e1;
+    if(cudaEventCreate(&e0) != cudaSuccess) return SFX_ERR_CUDA;
+    if(cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return SFX_ERR_CUDA;
+    }
+    const int cand[3] = {4, 8, 16};
+    int best = g->dev.lanes;
+    float best_ms = 1e30f;
+    int rc = SFX_OK;
+    for(int c = 0; c < 3 && !rc; ++c) {
+        rc = sfx_group_set_lanes(g, cand[c]);
+        if(rc) break;
+        /* timed on the gradient kernel, which only reads the states (the
+         * update kernel shares the setting); one untimed launch, then reps */
+        for(int r = 0; r <= reps && !rc; ++r) {
+            if(r == 1) cudaEventRecord(e0, s);
+            rc = sfx_split_group_phase(&g->dev, 0, sp, s);
+        }
+        cudaEventRecord(e1, s);
+        if(!rc) rc = cuda_ok(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        if(!rc) rc = cuda_ok(cudaEventElapsedTime(&ms, e0, e1));
+        if(!rc && ms < best_ms) {
+            best_ms = ms;
+            best = cand[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int r2 = sfx_group_set_lanes(g, best);
+    if(lanes_out) *lanes_out = best;
+    return rc ? rc : r2;
+}
+
+extern "C" int sfx_group_free(sfx_group* g) {
+    if(!g) return SFX_ERR_INVALID;
+    drop_graph(g);
+    if(g->dev.tab) cudaFree(g->dev.tab);
+    if(g->dev.pre) cudaFree(g->dev.pre);
+    if(g->d_err_out) cudaFree(g->d_err_out);
+    delete g;
+    return SFX_OK;
+}

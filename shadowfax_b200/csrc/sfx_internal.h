@@ -76,6 +76,24 @@ struct sfx_dmesh {
     double* dqv;
 };
 
+/* one mesh of a launch group (device table entry) */
+struct sfx_group_entry {
+    sfx_dmesh m;
+    float dt;
+    int32_t pad;
+};
+
+/* device view of a launch group: table of meshes and, per phase, the prefix
+ * sum of blocks over the meshes (3 arrays of n_meshes + 1) */
+struct sfx_group_dev {
+    sfx_group_entry* tab;
+    int32_t* pre;
+    int32_t n_meshes;
+    int32_t dim;
+    int32_t lanes; /* lanes per cell of the gradient and update kernels */
+    int32_t blocks[3];
+};
+
 struct sfx_solver_params {
     int32_t kind;
     double gamma, tol, cutoff;
@@ -110,5 +128,18 @@ int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* strea
 int sfx_split_export_W(const sfx_dmesh* m, void* stream);
 /* per-face dQ (FP32) widened into dQf (FP64 SoA), for parity checks */
 int sfx_split_export_dQ(const sfx_dmesh* m, void* stream);
+/* accessors of the C-ABI handles (sfx_api.cu) */
+sfx_dmesh* sfx_mesh_dev(sfx_mesh* m);
+sfx_ctx* sfx_mesh_ctx(sfx_mesh* m);
+void* sfx_ctx_stream(sfx_ctx* c);
+const sfx_config* sfx_ctx_config(sfx_ctx* c);
+const sfx_solver_params* sfx_ctx_params(sfx_ctx* c);
+
+/* grouped launches (sfx_split.cu) */
+int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);
+int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
+                          void* stream);
+int sfx_split_group_reset(const sfx_group_dev* g, void* stream);
+int sfx_split_group_collect(const sfx_group_dev* g, sfx_dev_error* d_out, void* stream);
 
 #endif

@@ -255,10 +255,9 @@ __device__ __forceinline__ double seg_sum(double v) {
     return v;
 }
 
-template <int D>
-__global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
-    constexpr int S = D + 2, G = (D * S + 3) / 4, LPC = Lanes<D>::value;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+template <int D, int LPC>
+__device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
+    constexpr int S = D + 2, G = (D * S + 3) / 4;
     const int i = t / LPC, lane = t % LPC;
     /* whole warps stay alive for the shuffles; lanes past the end idle */
     const bool live = i < m.n_cells && !failed(m.err);
@@ -366,9 +365,14 @@ __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
     for(int q = D * S; q < 4 * G; ++q) out[q] = 0.f;
 #pragma unroll
     for(int q = 0; q < G; ++q)
-        if(lane == q)
+        if(lane == q % LPC)
             m.cg[(size_t)G * i + q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2],
                                                   out[4 * q + 3]);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
+    sgrad_body<D, Lanes<D>::value>(m, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ----------------------------- face physics ----------------------------- */
@@ -822,10 +826,9 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
 }
 
 template <int D, int SOLVER>
-__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
-        k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
+__device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
+                                            const float dt, const int f) {
     constexpr int S = D + 2;
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if(f >= m.n_faces || failed(m.err)) return;
     float A, c[D], r[D], rn;
     geom<D>(m.fg, f, A, c, r, rn);
@@ -987,11 +990,17 @@ __global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
     if(status != SFX_OK) report_face(m.err, f, status);
 }
 
+template <int D, int SOLVER>
+__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
+        k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
+    sfaces_body<D, SOLVER>(m, sp, dt, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 /* ------------------------------- update ------------------------------- */
-template <int D>
-__global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
-    constexpr int S = D + 2, LPC = Lanes<D>::value;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+template <int D, int LPC>
+__device__ __forceinline__ void sapply_body(const sfx_dmesh& m, const double gamma,
+                                            const int t) {
+    constexpr int S = D + 2;
     const int i = t / LPC, lane = t % LPC;
     const bool live = i < m.n_cells && !failed(m.err);
     const int n = m.n_cells, F = m.n_faces;
@@ -1059,6 +1068,93 @@ __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
 #pragma unroll
     for(int k = 0; k < S; ++k) Wf[k] = (float)W[k];
     store_cell<D>(m.cw, i, Wf, (float)Q[0], (float)m.tarea[i]);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
+    sapply_body<D, Lanes<D>::value>(m, gamma, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+/* ------------------------- grouped (batched) launches -------------------------
+ * One launch per phase covers every mesh of a group: block b works on the
+ * mesh whose block range [pre[mi], pre[mi+1]) contains b, with the same
+ * per-mesh code as the single-mesh kernels. */
+__device__ __forceinline__ int group_mesh_of_block(const int* __restrict__ pre, int nm) {
+    __shared__ int s_mesh;
+    if(threadIdx.x == 0) {
+        const int b = blockIdx.x;
+        int lo = 0, hi = nm; /* largest mi with pre[mi] <= b */
+        while(hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if(__ldg(pre + mid) <= b)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        s_mesh = lo;
+    }
+    __syncthreads();
+    return s_mesh;
+}
+
+template <int D, int LPC>
+__global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
+                                                     int nm) {
+    const int mi = group_mesh_of_block(pre, nm);
+    sgrad_body<D, LPC>(tab[mi].m, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+}
+
+template <int D, int SOLVER>
+__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
+        k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
+                       sfx_solver_params sp) {
+    const int mi = group_mesh_of_block(pre, nm);
+    sfaces_body<D, SOLVER>(tab[mi].m, sp, tab[mi].dt,
+                           (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+}
+
+template <int D, int LPC>
+__global__ void __launch_bounds__(256) k_group_sapply(const sfx_group_entry* tab, const int* pre,
+                                                      int nm, double gamma) {
+    const int mi = group_mesh_of_block(pre, nm);
+    sapply_body<D, LPC>(tab[mi].m, gamma, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+}
+
+__global__ void k_group_reset_err(const sfx_group_entry* tab, int nm) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if(mi >= nm) return;
+    tab[mi].m.err->face_key = ~0ull;
+    tab[mi].m.err->cell_key = ~0ull;
+}
+
+__global__ void k_group_collect_err(const sfx_group_entry* tab, int nm, sfx_dev_error* out) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if(mi >= nm) return;
+    out[mi] = *tab[mi].m.err;
+}
+
+template <int D, int LPC>
+int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
+                cudaStream_t s) {
+    const int nm = g->n_meshes;
+    if(phase == 0) {
+        if(g->blocks[0])
+            k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm);
+    } else if(phase == 1) {
+        if(g->blocks[1]) {
+            if(sp->kind == SFX_SOLVER_EXACT)
+                k_group_sfaces<D, SFX_SOLVER_EXACT><<<g->blocks[1], 256, 0, s>>>(
+                        g->tab, g->pre + (nm + 1), nm, *sp);
+            else
+                k_group_sfaces<D, SFX_SOLVER_HLLC><<<g->blocks[1], 256, 0, s>>>(
+                        g->tab, g->pre + (nm + 1), nm, *sp);
+        }
+    } else {
+        if(g->blocks[2])
+            k_group_sapply<D, LPC><<<g->blocks[2], 256, 0, s>>>(g->tab, g->pre + 2 * (nm + 1),
+                                                                 nm, sp->gamma);
+    }
+    return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
 }
 
 inline int grid_for(long long n, int b) {
@@ -1149,5 +1245,44 @@ int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* strea
     else
         k_sapply<2><<<grid_for((long long)m->n_cells * Lanes<2>::value, 256), 256, 0, s>>>(
                 *m, sp->gamma);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {
+    (void)dim;
+    out[0] = grid_for((long long)n_cells * lanes, 256);
+    out[1] = grid_for(n_faces, 256);
+    out[2] = out[0];
+    return SFX_OK;
+}
+
+int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
+                          void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if(g->dim == 3) {
+        switch(g->lanes) {
+        case 4: return group_phase<3, 4>(g, phase, sp, s);
+        case 8: return group_phase<3, 8>(g, phase, sp, s);
+        case 16: return group_phase<3, 16>(g, phase, sp, s);
+        default: return SFX_ERR_INVALID;
+        }
+    }
+    switch(g->lanes) {
+    case 4: return group_phase<2, 4>(g, phase, sp, s);
+    case 8: return group_phase<2, 8>(g, phase, sp, s);
+    case 16: return group_phase<2, 16>(g, phase, sp, s);
+    default: return SFX_ERR_INVALID;
+    }
+}
+
+int sfx_split_group_reset(const sfx_group_dev* g, void* stream) {
+    k_group_reset_err<<<grid_for(g->n_meshes, 128), 128, 0, (cudaStream_t)stream>>>(g->tab,
+                                                                                  g->n_meshes);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_split_group_collect(const sfx_group_dev* g, sfx_dev_error* d_out, void* stream) {
+    k_group_collect_err<<<grid_for(g->n_meshes, 128), 128, 0, (cudaStream_t)stream>>>(
+            g->tab, g->n_meshes, d_out);
     return cuda_status(cudaGetLastError());
 }

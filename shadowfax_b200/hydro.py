@@ -208,3 +208,52 @@ class FluxPass:
         out = np.zeros(5)
         L.check(L.lib().sfx_mesh_totals(self.h, L.dptr(out)), "sfx_mesh_totals")
         return out[: self.S]
+
+
+class Group:
+    """Many meshes of one split-precision context advanced together: one
+    launch per phase for all members (sfx_group_*)."""
+
+    def __init__(self, ctx: Context, members: list[FluxPass], dts):
+        self.ctx = ctx
+        self.members = list(members)
+        n = len(self.members)
+        arr = (C.c_void_p * n)(*[m.h.value for m in self.members])
+        dt = np.ascontiguousarray(dts, np.float64)
+        h = C.c_void_p()
+        L.check(L.lib().sfx_group_create(ctx.h, n, arr, L.dptr(dt), C.byref(h)),
+                "sfx_group_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            L.lib().sfx_group_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_dt(self, dts):
+        dt = np.ascontiguousarray(dts, np.float64)
+        L.check(L.lib().sfx_group_set_dt(self.h, L.dptr(dt)), "sfx_group_set_dt")
+
+    def tune(self, reps: int = 3) -> int:
+        lanes = C.c_int32(0)
+        L.check(L.lib().sfx_group_tune(self.h, reps, C.byref(lanes)), "sfx_group_tune")
+        return lanes.value
+
+    def set_lanes(self, lanes: int):
+        L.check(L.lib().sfx_group_set_lanes(self.h, lanes), "sfx_group_set_lanes")
+
+    def step(self, nsteps: int = 1, graph: bool = True, status: bool = True):
+        """nsteps for every member; returns the per-member status array"""
+        st = np.zeros(len(self.members), np.int32) if status else None
+        rc = L.lib().sfx_group_step(self.h, nsteps, int(graph), L.iptr(st) if status else None)
+        if rc and not status:
+            raise L.SfxError(rc, "sfx_group_step")
+        if rc and st is not None and not np.any(st):
+            raise L.SfxError(rc, "sfx_group_step")
+        return st

@@ -106,3 +106,18 @@ def step_state2d(n: int, seed: int, solver: str = "HLLC", nsteps: int = 20) -> P
 def batch_sizes(count: int = 1024, lo: int = 1_000, hi: int = 100_000, seed: int = 4) -> np.ndarray:
     rng = np.random.Generator(np.random.PCG64(seed))
     return np.exp(rng.uniform(math.log(lo), math.log(hi), count)).astype(np.int64)
+
+
+def batch2d(count: int = 1024, seed: int = 4, solver: str = "HLLC", nsteps: int = 20,
+            workers: int = 0) -> list[Problem]:
+    """config 4: `count` independent 2D step-state meshes with generator
+    counts log-uniform in [1e3, 1e5]; meshes are tessellated concurrently
+    (the builder releases the interpreter lock)"""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    sizes = batch_sizes(count, seed=seed)
+    workers = workers or max(1, min(8, (os.cpu_count() or 4) // 2))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        futs = [ex.submit(step_state2d, int(n), seed * 100_000 + j, solver, nsteps)
+                for j, n in enumerate(sizes)]
+        return [f.result() for f in futs]

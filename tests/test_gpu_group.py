@@ -1,0 +1,87 @@
+"""Launch groups (many meshes per launch): each member's result equals the
+same mesh advanced alone, a failing member stops only itself."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(dim, solver, sizes, seed=40):
+    from shadowfax_b200 import workloads as wl
+    out = []
+    for j, n in enumerate(sizes):
+        if dim == 2:
+            pr = wl.step_state2d(int(n), seed + j, solver=solver, nsteps=5)
+        else:
+            pr = wl.sedov3d(n=int(n), seed=seed + j, solver=solver, nsteps=5)
+        out.append(pr)
+    return out
+
+
+def _alone(pr):
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    ctx = Context(pr.mesh.dim, RiemannSolverFactory.generate(pr.solver, pr.gamma), 1)
+    fp = FluxPass(ctx, pr.mesh)
+    fp.set_primitive(pr.W0)
+    fp.step(pr.dt, pr.nsteps)
+    return fp.state()
+
+
+@pytest.mark.parametrize("dim,solver", [(2, "HLLC"), (2, "Exact"), (3, "HLLC")])
+@pytest.mark.parametrize("graph", [False, True])
+def test_group_members_match_alone(cuda_ok, dim, solver, graph):
+    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
+    sizes = [300, 1700, 800, 4000, 150] if dim == 2 else [500, 2500, 1200]
+    probs = _problems(dim, solver, sizes)
+    ctx = Context(dim, RiemannSolverFactory.generate(solver), 1)
+    members = []
+    for pr in probs:
+        fp = FluxPass(ctx, pr.mesh)
+        fp.set_primitive(pr.W0)
+        members.append(fp)
+    g = Group(ctx, members, [pr.dt for pr in probs])
+    st = g.step(probs[0].nsteps, graph=graph)
+    assert np.all(st == 0)
+    for pr, fp in zip(probs, members):
+        W, Q = fp.state()
+        Wa, Qa = _alone(pr)
+        np.testing.assert_array_equal(Q, Qa)
+        np.testing.assert_array_equal(W, Wa)
+
+
+def test_failing_member_stops_only_itself(cuda_ok):
+    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
+    probs = _problems(2, "HLLC", [400, 900, 600])
+    ctx = Context(2, RiemannSolverFactory.generate("HLLC"), 1)
+    members = []
+    for j, pr in enumerate(probs):
+        fp = FluxPass(ctx, pr.mesh)
+        W0 = pr.W0.copy()
+        if j == 1:
+            W0[7, 0] = np.nan
+        fp.set_primitive(W0)
+        members.append(fp)
+    g = Group(ctx, members, [pr.dt for pr in probs])
+    st = g.step(probs[0].nsteps, graph=True)
+    assert st[1] != 0 and st[0] == 0 and st[2] == 0
+    for j in (0, 2):
+        np.testing.assert_array_equal(members[j].state()[1], _alone(probs[j])[1])
+
+
+def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
+    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
+    probs = _problems(3, "HLLC", [3000, 1500])
+    ctx = Context(3, RiemannSolverFactory.generate("HLLC"), 1)
+    members = [FluxPass(ctx, pr.mesh) for pr in probs]
+    for fp, pr in zip(members, probs):
+        fp.set_primitive(pr.W0)
+    g = Group(ctx, members, [pr.dt for pr in probs])
+    lanes = g.tune(2)
+    assert lanes in (4, 8, 16)
+    st = g.step(probs[0].nsteps)
+    assert np.all(st == 0)
+    for pr, fp in zip(probs, members):
+        Q = fp.state()[1]
+        Qa = _alone(pr)[1]
+        err = np.abs(Q - Qa).sum(0) / np.abs(Qa).sum(0)
+        assert np.all(err[[0, -1]] <= 1e-6)
