@@ -211,6 +211,11 @@ int sfx_riemann_eval(sfx_ctx* ctx, int32_t n, const double* WL, const double* WR
 /* conserved totals sum_i Q_i (m, p[dim], e), deterministic FP64 */
 int sfx_mesh_totals(sfx_mesh* mesh, double* totals);
 
+/* split pass: lanes of a warp that share one cell in the gradient and update
+ * kernels (1, 2, 4, 8 or 16; default 4).  Changes the summation tree of the
+ * per-cell sums, not the algorithm. */
+int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
+
 /* ---- launch groups: many meshes per launch (SFX_PREC_SPLIT) ----
  * A group runs one step of every member mesh with one launch per phase
  * (gradients, faces, update): block b of a launch works on the mesh whose

@@ -105,6 +105,7 @@ PROTOTYPES = {
     "sfx_voronoi_export": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip,
                                      _ip, _dp]),
     "sfx_voronoi_free": (None, [C.c_void_p]),
+    "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_group_create": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _dp,
                                    C.POINTER(C.c_void_p)]),
     "sfx_group_set_dt": (C.c_int, [C.c_void_p, _dp]),

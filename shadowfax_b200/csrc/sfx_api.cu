@@ -326,6 +326,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     d.n_faces = (int32_t)F;
     d.nnz = nnz;
     d.has_velocity = desc->face_velocity != nullptr;
+    d.lanes = 4;
     const int S = d.S;
     int rc = SFX_OK;
     auto A = [&](auto** p, size_t c) {
@@ -593,6 +594,13 @@ int sfx_riemann_eval(sfx_ctx* c, int32_t n, const double* WL, const double* WR,
     cudaFree(df);
     cudaFree(dc);
     return rc;
+}
+
+int sfx_mesh_set_lanes(sfx_mesh* m, int32_t lanes) {
+    if(!m || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16))
+        return SFX_ERR_INVALID;
+    m->d.lanes = lanes;
+    return SFX_OK;
 }
 
 int sfx_mesh_totals(sfx_mesh* m, double* totals) {

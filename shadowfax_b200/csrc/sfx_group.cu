@@ -100,7 +100,7 @@ extern "C" int sfx_group_create(sfx_ctx* ctx, int32_t n, sfx_mesh* const* meshes
     }
     g->dev.n_meshes = n;
     g->dev.dim = cfg->dim;
-    g->dev.lanes = cfg->dim == 3 ? 16 : 8;
+    g->dev.lanes = 4;
     int rc = cuda_ok(cudaSetDevice(cfg->device));
     if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.tab, sizeof(sfx_group_entry) * n));
     if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.pre, sizeof(int32_t) * 3 * (n + 1)));
@@ -124,7 +124,8 @@ extern "C" int sfx_group_set_dt(sfx_group* g, const double* dt) {
 }
 
 extern "C" int sfx_group_set_lanes(sfx_group* g, int32_t lanes) {
-    if(!g || (lanes != 4 && lanes != 8 && lanes != 16)) return SFX_ERR_INVALID;
+    if(!g || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16))
+        return SFX_ERR_INVALID;
     g->dev.lanes = lanes;
     return upload_layout(g);
 }
@@ -189,11 +190,11 @@ extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
         cudaEventDestroy(e0);
         return SFX_ERR_CUDA;
     }
-    const int cand[3] = {4, 8, 16};
+    const int cand[5] = {1, 2, 4, 8, 16};
     int best = g->dev.lanes;
     float best_ms = 1e30f;
     int rc = SFX_OK;
-    for(int c = 0; c < 3 && !rc; ++c) {
+    for(int c = 0; c < 5 && !rc; ++c) {
         rc = sfx_group_set_lanes(g, cand[c]);
         if(rc) break;
         /* timed on the gradient kernel, which only reads the states (the

@@ -28,6 +28,7 @@ struct sfx_dmesh {
     int32_t n_cells, n_faces;
     int64_t nnz;
     int32_t has_velocity;
+    int32_t lanes; /* split pass: lanes per cell of the gradient/update kernels */
     /* cells */
     double* pos;    /* [dim][n]  */
     double* cen;    /* [dim][n]  */

@@ -370,9 +370,9 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
                                                   out[4 * q + 3]);
 }
 
-template <int D>
+template <int D, int LPC>
 __global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
-    sgrad_body<D, Lanes<D>::value>(m, blockIdx.x * blockDim.x + threadIdx.x);
+    sgrad_body<D, LPC>(m, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ----------------------------- face physics ----------------------------- */
@@ -1070,9 +1070,9 @@ __device__ __forceinline__ void sapply_body(const sfx_dmesh& m, const double gam
     store_cell<D>(m.cw, i, Wf, (float)Q[0], (float)m.tarea[i]);
 }
 
-template <int D>
+template <int D, int LPC>
 __global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
-    sapply_body<D, Lanes<D>::value>(m, gamma, blockIdx.x * blockDim.x + threadIdx.x);
+    sapply_body<D, LPC>(m, gamma, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ------------------------- grouped (batched) launches -------------------------
@@ -1209,13 +1209,33 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
     return cuda_status(cudaGetLastError());
 }
 
+/* the per-cell kernels for the mesh's lanes-per-cell setting */
+template <int D>
+int cells_phase(const sfx_dmesh* m, int phase, double gamma, cudaStream_t s) {
+    const int G = grid_for((long long)m->n_cells * m->lanes, 256);
+#define SFX_LANES_CASE(LPC)                                        \
+    case LPC:                                                      \
+        if(phase == 0)                                             \
+            k_sgrad<D, LPC><<<G, 256, 0, s>>>(*m);                 \
+        else                                                       \
+            k_sapply<D, LPC><<<G, 256, 0, s>>>(*m, gamma);         \
+        break;
+    switch(m->lanes) {
+        SFX_LANES_CASE(1)
+        SFX_LANES_CASE(2)
+        SFX_LANES_CASE(4)
+        SFX_LANES_CASE(8)
+        SFX_LANES_CASE(16)
+    default:
+        return SFX_ERR_INVALID;
+    }
+#undef SFX_LANES_CASE
+    return cuda_status(cudaGetLastError());
+}
+
 int sfx_split_gradients(const sfx_dmesh* m, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    if(m->dim == 3)
-        k_sgrad<3><<<grid_for((long long)m->n_cells * Lanes<3>::value, 256), 256, 0, s>>>(*m);
-    else
-        k_sgrad<2><<<grid_for((long long)m->n_cells * Lanes<2>::value, 256), 256, 0, s>>>(*m);
-    return cuda_status(cudaGetLastError());
+    return m->dim == 3 ? cells_phase<3>(m, 0, 0., s) : cells_phase<2>(m, 0, 0., s);
 }
 
 int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, void* stream) {
@@ -1239,13 +1259,7 @@ int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, 
 
 int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    if(m->dim == 3)
-        k_sapply<3><<<grid_for((long long)m->n_cells * Lanes<3>::value, 256), 256, 0, s>>>(
-                *m, sp->gamma);
-    else
-        k_sapply<2><<<grid_for((long long)m->n_cells * Lanes<2>::value, 256), 256, 0, s>>>(
-                *m, sp->gamma);
-    return cuda_status(cudaGetLastError());
+    return m->dim == 3 ? cells_phase<3>(m, 2, sp->gamma, s) : cells_phase<2>(m, 2, sp->gamma, s);
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {
@@ -1261,6 +1275,8 @@ int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_pa
     cudaStream_t s = (cudaStream_t)stream;
     if(g->dim == 3) {
         switch(g->lanes) {
+        case 1: return group_phase<3, 1>(g, phase, sp, s);
+        case 2: return group_phase<3, 2>(g, phase, sp, s);
         case 4: return group_phase<3, 4>(g, phase, sp, s);
         case 8: return group_phase<3, 8>(g, phase, sp, s);
         case 16: return group_phase<3, 16>(g, phase, sp, s);
@@ -1268,6 +1284,8 @@ int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_pa
         }
     }
     switch(g->lanes) {
+    case 1: return group_phase<2, 1>(g, phase, sp, s);
+    case 2: return group_phase<2, 2>(g, phase, sp, s);
     case 4: return group_phase<2, 4>(g, phase, sp, s);
     case 8: return group_phase<2, 8>(g, phase, sp, s);
     case 16: return group_phase<2, 16>(g, phase, sp, s);

@@ -185,6 +185,24 @@ class FluxPass:
             raise L.SfxError(rc, "sfx_step", idx)
         return st
 
+    def set_lanes(self, lanes: int):
+        L.check(L.lib().sfx_mesh_set_lanes(self.h, lanes), "sfx_mesh_set_lanes")
+
+    def tune(self, dt: float, reps: int = 3) -> int:
+        """split pass: time the lanes-per-cell variants on this mesh's own
+        gradient+update kernels and keep the fastest (advances the state by
+        5 * (reps + 1) steps: call before loading the initial state)"""
+        best, best_ms = 4, 1e30
+        for lanes in (1, 2, 4, 8, 16):
+            self.set_lanes(lanes)
+            self.step_timed(dt, 1)
+            ms, _ = self.step_timed(dt, reps)
+            t = ms[0] + ms[2]
+            if t < best_ms:
+                best, best_ms = lanes, t
+        self.set_lanes(best)
+        return best
+
     def step_timed(self, dt: float, nsteps: int) -> tuple[np.ndarray, int]:
         """nsteps with per-kernel device times: (ms[gradients, faces, update],
         launches)"""
