@@ -1,25 +1,40 @@
 """Benchmark of the B200 flux pass (one JSON line on rank 0).
 
-Workload (N=1): the 3D Sedov-type blast on a static Voronoi mesh of 262,144
-generators uniform in the reflective unit cube (seed 2), gamma 5/3, HLLC
-solver, global CFL-0.4 time step; a "step" is one full pass of the hot path
-(gradients -> face fluxes -> update_Q/get_W) over the mesh.  The metric is
-face-steps per second (one nonzero-area face processed in one time step,
-with its share of the gradient and update work).
+Default workload (--workload serve): the config-5 request stream -- Poisson
+arrivals at 200 requests/s (seed 5), 70% 2D / 30% 3D static Voronoi meshes
+(periodic unit box) with generator counts log-uniform in [1e3, 1e6] served
+from a pre-tessellated pool (10 log-size bins per dimension), random-field
+states, U{10..200} steps, exact or HLLC 50/50.  A "step" is one request; the
+default run takes the stream's first 400 arrivals (about 2 s of the 60 s
+stream; --duration 60 runs it whole).  The unit of work is the face-step
+(one nonzero-area face processed in one time step, with its share of the
+gradient and update work).
+
+  value  the stream's requests with all states resident in HBM, co-batched
+         per (dimension, solver) class in launch groups, rounds of --chunk
+         steps, CUDA events on the device (FP32/FP64 split pass);
+  e2e    the same stream served by the request server (sfx_server_*) from
+         host memory at the arrival times: faces/s over the makespan, p50/p99
+         request latency; beside it the same stream served with the plain
+         FP64 pass one request at a time, and the split-vs-FP64 error.
+
+Other workloads: --workload sedov3d (config 2: 262,144 generators, HLLC, one
+mesh; --precision fp64|split) and --workload batch2d (config 4: 1,024 2D
+meshes in one launch group vs one FP64 launch sequence per mesh).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|split]
+                    [--workload serve|sedov3d|batch2d] [--precision fp64|split]
 
-Timing: CUDA events on the stream the library launches on, barrier +
-synchronize on both sides, max over ranks; W untimed warm-up steps.  The
-step's working set (about 300 MB: faces, cells, gradients, per-face fluxes)
-is larger than the 126 MB L2, so no separate L2 flush is done.
+Timing: CUDA events on the library's streams, barrier + synchronize on both
+sides, max over ranks; untimed warm-up before the timed region.  Working
+sets are larger than the 126 MB L2, so no separate L2 flush is done.
 
-N>1: every rank runs its own replica of the mesh (independent meshes, no
+N>1: every rank runs its own requests or meshes (independent units, no
 data-path collective): weak scaling.
 
 --impl reference times the reference's own CPU flux pass (the unmodified
-Shadowfax sources built into oracle/_ref) on the host cores on the same mesh.
+Shadowfax sources built into oracle/_ref) on the host cores: for the stream,
+one process per request on the first requests.
 """
 from __future__ import annotations
 
@@ -42,22 +57,34 @@ sys.path.insert(0, str(ROOT))
 N_GEN = 262_144
 SEED = 2
 METRIC = "faces/s (face-steps per second) of the flux pass"
+METRIC_SERVE = ("faces/s (face-steps per second) on 1 B200, served+batched FP32/FP64 split vs "
+                "plain FP64 at <=1e-6 rel L1; p50/p99 latency")
 UNIT = "face-steps/s"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (sedov3d 50, batch2d 20); serve: requests of the "
+                         "stream (default 400)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     ap.add_argument("--n", type=int, default=N_GEN, help="generators (default: config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="sedov3d", choices=["sedov3d", "batch2d"],
-                    help="sedov3d: config 2 on one mesh; batch2d: config 4, 1,024 meshes")
+    ap.add_argument("--workload", default="serve", choices=["serve", "sedov3d", "batch2d"],
+                    help="serve: config-5 request stream (default); sedov3d: config 2 on "
+                         "one mesh; batch2d: config 4, 1,024 meshes")
     ap.add_argument("--meshes", type=int, default=1024, help="batch2d: number of meshes")
-    return ap.parse_args()
+    ap.add_argument("--duration", type=float, default=None,
+                    help="serve: take every arrival of this many seconds of the stream "
+                         "instead of the first --steps requests (the full config is 60)")
+    ap.add_argument("--chunk", type=int, default=8, help="serve: steps per scheduling round")
+    a = ap.parse_args()
+    if a.steps is None:
+        a.steps = {"serve": 400, "sedov3d": 50, "batch2d": 20}[a.workload]
+    return a
 
 
 def dist_env():
@@ -165,6 +192,29 @@ def algorithmic_bytes(dim: int, n_cells: int, n_faces: int, nnz: int, precision:
     return {"gradients": grad, "faces": faces, "update": update}
 
 
+def split_kernel_bytes(dim: int, n_cells: int, n_faces: int, nnz: int):
+    """bytes each split-pass kernel must move at least once per launch, in
+    its device layout: face record fg (2 float4) + fi (int2) + shift code
+    (1 B) + FP64 area vector (8 dim); cell record cw (2 float4), cx
+    (float4), gradients cg (G float4, G = 4 in 3D, 2 in 2D); per-face dQ
+    {mass, energy} float2 + FP64 momentum (8 dim); Q FP64 (8 S).
+    gradients: cw, cx, offset, CSR entry, face fg + fi; write cg.
+    faces: face record, dQ write, and per cell cw, cx, cg.
+    update: offset, CSR entry, per-face dQ, Q read+write, volume, total
+    area (FP64), write cw."""
+    S = dim + 2
+    G = 16 * (4 if dim == 3 else 2)
+    grad = n_cells * (32 + 16 + 4 + G) + n_faces * (32 + 8) + nnz * 4
+    faces = n_faces * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + n_cells * (32 + 16 + G)
+    update = n_cells * (4 + 16 * S + 8 + 8 + 32) + nnz * 4 + n_faces * (8 + 8 * dim)
+    return {"gradients": grad, "faces": faces, "update": update}
+
+
+# bytes per face-step of the whole step, fixed for this workload's roofline:
+# face record + per-cell data / faces per cell (2D F ~ 3N, 3D F ~ 7.8N)
+STEP_BYTES = {("fp64", 2): 144, ("fp64", 3): 120, ("split", 2): 92, ("split", 3): 70}
+
+
 def build_problem(n: int):
     from shadowfax_b200 import workloads as wl
     return wl.sedov3d(n=n, seed=SEED, solver="HLLC")
@@ -194,7 +244,7 @@ def cpu_baseline_many(probs, steps: int = 2):
     from oracle.oracle import Params, ref_binary, run_reference
     if not ref_binary(2, "libm").exists():
         return None
-    P = os.cpu_count() or 1
+    P = min(os.cpu_count() or 1, len(probs))
     sample = probs[:P]
 
     def one(pr):
@@ -204,12 +254,14 @@ def cpu_baseline_many(probs, steps: int = 2):
 
     with ThreadPoolExecutor(max_workers=P) as ex:
         res = list(ex.map(one, sample))
-    work = sum(w for w, _ in res)
-    secs = max(s for _, s in res)
-    return {"value": work / secs, "unit": UNIT, "cores": P, "kind": "reference",
+    # sum of the per-process rates: every core kept busy (the makespan of
+    # unequal meshes would leave cores idle and understate the CPU)
+    value = sum(w / s for w, s in res)
+    return {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
             "sample": f"{len(sample)} meshes of the batch ({sum(p.mesh.n_cells for p in sample)} "
                       f"cells), {steps} timed steps each, one reference process per mesh on "
-                      f"{P} host cores concurrently (P processes, not an MPI run)"}
+                      f"{P} host cores concurrently (P processes, not an MPI run; value = "
+                      f"sum of the per-process rates)"}
 
 
 def bench_batch(args, rank, world, local, torch):
@@ -338,10 +390,377 @@ def bench_batch(args, rank, world, local, torch):
     return line
 
 
+SERVE_BUDGET = 150 << 30
+# reference processes of the CPU sample at most (each holds a whole mesh of
+# up to 7e5 cells in the reference's per-cell objects)
+SERVE_CPU_PROCS = 48
+
+
+def serve_requests(args, rank):
+    """the config-5 stream: first --steps arrivals, or --duration seconds"""
+    from shadowfax_b200 import workloads as wl
+    seed = 5 + 1000 * rank
+    if args.duration:
+        return wl.serve_stream(duration=args.duration, seed=seed)
+    return wl.serve_stream(count=args.steps, seed=seed)
+
+
+def l1_rel_fields(a, b):
+    """relative L1 error per conserved field (mass, momentum, energy); the
+    momentum components share the L1 norm of the momentum magnitude"""
+    D = b.shape[1] - 2
+    den = np.abs(b).sum(0)
+    den[1:D + 1] = np.sqrt((b[:, 1:D + 1] ** 2).sum(1)).sum()
+    e = np.abs(a - b).sum(0) / den
+    return np.array([e[0], e[1:D + 1].max(), e[D + 1]])
+
+
+def run_served(pool, reqs, precision, chunk, sample_every, device=0):
+    """serve the stream through the request server (C ABI, host states in
+    and out): submit each request at its arrival time from a feeder thread,
+    collect completions concurrently; returns per-request results (states
+    kept for every sample_every-th request), launches and server stats"""
+    from shadowfax_b200 import _lib as L
+    from shadowfax_b200.serve import Server
+    srv = Server(precision=precision, memory_budget=SERVE_BUDGET, chunk_steps=chunk,
+                 device=device)
+    try:
+        ids = {j: srv.add_mesh(m) for j, m in enumerate(pool.meshes) if m is not None}
+        # warm-up: a short request per class on the smallest meshes
+        warm = []
+        for j0 in (0, pool.k):
+            for solver in ("Exact", "HLLC"):
+                if j0 in ids:
+                    warm.append(srv.submit(ids[j0], pool.states[j0][0], solver,
+                                           pool.dts[j0][0], 3))
+        srv.drain(600.0)
+        for r in warm:
+            srv.poll(r, want_state=False)
+        lock = threading.Lock()
+        pending = {}
+        results = {}
+        n0 = L.lib().sfx_launch_count()
+        t_base = time.perf_counter()
+
+        def feeder():
+            for j, r in enumerate(reqs):
+                delay = t_base + r.t - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                rid = srv.submit(ids[r.mesh], pool.states[r.mesh][r.state], r.solver,
+                                 pool.dts[r.mesh][r.state], r.nsteps)
+                with lock:
+                    pending[rid] = j
+
+        th = threading.Thread(target=feeder, daemon=True)
+        th.start()
+        while len(results) < len(reqs):
+            with lock:
+                items = list(pending.items())
+            for rid, j in items:
+                res = srv.poll(rid, want_state=(j % sample_every == 0))
+                if res is not None:
+                    results[j] = res
+                    with lock:
+                        del pending[rid]
+            time.sleep(0.001)
+        th.join()
+        launches = L.lib().sfx_launch_count() - n0
+        st = srv.stats()
+    finally:
+        srv.shutdown()
+    return [results[j] for j in range(len(reqs))], launches, st
+
+
+def served_summary(res, reqs):
+    ok = [r for r in res if r.status == 0]
+    lat = np.array([r.t_done - r.t_submit for r in ok]) if ok else np.zeros(1)
+    t0 = min(r.t_submit for r in res)
+    t1 = max(r.t_done for r in res)
+    fs = sum(r.face_steps for r in ok)
+    return {"value": fs / (t1 - t0), "unit": UNIT, "requests": len(res), "completed": len(ok),
+            "failed": len(res) - len(ok), "face_steps": int(fs), "makespan_s": t1 - t0,
+            "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean())}
+
+
+def run_resident(pool, reqs, chunk, torch, local):
+    """the stream's requests with every state resident in HBM before the
+    timed region: requests co-batched per (dimension, solver) class, one
+    launch group per class on its own stream, rounds of `chunk` steps with
+    device step counters and the finished requests dropped between rounds
+    (the server's schedule without arrivals and host transfers).  Waves of
+    requests fit the 150 GB budget.  Returns (face_steps, ms, roofline)."""
+    from shadowfax_b200 import _lib as L
+    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
+    pool_ctx = {d: Context(d, RiemannSolverFactory.generate("HLLC"), L.PREC_SPLIT, device=local)
+                for d in (2, 3)}
+    bases = {j: FluxPass(pool_ctx[m.dim], m) for j, m in enumerate(pool.meshes) if m is not None}
+    classes = [(d, sv) for d in (2, 3) for sv in ("Exact", "HLLC")]
+    cctx, cstream = {}, {}
+    for c in classes:
+        cctx[c] = Context(c[0], RiemannSolverFactory.generate(c[1]), L.PREC_SPLIT, device=local)
+        cstream[c] = torch.cuda.Stream(device=local)
+        cctx[c].set_stream(cstream[c].cuda_stream)
+    main = torch.cuda.current_stream(local)
+    # waves under the budget, in arrival order
+    waves, cur, used = [], [], 0
+    for j, r in enumerate(reqs):
+        b = bases[r.mesh].clone_bytes(L.PREC_SPLIT)
+        if cur and used + b > SERVE_BUDGET:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += b
+    if cur:
+        waves.append(cur)
+    total_ms, face_steps, launches, roof = 0.0, 0, 0, None
+    failed = set()
+    for w, wave in enumerate(waves):
+        inst = {}
+        for j in wave:
+            r = reqs[j]
+            c = (pool.meshes[r.mesh].dim, r.solver)
+            fp = bases[r.mesh].clone(cctx[c])
+            fp.set_primitive(pool.states[r.mesh][r.state])
+            inst[j] = (c, fp)
+        if w == 0:
+            roof = resident_roofline(pool, reqs, inst, classes, cctx)
+            for j, (c, fp) in inst.items():      # back to the initial states
+                fp.set_primitive(pool.states[reqs[j].mesh][reqs[j].state])
+        torch.cuda.synchronize()
+        live = {c: [j for j in wave if inst[j][0] == c] for c in classes}
+        left = {j: reqs[j].nsteps for j in wave}
+        groups = {c: None for c in classes}
+        reused = {c: 0 for c in classes}
+        n0 = L.lib().sfx_launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for c in classes:
+            cstream[c].wait_event(e0)
+        while any(live.values()):
+            for c in classes:
+                if groups[c] is None and live[c]:
+                    groups[c] = Group(cctx[c], [inst[j][1] for j in live[c]],
+                                      [pool.dts[reqs[j].mesh][reqs[j].state] for j in live[c]])
+                    groups[c].set_steps([left[j] for j in live[c]])
+                    reused[c] = 0
+            for c in classes:
+                if groups[c] is not None:
+                    groups[c].step(chunk, graph=reused[c] > 0, status=False)
+            for c in classes:
+                g = groups[c]
+                if g is None:
+                    continue
+                steps_left = g.get_steps()
+                st = g.status()
+                for j, k, e in zip(live[c], steps_left, st):
+                    left[j] = 0 if e else int(k)
+                    if e:
+                        failed.add(j)
+                keep = [j for j in live[c] if left[j] > 0]
+                if len(keep) != len(live[c]):
+                    g.close()
+                    groups[c] = None
+                    live[c] = keep
+                else:
+                    reused[c] += 1
+        for c in classes:
+            ev = torch.cuda.Event()
+            ev.record(cstream[c])
+            main.wait_event(ev)
+        e1.record(main)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        launches += L.lib().sfx_launch_count() - n0
+        face_steps += sum(pool.meshes[reqs[j].mesh].n_active_faces * reqs[j].nsteps
+                          for j in wave if j not in failed)
+        for c in classes:
+            if groups[c] is not None:
+                groups[c].close()
+        for c, fp in inst.values():
+            fp.close()
+    for fp in bases.values():
+        fp.close()
+    for c in classes:
+        cctx[c].close()
+    for c in pool_ctx.values():
+        c.close()
+    return face_steps, total_ms, launches, roof, len(waves), len(failed)
+
+
+def resident_roofline(pool, reqs, inst, classes, cctx):
+    """per-kernel device times of the class with the most face work, all of
+    its requests in one launch group, CUDA events around each launch"""
+    from shadowfax_b200.hydro import Group
+    work = {c: 0 for c in classes}
+    for j, (c, fp) in inst.items():
+        work[c] += pool.meshes[reqs[j].mesh].n_active_faces * reqs[j].nsteps
+    top_c = max(classes, key=lambda c: work[c])
+    js = [j for j, (c, _) in inst.items() if c == top_c]
+    g = Group(cctx[top_c], [inst[j][1] for j in js],
+              [pool.dts[reqs[j].mesh][reqs[j].state] for j in js])
+    g.step_timed(1)
+    steps = 3
+    ms, nl = g.step_timed(steps)
+    g.close()
+    per_launch = ms / steps
+    names = ["gradients", "faces", "update"]
+    alg = {k: 0 for k in names}
+    faces = 0
+    for j in js:
+        m = pool.meshes[reqs[j].mesh]
+        b = split_kernel_bytes(m.dim, m.n_cells, m.n_faces, m.nnz)
+        for k in names:
+            alg[k] += b[k]
+        faces += m.n_active_faces
+    top = int(np.argmax(per_launch))
+    peak, peak_kind = peaks()
+    achieved = alg[names[top]] / (per_launch[top] / 1e3) / 1e9
+    D = top_c[0]
+    step_rate = faces / (per_launch.sum() / 1e3)
+    kname = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces",
+             "update": "k_group_sapply"}[names[top]]
+    return {"bound": "hbm", "kernel": kname,
+            "class": f"{D}D {top_c[1]}, {len(js)} requests, {faces} faces",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": f"hbm_gbs {peak_kind}",
+            "algorithmic_bytes_per_launch": alg[names[top]],
+            "kernel_ms": {k: float(v) for k, v in zip(names, per_launch)},
+            "step_bytes_per_face": STEP_BYTES[("split", D)],
+            "step_achieved_gbs": STEP_BYTES[("split", D)] * step_rate / 1e9,
+            "step_frac": STEP_BYTES[("split", D)] * step_rate / 1e9 / peak}
+
+
+def serve_cpu_sample(pool, reqs, steps: int = 2):
+    """the reference CPU pass on the stream's first P requests (P = host
+    cores), one process per request, concurrently"""
+    from shadowfax_b200.workloads import Problem
+    P = min(os.cpu_count() or 1, SERVE_CPU_PROCS)
+    probs = []
+    for r in reqs[:P]:
+        m = pool.meshes[r.mesh]
+        probs.append(Problem(f"req{len(probs)}", m, pool.states[r.mesh][r.state], r.solver,
+                             pool.dts[r.mesh][r.state], steps))
+    cb = cpu_baseline_many(probs, steps)
+    if cb is not None:
+        cb["sample"] = (f"the stream's first {len(probs)} requests ({sum(p.mesh.n_cells for p in probs)}"
+                        f" cells, both solvers, 2D and 3D), {steps} timed steps each, one "
+                        f"reference process per request on {P} host cores concurrently "
+                        f"(P processes, not an MPI run; value = sum of the per-process rates)")
+    return cb
+
+
+def bench_serve(args, rank, world, local, torch):
+    """config 5: the request stream served by the continuous-batching server
+    (FP32/FP64 split, co-batched) against the same stream served with the
+    plain FP64 pass one request at a time"""
+    from shadowfax_b200 import _lib as L
+    from shadowfax_b200 import workloads as wl
+    reqs = serve_requests(args, rank)
+    t_build = time.time()
+    used = sorted({r.mesh for r in reqs})
+    pool = wl.serve_pool(only=set(used))
+    t_build = time.time() - t_build
+    sample_every = max(1, len(reqs) // 24)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local) as clk:
+        clk.wait_first_sample()
+        clk.mark("t0")
+        # resident (device-timed) throughput and the roofline
+        fs, ms, launches_res, roof, nwaves, nfail_res = run_resident(pool, reqs, args.chunk,
+                                                                     torch, local)
+        # the same stream served from host memory
+        res32, launches, st32 = run_served(pool, reqs, L.PREC_SPLIT, args.chunk,
+                                           sample_every, local)
+        clk.mark("t1")
+        time.sleep(0.3)
+    res64, launches64, _ = run_served(pool, reqs, L.PREC_FP64, args.chunk, sample_every, local)
+    split = served_summary(res32, reqs)
+    fp64 = served_summary(res64, reqs)
+    # accuracy and conservation on the sampled requests
+    errs, drift = [], []
+    for j in range(0, len(reqs), sample_every):
+        a, b = res32[j], res64[j]
+        if a.status or b.status:
+            continue
+        errs.append(l1_rel_fields(a.Q, b.Q))
+        m = pool.meshes[reqs[j].mesh]
+        W0 = pool.states[reqs[j].mesh][reqs[j].state]
+        D = m.dim
+        V = m.cell_volume
+        mass0 = float((W0[:, 0] * V).sum())
+        e0 = float(((W0[:, D + 1] / (wl.GAMMA - 1) + 0.5 * W0[:, 0] *
+                     (W0[:, 1:D + 1] ** 2).sum(1)) * V).sum())
+        drift.append([abs(a.Q[:, 0].sum() - mass0) / mass0,
+                      abs(a.Q[:, D + 1].sum() - e0) / e0])
+    errs = np.max(errs, 0) if errs else np.full(3, np.nan)
+    drift = np.max(drift, 0) if drift else np.full(2, np.nan)
+    t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+    tf = torch.tensor([float(fs)], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(tf, op=torch.distributed.ReduceOp.SUM)
+    value = float(tf.item()) / (float(t.item()) / 1e3)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = serve_cpu_sample(pool, reqs)
+    h2d = sum(pool.states[r.mesh][r.state].nbytes for r in reqs)
+    d2h = 2 * h2d
+    n2 = sum(1 for r in reqs if r.mesh < pool.k)
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC_SERVE, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": len(reqs), "warmup": args.warmup,
+            "ms_per_step": float(t.item()) / len(reqs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"serve: config-5 request stream, {len(reqs)} Poisson arrivals "
+                                   f"at 200/s (seed 5; {'%.1f s' % reqs[-1].t} of the 60 s stream), "
+                                   f"{n2} 2D / {len(reqs) - n2} 3D, N log-uniform in [1e3, 1e6] "
+                                   f"from a pool of {len(used)} periodic meshes (10 log bins per "
+                                   f"dimension), random-field states, steps U{{10..200}}, "
+                                   f"exact/HLLC 50/50, 150 GB budget",
+                       "step": "one request of the stream",
+                       "precision": "split (FP32 reconstruction/HLLC, FP64 p* iteration, "
+                                    "FP64 accumulation)",
+                       "chunk_steps": args.chunk, "resident_waves": nwaves,
+                       "resident_failed_requests": nfail_res,
+                       "l2": "working set > L2 (no flush)",
+                       "parallelism": f"replicas x{world}",
+                       "pool_build_s": round(t_build, 1)},
+            "clocks": clk.summary(),
+            "served": split,
+            "served_fp64_per_request": fp64,
+            "served_speedup_vs_fp64": split["value"] / fp64["value"],
+            "split_vs_fp64_max_rel_l1": {"mass": errs[0], "momentum": errs[1],
+                                         "energy": errs[2],
+                                         "sample": f"every {sample_every}th request"},
+            "split_conservation_max_rel_drift": {"mass": drift[0], "energy": drift[1]},
+            "roofline": roof,
+            "cpu_baseline": cb,
+            "e2e": {"value": split["value"], "unit": UNIT, "h2d_bytes_per_step": h2d / len(reqs),
+                    "d2h_bytes_per_step": d2h / len(reqs),
+                    "note": "served stream: request states from host memory, results to host "
+                            "memory, makespan from first arrival to last completion"},
+            "p50_latency_s": split["p50_latency_s"], "p99_latency_s": split["p99_latency_s"],
+            "gpu_launches": int(launches_res),
+            "gpu_launches_served": int(launches),
+        }
+    return line
+
+
 def run_reference_arm(args, rank, world):
     """--impl reference: the reference's own CPU pass on the host cores"""
     if rank != 0:
         return
+    if args.workload == "serve":
+        return run_reference_serve(args)
     pr = build_problem(args.n)
     steps = max(1, min(args.steps, 5))
     from oracle.oracle import ref_binary
@@ -363,6 +782,34 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def run_reference_serve(args):
+    """--impl reference on the request stream: the reference CPU pass, one
+    process per request on all host cores, for the stream's first requests
+    (a bounded sample per step; the reference has no request loop)"""
+    from oracle.oracle import ref_binary
+    from shadowfax_b200 import workloads as wl
+    if not (ref_binary(2, "libm").exists() and ref_binary(3, "libm").exists()):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref reference harness not built (needs the reference tree)"}))
+        return
+    reqs = serve_requests(args, 0)
+    P = min(os.cpu_count() or 1, SERVE_CPU_PROCS)
+    pool = wl.serve_pool(only={r.mesh for r in reqs[:P]})
+    steps = max(1, min(args.steps, 2))
+    cb = serve_cpu_sample(pool, reqs, steps)
+    faces = sum(pool.meshes[r.mesh].n_active_faces for r in reqs[:P])
+    line = {"metric": METRIC_SERVE, "value": cb["value"], "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * faces / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "serve: config-5 request stream (first requests, one "
+                                   "reference process each)", "precision": "fp64"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -378,8 +825,9 @@ def main():
             dist.destroy_process_group()
         return
     torch.cuda.set_device(local)
-    if args.workload == "batch2d":
-        line = bench_batch(args, rank, world, local, torch)
+    if args.workload in ("batch2d", "serve"):
+        fn = bench_batch if args.workload == "batch2d" else bench_serve
+        line = fn(args, rank, world, local, torch)
         if line is not None:
             print(json.dumps(line))
         if world > 1:

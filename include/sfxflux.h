@@ -211,6 +211,15 @@ int sfx_riemann_eval(sfx_ctx* ctx, int32_t n, const double* WL, const double* WR
 /* conserved totals sum_i Q_i (m, p[dim], e), deterministic FP64 */
 int sfx_mesh_totals(sfx_mesh* mesh, double* totals);
 
+/* A new mesh handle on `ctx` that shares `base`'s device geometry and owns
+ * only a state (W, Q and the per-step scratch of ctx's precision): several
+ * integrations of one tessellation without copying it again.  `base` must
+ * outlive the clone and have been uploaded with the split arrays if ctx is
+ * SFX_PREC_SPLIT.  sfx_flux_pass is not available on split clones. */
+int sfx_mesh_clone(sfx_ctx* ctx, sfx_mesh* base, sfx_mesh** out);
+/* device bytes a clone of `base` at `precision` allocates */
+int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision);
+
 /* split pass: lanes of a warp that share one cell in the gradient and update
  * kernels (1, 2, 4, 8 or 16; default 4).  Changes the summation tree of the
  * per-cell sums, not the algorithm. */
@@ -236,6 +245,18 @@ int sfx_group_step(sfx_group* group, int32_t nsteps, int32_t use_graph,
  * gradient and update kernels; *lanes receives it */
 int sfx_group_tune(sfx_group* group, int32_t reps, int32_t* lanes);
 int sfx_group_set_lanes(sfx_group* group, int32_t lanes);
+/* per-member remaining step counts, kept on the device: a member at 0 is
+ * skipped by the launches and each step counts the others down, so members
+ * with different step counts share launches without host round trips */
+int sfx_group_set_steps(sfx_group* group, const int32_t* steps);
+int sfx_group_get_steps(sfx_group* group, int32_t* steps);
+/* nsteps without a graph, with CUDA events around each phase's launch:
+ * phase_ms[3] receives the summed device time of the gradient, face and
+ * update launches, *launches (may be NULL) the number of kernels launched */
+int sfx_group_step_timed(sfx_group* group, int32_t nsteps, float* phase_ms,
+                         int32_t* launches);
+/* per-member status of the last sfx_group_step (waits for the group) */
+int sfx_group_status(sfx_group* group, int32_t* mesh_status);
 int sfx_group_free(sfx_group* group);
 
 /* ---- host Voronoi face-list builder (inputs for the pass) ---- */
@@ -251,6 +272,68 @@ int sfx_voronoi_export(const sfx_voronoi* v, double* cell_centroid,
                        int32_t* face_left, int32_t* face_right,
                        int32_t* face_kind, double* face_right_pos);
 void sfx_voronoi_free(sfx_voronoi* v);
+
+/* ---- request server: continuous batching of static-mesh integrations ----
+ * No counterpart in the reference (Shadowfax runs one simulation per job).
+ * Meshes are added once to a device-resident pool; a request names a pool
+ * mesh, an initial state, a solver, a time step and a step count.  A worker
+ * thread admits queued requests in arrival order while the device-memory
+ * budget and the slot count allow, keeps admitted states resident, and
+ * advances all admitted requests of one (dimension, solver) class together:
+ * SFX_PREC_SPLIT co-batches them into one launch group per class and chunk
+ * of steps (per-request step counters on the device), SFX_PREC_FP64 steps
+ * each request alone (the per-request baseline).  Requests arriving while
+ * others run join at the next chunk.  Results wait in host memory until
+ * sfx_server_poll collects them. */
+typedef struct sfx_server sfx_server;
+
+typedef struct sfx_server_config {
+    int32_t device;
+    int32_t precision;      /* SFX_PREC_SPLIT (co-batched) or SFX_PREC_FP64     */
+    double gamma;
+    double tolerance;
+    double cutoff;
+    int64_t memory_budget;  /* device bytes for admitted request states       */
+    int32_t max_active;     /* admitted requests at most                      */
+    int32_t chunk_steps;    /* steps per scheduling round                     */
+} sfx_server_config;
+
+typedef struct sfx_request_info {
+    int32_t status;         /* SFX_OK or the request's error                  */
+    int32_t steps_done;
+    int32_t mesh_id;
+    int32_t solver;
+    double t_submit;        /* seconds on the server's clock                  */
+    double t_admit;
+    double t_done;
+    int64_t face_steps;     /* nonzero-area faces x steps done                */
+} sfx_request_info;
+
+typedef struct sfx_server_stats {
+    int64_t submitted, admitted, completed, failed, active, queued;
+    int64_t face_steps;     /* over completed requests                        */
+    int64_t bytes_in_use;   /* device bytes of admitted request states        */
+    int64_t rounds;         /* scheduling rounds run                          */
+    double now;             /* server clock, seconds                          */
+} sfx_server_stats;
+
+int sfx_server_create(const sfx_server_config* cfg, sfx_server** out);
+/* add a mesh to the device pool (upload once); *mesh_id identifies it */
+int sfx_server_add_mesh(sfx_server* srv, const sfx_mesh_desc* desc, int32_t* mesh_id);
+/* queue a request; W0 [n_cells][S] is copied; returns at once */
+int sfx_server_submit(sfx_server* srv, int32_t mesh_id, const double* W0, int32_t solver,
+                      double dt, int32_t nsteps, int64_t* request_id);
+/* SFX_ERR_NOT_READY while the request runs; then copies W and Q (either may
+ * be NULL to discard), fills info (may be NULL), forgets the request and
+ * returns its status */
+int sfx_server_poll(sfx_server* srv, int64_t request_id, double* W, double* Q,
+                    sfx_request_info* info);
+/* wait until nothing is queued or running (timeout_s <= 0: no limit);
+ * SFX_ERR_NOT_READY on timeout */
+int sfx_server_drain(sfx_server* srv, double timeout_s);
+int sfx_server_stats_get(sfx_server* srv, sfx_server_stats* stats);
+/* stop the worker, free every request and the pool */
+int sfx_server_shutdown(sfx_server* srv);
 
 /* ---- one FP64 flux pass that allocates nothing ----
  * No counterpart in the reference.  For callers that cannot allocate device
@@ -299,6 +382,9 @@ int sfx_flux_pass_noalloc(const sfx_device_mesh* mesh, const sfx_config* cfg, do
 
 /* library version string */
 const char* sfx_version(void);
+/* kernels this library has launched since it was loaded (all contexts;
+ * a replayed CUDA graph counts each kernel it runs) */
+int64_t sfx_launch_count(void);
 
 #ifdef __cplusplus
 }

@@ -20,10 +20,12 @@ STATUS_NAMES = {
     4: "SFX_ERR_NAN_FLUX", 5: "SFX_ERR_NEG_STATE", 6: "SFX_ERR_NOCONV",
     7: "SFX_ERR_BOUNDS", 8: "SFX_ERR_UNSUPPORTED", 9: "SFX_ERR_MESH",
     10: "SFX_ERR_NOMEM", 11: "SFX_ERR_NOT_READY", 12: "SFX_ERR_CLOSED",
+    13: "SFX_ERR_TOO_LARGE",
 }
 SFX_ERR_INVALID, SFX_ERR_CUDA, SFX_ERR_RIEMANN, SFX_ERR_NAN_FLUX = 1, 2, 3, 4
 SFX_ERR_NEG_STATE, SFX_ERR_NOCONV, SFX_ERR_BOUNDS, SFX_ERR_UNSUPPORTED = 5, 6, 7, 8
 SFX_ERR_MESH, SFX_ERR_NOMEM, SFX_ERR_NOT_READY, SFX_ERR_CLOSED = 9, 10, 11, 12
+SFX_ERR_TOO_LARGE = 13
 
 SOLVER_EXACT, SOLVER_HLLC = 0, 1
 PREC_FP64, PREC_SPLIT = 0, 1
@@ -73,6 +75,26 @@ class sfx_device_mesh(C.Structure):
                 ("face_kind", C.c_void_p), ("face_right_pos", C.c_void_p)]
 
 
+class sfx_server_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("gamma", C.c_double),
+                ("tolerance", C.c_double), ("cutoff", C.c_double),
+                ("memory_budget", C.c_int64), ("max_active", C.c_int32),
+                ("chunk_steps", C.c_int32)]
+
+
+class sfx_request_info(C.Structure):
+    _fields_ = [("status", C.c_int32), ("steps_done", C.c_int32), ("mesh_id", C.c_int32),
+                ("solver", C.c_int32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("face_steps", C.c_int64)]
+
+
+class sfx_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("failed", C.c_int64), ("active", C.c_int64), ("queued", C.c_int64),
+                ("face_steps", C.c_int64), ("bytes_in_use", C.c_int64), ("rounds", C.c_int64),
+                ("now", C.c_double)]
+
+
 class sfx_stats(C.Structure):
     _fields_ = [("status", C.c_int32), ("bad_face", C.c_int32), ("bad_cell", C.c_int32),
                 ("steps_done", C.c_int32), ("totals", C.c_double * 5)]
@@ -83,6 +105,7 @@ _lib = None
 # name -> (restype, argtypes); every exported symbol of include/sfxflux.h
 PROTOTYPES = {
     "sfx_version": (C.c_char_p, []),
+    "sfx_launch_count": (C.c_int64, []),
     "sfx_ctx_create": (C.c_int, [C.POINTER(sfx_config), C.POINTER(C.c_void_p)]),
     "sfx_ctx_destroy": (C.c_int, [C.c_void_p]),
     "sfx_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -106,6 +129,22 @@ PROTOTYPES = {
                                      _ip, _dp]),
     "sfx_voronoi_free": (None, [C.c_void_p]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sfx_mesh_clone": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sfx_mesh_clone_bytes": (C.c_int64, [C.c_void_p, C.c_int32]),
+    "sfx_group_set_steps": (C.c_int, [C.c_void_p, _ip]),
+    "sfx_group_get_steps": (C.c_int, [C.c_void_p, _ip]),
+    "sfx_group_status": (C.c_int, [C.c_void_p, _ip]),
+    "sfx_group_step_timed": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float),
+                                       C.POINTER(C.c_int32)]),
+    "sfx_server_create": (C.c_int, [C.POINTER(sfx_server_config), C.POINTER(C.c_void_p)]),
+    "sfx_server_add_mesh": (C.c_int, [C.c_void_p, C.POINTER(sfx_mesh_desc), _ip]),
+    "sfx_server_submit": (C.c_int, [C.c_void_p, C.c_int32, _dp, C.c_int32, C.c_double,
+                                    C.c_int32, C.POINTER(C.c_int64)]),
+    "sfx_server_poll": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp,
+                                  C.POINTER(sfx_request_info)]),
+    "sfx_server_drain": (C.c_int, [C.c_void_p, C.c_double]),
+    "sfx_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(sfx_server_stats)]),
+    "sfx_server_shutdown": (C.c_int, [C.c_void_p]),
     "sfx_group_create": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _dp,
                                    C.POINTER(C.c_void_p)]),
     "sfx_group_set_dt": (C.c_int, [C.c_void_p, _dp]),

@@ -37,6 +37,7 @@ UNITS = {
     "sfx_api.cu": [],
     "sfx_noalloc.cu": [],
     "sfx_group.cu": [],
+    "sfx_server.cu": [],
     "sfx_voronoi.cpp": [],
 }
 

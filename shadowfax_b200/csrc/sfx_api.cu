@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <unordered_map>
@@ -125,6 +126,13 @@ int reset_err(sfx_mesh* m) {
 sfx_dmesh* sfx_mesh_dev(sfx_mesh* m) {
     return &m->d;
 }
+int sfx_mesh_last_status(sfx_mesh* m, int32_t* bad_index) {
+    sfx_stats st;
+    std::memset(&st, 0, sizeof st);
+    const int rc = check_err(m, &st);
+    if(bad_index) *bad_index = st.bad_face >= 0 ? st.bad_face : st.bad_cell;
+    return rc;
+}
 sfx_ctx* sfx_mesh_ctx(sfx_mesh* m) {
     return m->ctx;
 }
@@ -138,7 +146,24 @@ const sfx_solver_params* sfx_ctx_params(sfx_ctx* c) {
     return &c->sp;
 }
 
+namespace {
+std::atomic<long long> g_launches{0};
+thread_local bool t_capturing = false;
+}  // namespace
+
+void sfx_count_launches(int n) {
+    if(!t_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+void sfx_launch_capture(bool on) {
+    t_capturing = on;
+}
+
 extern "C" {
+
+int64_t sfx_launch_count(void) {
+    return g_launches.load(std::memory_order_relaxed);
+}
 
 const char* sfx_version(void) {
     return "sfxflux 0.1 (sm_100a)";
@@ -524,6 +549,7 @@ int sfx_flux_pass(sfx_mesh* m, double dt, double* grad, double* dQ_face,
     const int64_t n = m->d.n_cells, F = m->d.n_faces;
     const int S = m->d.S, D = m->d.dim;
     const bool split = c->cfg.precision == SFX_PREC_SPLIT;
+    if(!m->d.dQf) return SFX_ERR_UNSUPPORTED; /* a split clone keeps no FP64 dQ */
     SFX_TRY(reset_err(m));
     SFX_TRY(run_phase(m, 0, dt, 1, s));
     SFX_TRY(run_phase(m, 1, dt, 1, s));
@@ -594,6 +620,69 @@ int sfx_riemann_eval(sfx_ctx* c, int32_t n, const double* WL, const double* WR,
     cudaFree(df);
     cudaFree(dc);
     return rc;
+}
+
+int sfx_mesh_clone(sfx_ctx* ctx, sfx_mesh* base, sfx_mesh** out) {
+    if(!ctx || !base || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    const sfx_dmesh& b = base->d;
+    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
+    if(ctx->cfg.dim != b.dim || ctx->closing) return SFX_ERR_INVALID;
+    if(split && !b.fg) return SFX_ERR_INVALID; /* base has no split geometry */
+    if(cudaSetDevice(ctx->cfg.device) != cudaSuccess) return SFX_ERR_CUDA;
+    sfx_mesh* m = new(std::nothrow) sfx_mesh;
+    if(!m) return SFX_ERR_NOMEM;
+    m->ctx = ctx;
+    ctx->live_meshes++;
+    m->d = b; /* geometry pointers shared with the base */
+    sfx_dmesh& d = m->d;
+    const int64_t n = d.n_cells, F = d.n_faces;
+    const int S = d.S, dim = d.dim;
+    d.W = d.Q = d.grad = d.dQf = nullptr;
+    d.branch = nullptr;
+    d.err = nullptr;
+    d.totals_scratch = nullptr;
+    d.cw = d.cg = nullptr;
+    d.dqm = nullptr;
+    d.dqv = nullptr;
+    int rc = SFX_OK;
+    auto A = [&](auto** p, size_t c) {
+        if(rc == SFX_OK) rc = dalloc(m, p, c);
+    };
+    A(&d.W, n * S);
+    A(&d.Q, n * S);
+    A(&d.err, 1);
+    A(&d.totals_scratch, (size_t)(S + 1) * 1024);
+    if(split) {
+        A(&d.cw, 2 * n);
+        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
+        A(&d.dqm, F);
+        A(&d.dqv, (size_t)dim * F);
+    } else {
+        A(&d.grad, n * dim * S);
+        A(&d.dQf, F * S);
+        A(&d.branch, F);
+    }
+    if(!rc) rc = reset_err(m);
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(ctx->stream));
+    if(rc) {
+        sfx_mesh_free(m);
+        return rc;
+    }
+    *out = m;
+    return SFX_OK;
+}
+
+int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
+    if(!base) return -1;
+    const sfx_dmesh& b = base->d;
+    const int64_t n = b.n_cells, F = b.n_faces, S = b.S, D = b.dim;
+    int64_t bytes = n * S * 16 + (S + 1) * 1024 * 8 + 64;
+    if(precision == SFX_PREC_SPLIT)
+        bytes += n * 32 + n * 16 * ((D * S + 3) / 4) + F * 8 + F * D * 8;
+    else
+        bytes += n * D * S * 8 + F * S * 8 + F * 4;
+    return bytes;
 }
 
 int sfx_mesh_set_lanes(sfx_mesh* m, int32_t lanes) {

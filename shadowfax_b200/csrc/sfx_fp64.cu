@@ -1236,6 +1236,7 @@ int sfx_fp64_gradients(const sfx_dmesh* m, void* stream) {
         k_gradients<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m);
     else
         k_gradients<2><<<grid_for(m->n_cells, B), B, 0, s>>>(*m);
+    sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1256,6 +1257,7 @@ int sfx_fp64_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
         else
             k_faces<2, SFX_SOLVER_HLLC><<<G, B, 0, s>>>(*m, *sp, dt, write_branch);
     }
+    sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1267,6 +1269,7 @@ int sfx_fp64_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream
         k_apply<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma);
     else
         k_apply<2><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma);
+    sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1278,6 +1281,7 @@ int sfx_fp64_init_Q(const sfx_dmesh* m, const sfx_solver_params* sp, void* strea
         k_init_Q<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma, sp->kind);
     else
         k_init_Q<2><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma, sp->kind);
+    sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1286,6 +1290,7 @@ int sfx_fp64_totals(const sfx_dmesh* m, double* host_out, void* stream) {
     k_totals_partial<<<kTotBlocks, kTotThreads, 0, s>>>(m->Q, m->n_cells, m->S,
                                                          m->totals_scratch);
     k_totals_final<<<1, 256, 0, s>>>(m->totals_scratch, m->S);
+    sfx_count_launches(2);
     cudaError_t e = cudaMemcpyAsync(host_out, m->totals_scratch + (size_t)m->S * kTotBlocks,
                                     sizeof(double) * m->S, cudaMemcpyDeviceToHost, s);
     if(e != cudaSuccess) return SFX_ERR_CUDA;
@@ -1313,5 +1318,6 @@ int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n, const double* 
             k_riemann<2, SFX_SOLVER_HLLC><<<G, B, 0, s>>>(*sp, n, dWL, dWR, dn, reflective,
                                                          dhalf, dflux, dcode);
     }
+    sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }

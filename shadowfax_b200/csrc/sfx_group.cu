@@ -23,6 +23,7 @@ struct sfx_group {
     std::vector<sfx_group_entry> host_tab;
     sfx_group_dev dev{};
     sfx_dev_error* d_err_out = nullptr;
+    int32_t* d_steps = nullptr; /* per-member step counters (after set_steps) */
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1;
 };
@@ -69,12 +70,23 @@ int upload_layout(sfx_group* g) {
 
 int run_steps(sfx_group* g, int nsteps, cudaStream_t s) {
     const sfx_solver_params* sp = sfx_ctx_params(g->ctx);
-    for(int t = 0; t < nsteps; ++t)
+    for(int t = 0; t < nsteps; ++t) {
         for(int ph = 0; ph < 3; ++ph) {
             int rc = sfx_split_group_phase(&g->dev, ph, sp, s);
             if(rc) return rc;
         }
+        if(g->d_steps) {
+            int rc = sfx_split_group_tick(&g->dev, s);
+            if(rc) return rc;
+        }
+    }
     return SFX_OK;
+}
+
+bool same_config(const sfx_config* a, const sfx_config* b) {
+    return a->dim == b->dim && a->solver == b->solver && a->precision == b->precision &&
+           a->gamma == b->gamma && a->tolerance == b->tolerance && a->cutoff == b->cutoff &&
+           a->device == b->device;
 }
 
 }  // namespace
@@ -86,7 +98,8 @@ extern "C" int sfx_group_create(sfx_ctx* ctx, int32_t n, sfx_mesh* const* meshes
     const sfx_config* cfg = sfx_ctx_config(ctx);
     if(cfg->precision != SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
     for(int i = 0; i < n; ++i) {
-        if(!meshes[i] || sfx_mesh_ctx(meshes[i]) != ctx || !(dt[i] > 0.)) return SFX_ERR_INVALID;
+        if(!meshes[i] || !(dt[i] > 0.)) return SFX_ERR_INVALID;
+        if(!same_config(sfx_ctx_config(sfx_mesh_ctx(meshes[i])), cfg)) return SFX_ERR_INVALID;
     }
     sfx_group* g = new(std::nothrow) sfx_group;
     if(!g) return SFX_ERR_NOMEM;
@@ -142,7 +155,9 @@ extern "C" int sfx_group_step(sfx_group* g, int32_t nsteps, int32_t use_graph,
             cudaGraph_t graph = nullptr;
             rc = cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             if(rc) return rc;
+            sfx_launch_capture(true);
             const int rr = run_steps(g, nsteps, s);
+            sfx_launch_capture(false);
             rc = cuda_ok(cudaStreamEndCapture(s, &graph));
             if(!rc && rr) rc = rr;
             if(!rc) rc = cuda_ok(cudaGraphInstantiate(&g->graph, graph, 0));
@@ -154,6 +169,11 @@ extern "C" int sfx_group_step(sfx_group* g, int32_t nsteps, int32_t use_graph,
             g->graph_steps = nsteps;
         }
         rc = cuda_ok(cudaGraphLaunch(g->graph, s));
+        if(!rc) {
+            int per_step = g->d_steps ? 1 : 0;
+            for(int p = 0; p < 3; ++p) per_step += g->dev.blocks[p] > 0;
+            sfx_count_launches(per_step * nsteps);
+        }
     } else {
         rc = run_steps(g, nsteps, s);
     }
@@ -162,6 +182,69 @@ extern "C" int sfx_group_step(sfx_group* g, int32_t nsteps, int32_t use_graph,
     const int nm = g->dev.n_meshes;
     std::vector<sfx_dev_error> e(nm);
     rc = sfx_split_group_collect(&g->dev, g->d_err_out, s);
+    if(!rc)
+        rc = cuda_ok(cudaMemcpyAsync(e.data(), g->d_err_out, sizeof(sfx_dev_error) * nm,
+                                     cudaMemcpyDeviceToHost, s));
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    if(rc) return rc;
+    int first = SFX_OK;
+    for(int i = 0; i < nm; ++i) {
+        int st = SFX_OK;
+        if(e[i].face_key != ~0ull)
+            st = (int)(e[i].face_key & 0xff);
+        else if(e[i].cell_key != ~0ull)
+            st = (int)(e[i].cell_key & 0xff);
+        mesh_status[i] = st;
+        if(st && !first) first = st;
+    }
+    return first;
+}
+
+extern "C" int sfx_group_step_timed(sfx_group* g, int32_t nsteps, float* phase_ms,
+                                    int32_t* launches) {
+    if(!g || nsteps < 0 || !phase_ms) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    const sfx_solver_params* sp = sfx_ctx_params(g->ctx);
+    cudaEvent_t ev[4];
+    int made = 0;
+    int rc = SFX_OK;
+    for(; made < 4 && !rc; ++made)
+        if(cudaEventCreate(&ev[made]) != cudaSuccess) rc = SFX_ERR_CUDA;
+    if(rc) made -= 1;
+    double acc[3] = {0., 0., 0.};
+    int nl = 0;
+    if(!rc) rc = sfx_split_group_reset(&g->dev, s);
+    for(int t = 0; t < nsteps && !rc; ++t) {
+        for(int ph = 0; ph < 3 && !rc; ++ph) {
+            cudaEventRecord(ev[ph], s);
+            rc = sfx_split_group_phase(&g->dev, ph, sp, s);
+            nl += 1;
+        }
+        cudaEventRecord(ev[3], s);
+        if(!rc && g->d_steps) {
+            rc = sfx_split_group_tick(&g->dev, s);
+            nl += 1;
+        }
+        if(!rc) rc = cuda_ok(cudaEventSynchronize(ev[3]));
+        for(int k = 0; k < 3 && !rc; ++k) {
+            float ms = 0.f;
+            rc = cuda_ok(cudaEventElapsedTime(&ms, ev[k], k < 2 ? ev[k + 1] : ev[3]));
+            acc[k] += ms;
+        }
+    }
+    if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
+    for(int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+    for(int k = 0; k < 3; ++k) phase_ms[k] = (float)acc[k];
+    if(launches) *launches = nl;
+    return rc;
+}
+
+extern "C" int sfx_group_status(sfx_group* g, int32_t* mesh_status) {
+    if(!g || !mesh_status) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    const int nm = g->dev.n_meshes;
+    std::vector<sfx_dev_error> e(nm);
+    int rc = sfx_split_group_collect(&g->dev, g->d_err_out, s);
     if(!rc)
         rc = cuda_ok(cudaMemcpyAsync(e.data(), g->d_err_out, sizeof(sfx_dev_error) * nm,
                                      cudaMemcpyDeviceToHost, s));
@@ -219,9 +302,37 @@ extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
     return rc ? rc : r2;
 }
 
+extern "C" int sfx_group_set_steps(sfx_group* g, const int32_t* steps) {
+    if(!g || !steps) return SFX_ERR_INVALID;
+    const int nm = g->dev.n_meshes;
+    for(int i = 0; i < nm; ++i)
+        if(steps[i] < 0) return SFX_ERR_INVALID;
+    if(!g->d_steps) {
+        int rc = cuda_ok(cudaMalloc((void**)&g->d_steps, sizeof(int32_t) * nm));
+        if(rc) return rc;
+        for(int i = 0; i < nm; ++i) g->host_tab[i].steps_left = g->d_steps + i;
+    }
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    int rc = cuda_ok(cudaMemcpyAsync(g->d_steps, steps, sizeof(int32_t) * nm,
+                                     cudaMemcpyHostToDevice, s));
+    if(rc) return rc;
+    return upload_layout(g); /* the table now points at the counters */
+}
+
+extern "C" int sfx_group_get_steps(sfx_group* g, int32_t* steps) {
+    if(!g || !steps) return SFX_ERR_INVALID;
+    if(!g->d_steps) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    int rc = cuda_ok(cudaMemcpyAsync(steps, g->d_steps, sizeof(int32_t) * g->dev.n_meshes,
+                                     cudaMemcpyDeviceToHost, s));
+    if(rc) return rc;
+    return cuda_ok(cudaStreamSynchronize(s));
+}
+
 extern "C" int sfx_group_free(sfx_group* g) {
     if(!g) return SFX_ERR_INVALID;
     drop_graph(g);
+    if(g->d_steps) cudaFree(g->d_steps);
     if(g->dev.tab) cudaFree(g->dev.tab);
     if(g->dev.pre) cudaFree(g->dev.pre);
     if(g->d_err_out) cudaFree(g->d_err_out);

@@ -77,11 +77,14 @@ struct sfx_dmesh {
     double* dqv;
 };
 
-/* one mesh of a launch group (device table entry) */
+/* one mesh of a launch group (device table entry); steps_left, when not
+ * NULL, is the member's remaining step count: the kernels skip a member at 0
+ * and a tick after each step counts it down */
 struct sfx_group_entry {
     sfx_dmesh m;
     float dt;
     int32_t pad;
+    int32_t* steps_left;
 };
 
 /* device view of a launch group: table of meshes and, per phase, the prefix
@@ -129,8 +132,15 @@ int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* strea
 int sfx_split_export_W(const sfx_dmesh* m, void* stream);
 /* per-face dQ (FP32) widened into dQf (FP64 SoA), for parity checks */
 int sfx_split_export_dQ(const sfx_dmesh* m, void* stream);
+/* kernel launch counter behind sfx_launch_count (sfx_api.cu).  Launches made
+ * while the calling thread captures a CUDA graph are not counted (the
+ * graph's kernels are counted when it is launched). */
+void sfx_count_launches(int n);
+void sfx_launch_capture(bool on);
 /* accessors of the C-ABI handles (sfx_api.cu) */
 sfx_dmesh* sfx_mesh_dev(sfx_mesh* m);
+/* status of the mesh's error record (waits for its stream) */
+int sfx_mesh_last_status(sfx_mesh* m, int32_t* bad_index);
 sfx_ctx* sfx_mesh_ctx(sfx_mesh* m);
 void* sfx_ctx_stream(sfx_ctx* c);
 const sfx_config* sfx_ctx_config(sfx_ctx* c);
@@ -141,6 +151,7 @@ int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out)
 int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                           void* stream);
 int sfx_split_group_reset(const sfx_group_dev* g, void* stream);
+int sfx_split_group_tick(const sfx_group_dev* g, void* stream);
 int sfx_split_group_collect(const sfx_group_dev* g, sfx_dev_error* d_out, void* stream);
 
 #endif

@@ -1,0 +1,504 @@
+/*
+ * Request server: continuous batching of static-mesh integrations on one GPU.
+ *
+ * Shadowfax integrates one simulation per job; this server turns the flux
+ * pass into a service.  Meshes are uploaded once into a device pool.  A
+ * request (pool mesh, initial state, solver, dt, step count) is queued by
+ * sfx_server_submit and admitted by the worker thread in arrival order while
+ * the device-memory budget and the slot count allow: its state is cloned
+ * onto the pool mesh's geometry (sfx_mesh_clone) and stays resident until it
+ * finishes.  Each scheduling round advances every admitted request by up to
+ * `chunk_steps` steps:
+ *   SFX_PREC_SPLIT  all requests of one (dimension, solver) class share one
+ *                   launch group (one launch per phase for all of them,
+ *                   captured in a CUDA graph); per-request step counters live
+ *                   on the device, so a request that finishes inside a chunk
+ *                   stops there while the others go on;
+ *   SFX_PREC_FP64   every request is stepped on its own (the per-request
+ *                   baseline).
+ * The classes run on their own streams and overlap on the device.  Requests
+ * that arrive while a round runs join at the next round.  Finished requests
+ * are downloaded to host memory, their device state is freed, and they wait
+ * for sfx_server_poll.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "sfx_internal.h"
+
+namespace {
+
+struct Request {
+    int64_t id = 0;
+    int32_t mesh_id = 0, solver = 0, nsteps = 0;
+    double dt = 0.;
+    std::vector<double> W0, W, Q;
+    double t_submit = 0., t_admit = 0., t_done = 0.;
+    int32_t status = SFX_OK, steps_done = 0;
+    int64_t face_steps = 0;
+    bool done = false;
+    sfx_mesh* inst = nullptr;
+    int64_t bytes = 0;
+    int32_t remaining = 0;
+    int32_t chunk = 0; /* steps launched this round (FP64 mode) */
+};
+
+struct PoolMesh {
+    sfx_mesh* mesh = nullptr;
+    int dim = 0;
+    int32_t n_cells = 0;
+    int64_t active_faces = 0;
+    int64_t clone_bytes = 0;
+};
+
+struct Class {
+    sfx_ctx* ctx = nullptr;
+    std::vector<Request*> members;
+    sfx_group* group = nullptr;
+    bool dirty = false;
+    int reused = 0; /* rounds the current group has run unchanged */
+};
+
+}  // namespace
+
+struct sfx_server {
+    sfx_server_config cfg;
+    sfx_ctx* pool_ctx[2] = {nullptr, nullptr};
+    Class cls[2][2]; /* [dim - 2][solver] */
+    std::vector<std::unique_ptr<PoolMesh>> pool;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queue;
+    std::unordered_map<int64_t, Request*> reqs;
+    int64_t next_id = 1;
+    int64_t n_submitted = 0, n_admitted = 0, n_completed = 0, n_failed = 0;
+    int64_t face_steps = 0, rounds = 0;
+    int64_t bytes_in_use = 0;
+    int active = 0;
+    bool stop = false;
+    std::thread worker;
+    std::chrono::steady_clock::time_point t0;
+};
+
+namespace {
+
+double now_s(const sfx_server* s) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+sfx_config make_cfg(const sfx_server* s, int dim, int solver) {
+    sfx_config c;
+    std::memset(&c, 0, sizeof c);
+    c.dim = dim;
+    c.solver = solver;
+    c.gamma = s->cfg.gamma;
+    c.tolerance = s->cfg.tolerance;
+    c.cutoff = s->cfg.cutoff;
+    c.precision = s->cfg.precision;
+    c.device = s->cfg.device;
+    return c;
+}
+
+/* worker thread only: request leaves the device */
+void finish(sfx_server* s, Request* r, int status) {
+    if(r->inst) {
+        const int64_t n = sfx_mesh_dev(r->inst)->n_cells;
+        const int S = sfx_mesh_dev(r->inst)->S;
+        r->W.resize((size_t)n * S);
+        r->Q.resize((size_t)n * S);
+        int rc = sfx_state_download(r->inst, r->W.data(), r->Q.data());
+        if(rc && status == SFX_OK) status = rc;
+        sfx_mesh_free(r->inst);
+        r->inst = nullptr;
+    }
+    PoolMesh* pm;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        pm = s->pool[r->mesh_id].get();
+    }
+    r->steps_done = r->nsteps - r->remaining;
+    r->face_steps = (int64_t)r->steps_done * pm->active_faces;
+    r->status = status;
+    r->t_done = now_s(s);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->bytes_in_use -= r->bytes;
+    s->active -= 1;
+    r->done = true;
+    if(status == SFX_OK) {
+        s->n_completed += 1;
+        s->face_steps += r->face_steps;
+    } else {
+        s->n_failed += 1;
+    }
+    s->cv_done.notify_all();
+}
+
+/* admit queued requests in arrival order while budget and slots allow */
+void admit(sfx_server* s) {
+    for(;;) {
+        Request* r;
+        PoolMesh* pm;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if(s->stop || s->queue.empty() || s->active >= s->cfg.max_active) return;
+            r = s->queue.front();
+            pm = s->pool[r->mesh_id].get();
+            if(s->bytes_in_use + pm->clone_bytes > s->cfg.memory_budget && s->active > 0) return;
+            s->queue.pop_front();
+            s->bytes_in_use += pm->clone_bytes;
+            s->active += 1;
+            s->n_admitted += 1;
+        }
+        r->bytes = pm->clone_bytes;
+        r->remaining = r->nsteps;
+        r->t_admit = now_s(s);
+        Class& c = s->cls[pm->dim - 2][r->solver];
+        int rc = sfx_mesh_clone(c.ctx, pm->mesh, &r->inst);
+        if(!rc) rc = sfx_state_upload_W(r->inst, r->W0.data());
+        std::vector<double>().swap(r->W0);
+        if(rc) {
+            finish(s, r, rc);
+            continue;
+        }
+        if(r->nsteps == 0) {
+            finish(s, r, SFX_OK);
+            continue;
+        }
+        c.members.push_back(r);
+        c.dirty = true;
+    }
+}
+
+int rebuild_group(sfx_server* s, Class& c) {
+    if(c.group) sfx_group_free(c.group);
+    c.group = nullptr;
+    c.dirty = false;
+    if(c.members.empty()) return SFX_OK;
+    std::vector<sfx_mesh*> ms;
+    std::vector<double> dts;
+    std::vector<int32_t> steps;
+    for(Request* r : c.members) {
+        ms.push_back(r->inst);
+        dts.push_back(r->dt);
+        steps.push_back(r->remaining);
+    }
+    int rc = sfx_group_create(c.ctx, (int32_t)ms.size(), ms.data(), dts.data(), &c.group);
+    if(!rc) rc = sfx_group_set_steps(c.group, steps.data());
+    return rc;
+}
+
+void round_split(sfx_server* s) {
+    const int chunk = std::max(1, s->cfg.chunk_steps);
+    /* rebuild the groups whose membership changed first: freeing device
+     * memory waits for the whole device, so it must not sit between the
+     * launches of the classes */
+    for(auto& row : s->cls)
+        for(Class& c : row) {
+            if(c.members.empty()) {
+                if(c.group) sfx_group_free(c.group);
+                c.group = nullptr;
+                continue;
+            }
+            if(c.dirty || !c.group) {
+                c.reused = 0;
+                int rc = rebuild_group(s, c);
+                if(rc) {
+                    for(Request* r : c.members) finish(s, r, rc);
+                    c.members.clear();
+                }
+            } else {
+                c.reused += 1;
+            }
+        }
+    /* launch every class, then collect, so the classes overlap; a group
+     * that survives a round is replayed as a CUDA graph from then on */
+    for(auto& row : s->cls)
+        for(Class& c : row) {
+            if(c.members.empty() || !c.group) continue;
+            int rc = sfx_group_step(c.group, chunk, c.reused > 0, nullptr);
+            if(rc) {
+                for(Request* r : c.members) finish(s, r, rc);
+                c.members.clear();
+                c.dirty = true;
+            }
+        }
+    for(auto& row : s->cls)
+        for(Class& c : row) {
+            if(c.members.empty() || !c.group) continue;
+            const size_t nm = c.members.size();
+            std::vector<int32_t> left(nm), st(nm);
+            int rc = sfx_group_get_steps(c.group, left.data());
+            if(!rc) {
+                const int rs = sfx_group_status(c.group, st.data());
+                /* a member's failure comes back in st; other codes are the
+                 * group's own */
+                bool any = false;
+                for(int32_t v : st) any = any || v != SFX_OK;
+                if(rs && !any) rc = rs;
+            }
+            std::vector<Request*> keep;
+            for(size_t i = 0; i < nm; ++i) {
+                Request* r = c.members[i];
+                if(rc) {
+                    finish(s, r, rc);
+                    continue;
+                }
+                r->remaining = left[i];
+                if(st[i] != SFX_OK)
+                    finish(s, r, st[i]);
+                else if(left[i] == 0)
+                    finish(s, r, SFX_OK);
+                else
+                    keep.push_back(r);
+            }
+            if(keep.size() != nm) c.dirty = true;
+            c.members.swap(keep);
+        }
+}
+
+void round_fp64(sfx_server* s) {
+    const int chunk = std::max(1, s->cfg.chunk_steps);
+    for(auto& row : s->cls)
+        for(Class& c : row)
+            for(Request* r : c.members) {
+                r->chunk = std::min(chunk, r->remaining);
+                if(sfx_step(r->inst, r->dt, r->chunk, nullptr) != SFX_OK) r->chunk = -1;
+            }
+    for(auto& row : s->cls)
+        for(Class& c : row) {
+            if(c.members.empty()) continue;
+            sfx_ctx_synchronize(c.ctx);
+            std::vector<Request*> keep;
+            for(Request* r : c.members) {
+                int32_t bad = -1;
+                int st = r->chunk < 0 ? SFX_ERR_CUDA : sfx_mesh_last_status(r->inst, &bad);
+                if(r->chunk > 0) r->remaining -= r->chunk;
+                if(st != SFX_OK)
+                    finish(s, r, st);
+                else if(r->remaining == 0)
+                    finish(s, r, SFX_OK);
+                else
+                    keep.push_back(r);
+            }
+            c.members.swap(keep);
+        }
+}
+
+void worker_main(sfx_server* s) {
+    cudaSetDevice(s->cfg.device);
+    for(;;) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if(s->stop) break;
+        }
+        admit(s);
+        int active;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            active = s->active;
+        }
+        if(active == 0) {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(20),
+                                [&] { return s->stop || !s->queue.empty(); });
+            continue;
+        }
+        if(s->cfg.precision == SFX_PREC_SPLIT)
+            round_split(s);
+        else
+            round_fp64(s);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->rounds += 1;
+    }
+}
+
+}  // namespace
+
+extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out) {
+    if(!cfg || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    if(cfg->precision != SFX_PREC_SPLIT && cfg->precision != SFX_PREC_FP64) return SFX_ERR_INVALID;
+    if(cfg->max_active <= 0 || cfg->memory_budget <= 0 || cfg->chunk_steps <= 0)
+        return SFX_ERR_INVALID;
+    sfx_server* s = new(std::nothrow) sfx_server;
+    if(!s) return SFX_ERR_NOMEM;
+    s->cfg = *cfg;
+    s->t0 = std::chrono::steady_clock::now();
+    int rc = SFX_OK;
+    for(int d = 0; d < 2 && !rc; ++d) {
+        sfx_config pc = make_cfg(s, d + 2, SFX_SOLVER_HLLC);
+        rc = sfx_ctx_create(&pc, &s->pool_ctx[d]);
+        for(int k = 0; k < 2 && !rc; ++k) {
+            sfx_config cc = make_cfg(s, d + 2, k);
+            rc = sfx_ctx_create(&cc, &s->cls[d][k].ctx);
+        }
+    }
+    if(rc) {
+        sfx_server_shutdown(s);
+        return rc;
+    }
+    s->worker = std::thread(worker_main, s);
+    *out = s;
+    return SFX_OK;
+}
+
+extern "C" int sfx_server_add_mesh(sfx_server* s, const sfx_mesh_desc* desc, int32_t* mesh_id) {
+    if(!s || !desc || !mesh_id) return SFX_ERR_INVALID;
+    if(desc->dim != 2 && desc->dim != 3) return SFX_ERR_INVALID;
+    std::unique_ptr<PoolMesh> pm(new(std::nothrow) PoolMesh);
+    if(!pm) return SFX_ERR_NOMEM;
+    int rc = sfx_mesh_upload(s->pool_ctx[desc->dim - 2], desc, &pm->mesh);
+    if(rc) return rc;
+    pm->dim = desc->dim;
+    pm->n_cells = desc->n_cells;
+    for(int32_t f = 0; f < desc->n_faces; ++f) pm->active_faces += desc->face_area[f] != 0.;
+    pm->clone_bytes = sfx_mesh_clone_bytes(pm->mesh, s->cfg.precision);
+    std::lock_guard<std::mutex> lk(s->mu);
+    *mesh_id = (int32_t)s->pool.size();
+    s->pool.push_back(std::move(pm));
+    return SFX_OK;
+}
+
+extern "C" int sfx_server_submit(sfx_server* s, int32_t mesh_id, const double* W0,
+                                 int32_t solver, double dt, int32_t nsteps,
+                                 int64_t* request_id) {
+    if(!s || !W0 || !request_id || nsteps < 0 || !(dt > 0.)) return SFX_ERR_INVALID;
+    if(solver != SFX_SOLVER_EXACT && solver != SFX_SOLVER_HLLC) return SFX_ERR_UNSUPPORTED;
+    Request* r = new(std::nothrow) Request;
+    if(!r) return SFX_ERR_NOMEM;
+    int64_t n;
+    int S;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if(s->stop) {
+            delete r;
+            return SFX_ERR_CLOSED;
+        }
+        if(mesh_id < 0 || mesh_id >= (int32_t)s->pool.size()) {
+            delete r;
+            return SFX_ERR_INVALID;
+        }
+        n = s->pool[mesh_id]->n_cells;
+        S = s->pool[mesh_id]->dim + 2;
+    }
+    r->W0.assign(W0, W0 + (size_t)n * S);
+    r->mesh_id = mesh_id;
+    r->solver = solver;
+    r->dt = dt;
+    r->nsteps = nsteps;
+    r->t_submit = now_s(s);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        s->reqs[r->id] = r;
+        s->queue.push_back(r);
+        s->n_submitted += 1;
+        *request_id = r->id;
+    }
+    s->cv_work.notify_one();
+    return SFX_OK;
+}
+
+extern "C" int sfx_server_poll(sfx_server* s, int64_t id, double* W, double* Q,
+                               sfx_request_info* info) {
+    if(!s) return SFX_ERR_INVALID;
+    Request* r;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        if(it == s->reqs.end()) return SFX_ERR_INVALID;
+        r = it->second;
+        if(!r->done) return SFX_ERR_NOT_READY;
+        s->reqs.erase(it);
+    }
+    if(W && !r->W.empty()) std::memcpy(W, r->W.data(), r->W.size() * sizeof(double));
+    if(Q && !r->Q.empty()) std::memcpy(Q, r->Q.data(), r->Q.size() * sizeof(double));
+    if(info) {
+        info->status = r->status;
+        info->steps_done = r->steps_done;
+        info->mesh_id = r->mesh_id;
+        info->solver = r->solver;
+        info->t_submit = r->t_submit;
+        info->t_admit = r->t_admit;
+        info->t_done = r->t_done;
+        info->face_steps = r->face_steps;
+    }
+    const int st = r->status;
+    delete r;
+    return st;
+}
+
+extern "C" int sfx_server_drain(sfx_server* s, double timeout_s) {
+    if(!s) return SFX_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto idle = [&] { return s->queue.empty() && s->active == 0; };
+    if(timeout_s <= 0.) {
+        s->cv_done.wait(lk, idle);
+        return SFX_OK;
+    }
+    return s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), idle)
+                   ? SFX_OK
+                   : SFX_ERR_NOT_READY;
+}
+
+extern "C" int sfx_server_stats_get(sfx_server* s, sfx_server_stats* st) {
+    if(!s || !st) return SFX_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    st->submitted = s->n_submitted;
+    st->admitted = s->n_admitted;
+    st->completed = s->n_completed;
+    st->failed = s->n_failed;
+    st->active = s->active;
+    st->queued = (int64_t)s->queue.size();
+    st->face_steps = s->face_steps;
+    st->bytes_in_use = s->bytes_in_use;
+    st->rounds = s->rounds;
+    st->now = now_s(s);
+    return SFX_OK;
+}
+
+extern "C" int sfx_server_shutdown(sfx_server* s) {
+    if(!s) return SFX_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if(s->worker.joinable()) s->worker.join();
+    for(auto& row : s->cls)
+        for(Class& c : row) {
+            if(c.group) sfx_group_free(c.group);
+            for(Request* r : c.members)
+                if(r->inst) {
+                    sfx_mesh_free(r->inst);
+                    r->inst = nullptr;
+                }
+            c.members.clear();
+        }
+    for(auto& kv : s->reqs) {
+        if(kv.second->inst) sfx_mesh_free(kv.second->inst);
+        delete kv.second;
+    }
+    s->reqs.clear();
+    for(auto& pm : s->pool)
+        if(pm->mesh) sfx_mesh_free(pm->mesh);
+    s->pool.clear();
+    for(auto& row : s->cls)
+        for(Class& c : row)
+            if(c.ctx) sfx_ctx_destroy(c.ctx);
+    for(sfx_ctx* c : s->pool_ctx)
+        if(c) sfx_ctx_destroy(c);
+    delete s;
+    return SFX_OK;
+}

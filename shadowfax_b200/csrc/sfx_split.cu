@@ -1097,10 +1097,17 @@ __device__ __forceinline__ int group_mesh_of_block(const int* __restrict__ pre, 
     return s_mesh;
 }
 
+/* a member whose step counter reached 0 is done: all its blocks return */
+__device__ __forceinline__ bool member_done(const sfx_group_entry* tab, int mi) {
+    const int32_t* sl = tab[mi].steps_left;
+    return sl && *(volatile const int32_t*)sl <= 0;
+}
+
 template <int D, int LPC>
 __global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
                                                      int nm) {
     const int mi = group_mesh_of_block(pre, nm);
+    if(member_done(tab, mi)) return;
     sgrad_body<D, LPC>(tab[mi].m, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
@@ -1109,6 +1116,7 @@ __global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
     const int mi = group_mesh_of_block(pre, nm);
+    if(member_done(tab, mi)) return;
     sfaces_body<D, SOLVER>(tab[mi].m, sp, tab[mi].dt,
                            (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
@@ -1117,7 +1125,16 @@ template <int D, int LPC>
 __global__ void __launch_bounds__(256) k_group_sapply(const sfx_group_entry* tab, const int* pre,
                                                       int nm, double gamma) {
     const int mi = group_mesh_of_block(pre, nm);
+    if(member_done(tab, mi)) return;
     sapply_body<D, LPC>(tab[mi].m, gamma, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+}
+
+/* after a step: count the members' remaining steps down */
+__global__ void k_group_tick(const sfx_group_entry* tab, int nm) {
+    const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if(mi >= nm) return;
+    int32_t* sl = tab[mi].steps_left;
+    if(sl && *sl > 0) *sl -= 1;
 }
 
 __global__ void k_group_reset_err(const sfx_group_entry* tab, int nm) {
@@ -1154,14 +1171,17 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
             k_group_sapply<D, LPC><<<g->blocks[2], 256, 0, s>>>(g->tab, g->pre + 2 * (nm + 1),
                                                                  nm, sp->gamma);
     }
+    if(g->blocks[phase]) sfx_count_launches(1);
     return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
 }
 
 inline int grid_for(long long n, int b) {
     return (int)((n + b - 1) / b);
 }
-inline int cuda_status(cudaError_t e) {
-    return e == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+/* status of the n kernel launches just made, counted for sfx_launch_count */
+inline int launched(int n) {
+    sfx_count_launches(n);
+    return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
 }
 
 }  // namespace
@@ -1178,7 +1198,7 @@ int sfx_split_prepare(const sfx_dmesh* m, void* stream) {
         k_prep_cells<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
     else
         k_prep_cells<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
-    return cuda_status(cudaGetLastError());
+    return launched(m->n_faces ? 2 : 1);
 }
 
 int sfx_split_load_state(const sfx_dmesh* m, void* stream) {
@@ -1187,7 +1207,7 @@ int sfx_split_load_state(const sfx_dmesh* m, void* stream) {
         k_load_state<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
     else
         k_load_state<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 int sfx_split_export_W(const sfx_dmesh* m, void* stream) {
@@ -1196,7 +1216,7 @@ int sfx_split_export_W(const sfx_dmesh* m, void* stream) {
         k_export_W<3><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
     else
         k_export_W<2><<<grid_for(m->n_cells, 256), 256, 0, s>>>(*m);
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
@@ -1206,7 +1226,7 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
         k_export_dQ<3><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
     else
         k_export_dQ<2><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 /* the per-cell kernels for the mesh's lanes-per-cell setting */
@@ -1230,7 +1250,7 @@ int cells_phase(const sfx_dmesh* m, int phase, double gamma, cudaStream_t s) {
         return SFX_ERR_INVALID;
     }
 #undef SFX_LANES_CASE
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 int sfx_split_gradients(const sfx_dmesh* m, void* stream) {
@@ -1254,7 +1274,7 @@ int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, 
         else
             k_sfaces<2, SFX_SOLVER_HLLC><<<G, 256, 0, s>>>(*m, *sp, fdt);
     }
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
@@ -1293,14 +1313,20 @@ int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_pa
     }
 }
 
+int sfx_split_group_tick(const sfx_group_dev* g, void* stream) {
+    k_group_tick<<<grid_for(g->n_meshes, 128), 128, 0, (cudaStream_t)stream>>>(g->tab,
+                                                                            g->n_meshes);
+    return launched(1);
+}
+
 int sfx_split_group_reset(const sfx_group_dev* g, void* stream) {
     k_group_reset_err<<<grid_for(g->n_meshes, 128), 128, 0, (cudaStream_t)stream>>>(g->tab,
                                                                                   g->n_meshes);
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }
 
 int sfx_split_group_collect(const sfx_group_dev* g, sfx_dev_error* d_out, void* stream) {
     k_group_collect_err<<<grid_for(g->n_meshes, 128), 128, 0, (cudaStream_t)stream>>>(
             g->tab, g->n_meshes, d_out);
-    return cuda_status(cudaGetLastError());
+    return launched(1);
 }

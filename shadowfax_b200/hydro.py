@@ -147,6 +147,21 @@ class FluxPass:
         self.h = h
         self.S = mesh.dim + 2
 
+    def clone(self, ctx: Context | None = None) -> "FluxPass":
+        """a new state on this mesh's device geometry (sfx_mesh_clone): the
+        clone owns only W, Q and per-step scratch; this FluxPass must outlive
+        it"""
+        ctx = ctx or self.ctx
+        h = C.c_void_p()
+        L.check(L.lib().sfx_mesh_clone(ctx.h, self.h, C.byref(h)), "sfx_mesh_clone")
+        fp = FluxPass.__new__(FluxPass)
+        fp.ctx, fp.mesh, fp.h, fp.S = ctx, self.mesh, h, self.S
+        fp.base = self
+        return fp
+
+    def clone_bytes(self, precision: int) -> int:
+        return int(L.lib().sfx_mesh_clone_bytes(self.h, precision))
+
     def close(self):
         if self.h:
             L.lib().sfx_mesh_free(self.h)
@@ -265,6 +280,31 @@ class Group:
 
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_group_set_lanes(self.h, lanes), "sfx_group_set_lanes")
+
+    def set_steps(self, steps):
+        """per-member remaining step counts on the device: a member at 0 is
+        skipped, the others count down each step"""
+        st = np.ascontiguousarray(steps, np.int32)
+        L.check(L.lib().sfx_group_set_steps(self.h, L.iptr(st)), "sfx_group_set_steps")
+
+    def get_steps(self) -> np.ndarray:
+        st = np.zeros(len(self.members), np.int32)
+        L.check(L.lib().sfx_group_get_steps(self.h, L.iptr(st)), "sfx_group_get_steps")
+        return st
+
+    def status(self) -> np.ndarray:
+        st = np.zeros(len(self.members), np.int32)
+        L.lib().sfx_group_status(self.h, L.iptr(st))
+        return st
+
+    def step_timed(self, nsteps: int) -> tuple[np.ndarray, int]:
+        """nsteps without a graph; (ms[gradients, faces, update] summed over
+        the steps, kernels launched)"""
+        ms = (C.c_float * 3)()
+        nl = C.c_int32(0)
+        L.check(L.lib().sfx_group_step_timed(self.h, nsteps, ms, C.byref(nl)),
+                "sfx_group_step_timed")
+        return np.array(list(ms), dtype=np.float64), nl.value
 
     def step(self, nsteps: int = 1, graph: bool = True, status: bool = True):
         """nsteps for every member; returns the per-member status array"""

@@ -121,3 +121,98 @@ def batch2d(count: int = 1024, seed: int = 4, solver: str = "HLLC", nsteps: int 
         futs = [ex.submit(step_state2d, int(n), seed * 100_000 + j, solver, nsteps)
                 for j, n in enumerate(sizes)]
         return [f.result() for f in futs]
+
+
+# ---- c5: the request stream --------------------------------------------
+
+SERVE_LO, SERVE_HI = 1_000, 1_000_000
+
+
+def serve_pool_sizes(k: int = 10, lo: int = SERVE_LO, hi: int = SERVE_HI) -> np.ndarray:
+    """pool mesh sizes: the geometric centres of k equal bins of log N over
+    [lo, hi]; a request's log-uniform N is served by its bin's mesh, so the
+    pool keeps the distribution's mean to about 2% (mean of the centres
+    1.42e5 for k = 10 against 1.45e5)"""
+    a, b = math.log(lo), math.log(hi)
+    return np.exp(a + (b - a) * (np.arange(k) + 0.5) / k).round().astype(np.int64)
+
+
+def random_field_state(mesh: Mesh, seed: int) -> np.ndarray:
+    """the c3 state on any mesh: ln rho ~ N(-1/2, 1) (mean rho 1), p = 1,
+    each velocity component ~ N(0, 1)"""
+    n, D = mesh.n_cells, mesh.dim
+    rng = np.random.Generator(np.random.PCG64(seed))
+    W = np.zeros((n, D + 2))
+    W[:, 0] = np.exp(rng.normal(-0.5, 1.0, n))
+    W[:, 1:D + 1] = rng.normal(0.0, 1.0, (n, D))
+    W[:, D + 1] = 1.0
+    return W
+
+
+@dataclass
+class ServePool:
+    """pre-tessellated meshes of the stream (periodic unit box) with a few
+    random-field states each and their CFL-0.4 time steps; mesh (dim, bin)
+    sits at index (dim - 2) * k + bin (None where not built)"""
+    k: int
+    meshes: list
+    states: list        # states[mesh] = [W, ...]
+    dts: list           # dts[mesh] = [dt, ...]
+
+
+@dataclass
+class ServeRequest:
+    t: float            # arrival, seconds after the stream starts
+    mesh: int           # pool mesh index: (dim - 2) * k + size bin
+    state: int          # state index of that mesh
+    solver: str
+    nsteps: int
+
+
+def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
+               workers: int = 0) -> ServePool:
+    """the pool meshes (all 2k, or the indices in `only`), tessellated
+    concurrently, largest first"""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    sizes = serve_pool_sizes(k)
+    jobs = [j for j in range(2 * k) if only is None or j in only]
+    workers = workers or max(1, min(4, (os.cpu_count() or 4) // 4))
+
+    def one(j):
+        dim, b = 2 + j // k, j % k
+        n = int(sizes[b])
+        pos = random_generators(n, dim, seed * 1_000_003 + dim * 1000 + b)
+        mesh = build_voronoi(pos, periodic=True)
+        Ws = [random_field_state(mesh, seed * 7919 + dim * 1000 + b * 10 + s)
+              for s in range(states_per_mesh)]
+        return mesh, Ws, [cfl_dt(mesh, W) for W in Ws]
+
+    order = sorted(jobs, key=lambda j: -int(sizes[j % k]) * (3 if j >= k else 1))
+    meshes, states, dts = [None] * (2 * k), [None] * (2 * k), [None] * (2 * k)
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for j, (m, Ws, ds) in zip(order, ex.map(one, order)):
+            meshes[j], states[j], dts[j] = m, Ws, ds
+    return ServePool(k, meshes, states, dts)
+
+
+def serve_stream(k: int = 10, rate: float = 200.0, duration: float = 60.0, seed: int = 5,
+                 frac2d: float = 0.7, steps: tuple = (10, 200), states_per_mesh: int = 2,
+                 count: int | None = None) -> list:
+    """config 5: Poisson arrivals at `rate` per second for `duration`
+    seconds (or the first `count` arrivals); 70% 2D / 30% 3D; N log-uniform
+    in [1e3, 1e6] (served by the pool mesh of its bin); step count uniform on
+    {10..200}; exact or HLLC 50/50"""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if (count is None and t >= duration) or (count is not None and len(out) >= count):
+            break
+        dim = 2 if rng.random() < frac2d else 3
+        b = min(k - 1, int(rng.random() * k))    # log N uniform -> equal bins
+        si = int(rng.integers(states_per_mesh))
+        solver = "Exact" if rng.random() < 0.5 else "HLLC"
+        nsteps = int(rng.integers(steps[0], steps[1] + 1))
+        out.append(ServeRequest(t, (dim - 2) * k + b, si, solver, nsteps))
+    return out

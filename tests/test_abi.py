@@ -48,3 +48,19 @@ def test_branch_code_layout_matches_oracle():
         va = re.search(rf"#define SFX_BRANCH_{a} (.+)", h).group(1).strip()
         vb = re.search(rf"#define SFXB_{b} (.+)", o).group(1).strip()
         assert eval(va) == eval(vb), (a, va, vb)
+
+
+def test_server_rejects_bad_config():
+    """argument checks run before any device work"""
+    import ctypes as C
+    from shadowfax_b200 import _lib as L
+    for kw in ({"precision": 7}, {"max_active": 0}, {"memory_budget": 0}, {"chunk_steps": 0}):
+        base = dict(device=0, precision=1, gamma=5 / 3, tolerance=1e-8, cutoff=-5.0,
+                    memory_budget=1 << 30, max_active=16, chunk_steps=4)
+        base.update(kw)
+        cfg = L.sfx_server_config(**base)
+        h = C.c_void_p()
+        assert L.lib().sfx_server_create(C.byref(cfg), C.byref(h)) == L.SFX_ERR_INVALID
+        assert not h.value
+    assert L.lib().sfx_server_poll(None, 1, None, None, None) == L.SFX_ERR_INVALID
+    assert L.lib().sfx_server_shutdown(None) == L.SFX_ERR_INVALID
