@@ -452,92 +452,124 @@ __device__ __forceinline__ void spredict(float gamma, float hdt, float* Wt, cons
     }
 }
 
-/* HLLC (HLLCRiemannSolver.cpp:258-403) in FP32; the vacuum branch
- * (HLLCRiemannSolver.cpp:44-209) samples the exact vacuum solution */
-template <int D>
-__device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflective,
-                      SFlux<D>& F) {
+/* HLLC (HLLCRiemannSolver.cpp:258-403) in precision T; the vacuum branch
+ * (HLLCRiemannSolver.cpp:44-209) samples the exact vacuum solution.
+ *
+ * The wave speeds S_K = u_K -+ a_K q_K are formed as
+ * a_K q_K = sqrt(gamma / rho_K (p_K + (gamma+1)/(2 gamma) (pstar - p_K)))
+ * (the same quantity as the reference's a_K sqrt(1 + (gamma+1)/(2 gamma)
+ * (pstar / p_K - 1)), without the ratio pstar / p_K): a predicted face
+ * pressure far below the cell pressures (down to FP32 subnormals near the
+ * 1e-30 floor) would overflow that ratio in FP32, and 0 * inf in S_star then
+ * gives NaN.  The FP64 pass keeps the reference's form. */
+template <typename T>
+struct RT;
+template <>
+struct RT<float> {
+    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float pow_(float x, float y) { return powf(x, y); }
+    static __device__ __forceinline__ float max_(float x, float y) { return fmaxf(x, y); }
+};
+template <>
+struct RT<double> {
+    static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double pow_(double x, double y) { return pow(x, y); }
+    static __device__ __forceinline__ double max_(double x, double y) { return fmax(x, y); }
+};
+
+template <int D, typename T>
+struct TFlux {
+    T m, mv[D], P, E;
+};
+
+template <int D, typename T>
+__device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* n,
+                                      bool reflective, TFlux<D, T>& F) {
+    using R = RT<T>;
     constexpr int S = D + 2;
-    F.m = 0.f;
-    F.P = 0.f;
-    F.E = 0.f;
+    const T zero = T(0), one = T(1), two = T(2), half = T(0.5);
+    F.m = zero;
+    F.P = zero;
+    F.E = zero;
 #pragma unroll
-    for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
-    if(WL[0] == 0.f && (reflective || WR[0] == 0.f)) return;
-    float uL = 0.f, uR = 0.f;
+    for(int l = 0; l < D; ++l) F.mv[l] = zero;
+    if(WL[0] == zero && (reflective || WRin[0] == zero)) return;
+    /* the reflective right state is the left state with its normal velocity
+     * reversed (only u_R enters below) */
+    const T* WR = reflective ? WL : WRin;
+    T uL = zero, uR = zero;
 #pragma unroll
-    for(int l = 0; l < D; ++l) {
-        uL += WL[1 + l] * n[l];
-        uR += WR[1 + l] * n[l];
-    }
+    for(int l = 0; l < D; ++l) uL += WL[1 + l] * n[l];
     if(reflective) {
-#pragma unroll
-        for(int k = 0; k < S; ++k) WR[k] = WL[k];
         uR = -uL;
+    } else {
+#pragma unroll
+        for(int l = 0; l < D; ++l) uR += WR[1 + l] * n[l];
     }
-    const float gm1 = g - 1.f;
-    const float aL = WL[0] != 0.f ? sqrtf(g * WL[D + 1] / WL[0]) : 0.f;
-    const float aR = WR[0] != 0.f ? sqrtf(g * WR[D + 1] / WR[0]) : 0.f;
-    if(WL[0] == 0.f || WR[0] == 0.f || 2.f * (aL + aR) / gm1 <= uR - uL) {
+    const T gm1 = g - one;
+    const T aL = WL[0] != zero ? R::sqrt_(g * WL[D + 1] / WL[0]) : zero;
+    const T aR = WR[0] != zero ? R::sqrt_(g * WR[D + 1] / WR[0]) : zero;
+    if(WL[0] == zero || WR[0] == zero || two * (aL + aR) / gm1 <= uR - uL) {
         /* exact vacuum solution at x/t = 0 */
-        float sol[S], vhalf = 0.f;
-        const float tdgp1 = 2.f / (g + 1.f), gm1dgp1 = gm1 / (g + 1.f);
+        T sol[S], vhalf = zero;
+        const T tdgp1 = two / (g + one), gm1dgp1 = gm1 / (g + one);
         bool vac = false, fan = false;
-        const float* Ws = WL;
-        if(WR[0] == 0.f) {
+        const T* Ws = WL;
+        if(WR[0] == zero) {
             Ws = WL;
             if(aL > uL) {
-                if(uL + 2.f * aL / gm1 > 0.f) {
-                    const float base = tdgp1 + gm1dgp1 / aL * uL;
-                    vhalf = tdgp1 * (aL + 0.5f * gm1 * uL) - uL;
+                if(uL + two * aL / gm1 > zero) {
+                    /* base > 0 in exact arithmetic on this branch */
+                    const T base = R::max_(zero, tdgp1 + gm1dgp1 / aL * uL);
+                    vhalf = tdgp1 * (aL + half * gm1 * uL) - uL;
 #pragma unroll
                     for(int k = 0; k < S; ++k) sol[k] = WL[k];
-                    sol[0] = WL[0] * powf(base, 2.f / gm1);
-                    sol[D + 1] = WL[D + 1] * powf(base, 2.f * g / gm1);
+                    sol[0] = WL[0] * R::pow_(base, two / gm1);
+                    sol[D + 1] = WL[D + 1] * R::pow_(base, two * g / gm1);
                     fan = true;
                 } else {
                     vac = true;
                 }
             }
-        } else if(WL[0] == 0.f) {
+        } else if(WL[0] == zero) {
             Ws = WR;
             if(-uR < aR) {
-                if(uR - 2.f * aR / gm1 >= 0.f) {
+                if(uR - two * aR / gm1 >= zero) {
                     vac = true;
                 } else {
-                    const float base = tdgp1 - gm1dgp1 / aR * uR;
-                    vhalf = tdgp1 * (-aR + 0.5f * gm1 * uR) - uR;
+                    const T base = R::max_(zero, tdgp1 - gm1dgp1 / aR * uR);
+                    vhalf = tdgp1 * (-aR + half * gm1 * uR) - uR;
 #pragma unroll
                     for(int k = 0; k < S; ++k) sol[k] = WR[k];
-                    sol[0] = WR[0] * powf(base, 2.f / gm1);
-                    sol[D + 1] = WR[D + 1] * powf(base, 2.f * g / gm1);
+                    sol[0] = WR[0] * R::pow_(base, two / gm1);
+                    sol[D + 1] = WR[D + 1] * R::pow_(base, two * g / gm1);
                     fan = true;
                 }
             }
         } else {
-            const float SR = uR - 2.f * aR / gm1, SL = uL + 2.f * aL / gm1;
-            if(SR > 0.f && SL < 0.f) {
+            const T SR = uR - two * aR / gm1, SL = uL + two * aL / gm1;
+            if(SR > zero && SL < zero) {
                 vac = true;
-            } else if(SL >= 0.f) {
+            } else if(SL >= zero) {
                 Ws = WL;
                 if(aL > uL) {
-                    const float base = tdgp1 + gm1dgp1 / aL * uL;
-                    vhalf = tdgp1 * (aL + 0.5f * gm1 * uL) - uL;
+                    const T base = R::max_(zero, tdgp1 + gm1dgp1 / aL * uL);
+                    vhalf = tdgp1 * (aL + half * gm1 * uL) - uL;
 #pragma unroll
                     for(int k = 0; k < S; ++k) sol[k] = WL[k];
-                    sol[0] = WL[0] * powf(base, 2.f / gm1);
-                    sol[D + 1] = WL[D + 1] * powf(base, 2.f * g / gm1);
+                    sol[0] = WL[0] * R::pow_(base, two / gm1);
+                    sol[D + 1] = WL[D + 1] * R::pow_(base, two * g / gm1);
                     fan = true;
                 }
             } else {
                 Ws = WR;
                 if(-uR < aR) {
-                    const float base = tdgp1 - gm1dgp1 / aR * uR;
-                    vhalf = tdgp1 * (-aR + 0.5f * gm1 * uR) - uR;
+                    const T base = R::max_(zero, tdgp1 - gm1dgp1 / aR * uR);
+                    vhalf = tdgp1 * (-aR + half * gm1 * uR) - uR;
 #pragma unroll
                     for(int k = 0; k < S; ++k) sol[k] = WR[k];
-                    sol[0] = WR[0] * powf(base, 2.f / gm1);
-                    sol[D + 1] = WR[D + 1] * powf(base, 2.f * g / gm1);
+                    sol[0] = WR[0] * R::pow_(base, two / gm1);
+                    sol[D + 1] = WR[D + 1] * R::pow_(base, two * g / gm1);
                     fan = true;
                 }
             }
@@ -549,8 +581,8 @@ __device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflec
         }
 #pragma unroll
         for(int l = 0; l < D; ++l) sol[1 + l] += vhalf * n[l];
-        if(sol[0] == 0.f) return;
-        float vsol = 0.f, v2 = 0.f;
+        if(sol[0] == zero) return;
+        T vsol = zero, v2 = zero;
 #pragma unroll
         for(int l = 0; l < D; ++l) {
             vsol += sol[1 + l] * n[l];
@@ -560,44 +592,105 @@ __device__ void shllc(float g, float* WL, float* WR, const float* n, bool reflec
 #pragma unroll
         for(int l = 0; l < D; ++l) F.mv[l] = F.m * sol[1 + l];
         F.P = sol[D + 1];
-        const float e = sol[D + 1] / gm1 / sol[0] + 0.5f * v2;
+        const T e = sol[D + 1] / gm1 / sol[0] + half * v2;
         F.E = (sol[0] * e + sol[D + 1]) * vsol;
         return;
     }
-    const float rhobar = 0.5f * (WL[0] + WR[0]);
-    const float abar = 0.5f * (aL + aR);
-    const float pstar = fmaxf(0.f, 0.5f * (WL[D + 1] + WR[D + 1]) - 0.5f * (uR - uL) * rhobar * abar);
-    const float gp = 0.5f * (g + 1.f) / g;
-    const float qL = pstar > WL[D + 1] ? sqrtf(1.f + gp * (pstar / WL[D + 1] - 1.f)) : 1.f;
-    const float qR = pstar > WR[D + 1] ? sqrtf(1.f + gp * (pstar / WR[D + 1] - 1.f)) : 1.f;
-    const float SL = uL - aL * qL;
-    const float SR = uR + aR * qR;
-    const float Sstar = (WR[D + 1] - WL[D + 1] + WL[0] * uL * (SL - uL) - WR[0] * uR * (SR - uR)) /
-                        (WL[0] * (SL - uL) - WR[0] * (SR - uR));
-    const bool left = Sstar >= 0.f;
-    const float* Wk = left ? WL : WR;
-    const float uk = left ? uL : uR;
-    const float Sk = left ? SL : SR;
-    float v2 = 0.f;
+    const T rhobar = half * (WL[0] + WR[0]);
+    const T abar = half * (aL + aR);
+    const T pstar = R::max_(zero, half * (WL[D + 1] + WR[D + 1]) - half * (uR - uL) * rhobar * abar);
+    const T gp = half * (g + one) / g;
+    /* a_K q_K */
+    const T wL = pstar > WL[D + 1] ? R::sqrt_(g * (WL[D + 1] + gp * (pstar - WL[D + 1])) / WL[0])
+                                   : aL;
+    const T wR = pstar > WR[D + 1] ? R::sqrt_(g * (WR[D + 1] + gp * (pstar - WR[D + 1])) / WR[0])
+                                   : aR;
+    const T SL = uL - wL;
+    const T SR = uR + wR;
+    const T Sstar = (WR[D + 1] - WL[D + 1] + WL[0] * uL * (SL - uL) - WR[0] * uR * (SR - uR)) /
+                    (WL[0] * (SL - uL) - WR[0] * (SR - uR));
+    const bool left = Sstar >= zero;
+    const T* Wk = left ? WL : WR;
+    const T uk = left ? uL : uR;
+    const T Sk = left ? SL : SR;
+    T v2 = zero;
 #pragma unroll
     for(int l = 0; l < D; ++l) v2 += Wk[1 + l] * Wk[1 + l];
-    const float ek = Wk[D + 1] / gm1 / Wk[0] + 0.5f * v2;
+    const T ek = Wk[D + 1] / gm1 / Wk[0] + half * v2;
     /* momentum flux = (mass flux) v + P n with P the star pressure
      * p_K + S_K fac (S* - u_K) when the star state is used */
-    float mk = Wk[0] * uk;
+    T mk = Wk[0] * uk;
     F.P = Wk[D + 1];
     F.E = (Wk[0] * ek + Wk[D + 1]) * uk;
-    if(left ? (SL < 0.f) : (SR > 0.f)) {
-        const float fac = Wk[0] * (Sk - uk) / (Sk - Sstar);
-        const float ds = Sstar - uk;
+    if(left ? (SL < zero) : (SR > zero)) {
+        const T fac = Wk[0] * (Sk - uk) / (Sk - Sstar);
+        const T ds = Sstar - uk;
         mk += Sk * (fac - Wk[0]);
         F.P += Sk * fac * ds;
-        const float Ue = ek + ds * (Sstar + Wk[D + 1] / (Wk[0] * (Sk - uk)));
+        const T Ue = ek + ds * (Sstar + Wk[D + 1] / (Wk[0] * (Sk - uk)));
         F.E += Sk * (Ue * fac - Wk[0] * ek);
     }
     F.m = mk;
 #pragma unroll
     for(int l = 0; l < D; ++l) F.mv[l] = mk * Wk[1 + l];
+}
+
+__device__ __forceinline__ bool finite4(float a, float b, float c, float d) {
+    return isfinite(a) && isfinite(b) && isfinite(c) && isfinite(d);
+}
+
+/* the two face states and the normal, passed by value to the out-of-line
+ * FP64 re-solve so that nothing goes through local memory on the hot path */
+template <int D>
+struct FaceStates {
+    float L[D + 2], R[D + 2], n[D];
+};
+
+template <int D>
+__device__ __noinline__ SFlux<D> shllc_fp64(float g, FaceStates<D> in, bool reflective) {
+    constexpr int S = D + 2;
+    double dL[S], dR[S], dn[D];
+    for(int k = 0; k < S; ++k) {
+        dL[k] = in.L[k];
+        dR[k] = in.R[k];
+    }
+    for(int l = 0; l < D; ++l) dn[l] = in.n[l];
+    TFlux<D, double> H;
+    thllc<D, double>((double)g, dL, dR, dn, reflective, H);
+    SFlux<D> F;
+    F.m = (float)H.m;
+    for(int l = 0; l < D; ++l) F.mv[l] = (float)H.mv[l];
+    F.P = (float)H.P;
+    F.E = (float)H.E;
+    return F;
+}
+
+/* FP32 HLLC; a face whose FP32 flux is not finite is solved again in FP64 */
+template <int D>
+__device__ __forceinline__ void shllc(float g, const float* WL, const float* WR, const float* n,
+                                      bool reflective, SFlux<D>& F) {
+    TFlux<D, float> G;
+    thllc<D, float>(g, WL, WR, n, reflective, G);
+    float mvs = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) mvs += G.mv[l];
+    if(__builtin_expect(!finite4(G.m, G.P, G.E, mvs), 0)) {
+        FaceStates<D> in;
+#pragma unroll
+        for(int k = 0; k < D + 2; ++k) {
+            in.L[k] = WL[k];
+            in.R[k] = WR[k];
+        }
+#pragma unroll
+        for(int l = 0; l < D; ++l) in.n[l] = n[l];
+        F = shllc_fp64<D>(g, in, reflective);
+        return;
+    }
+    F.m = G.m;
+#pragma unroll
+    for(int l = 0; l < D; ++l) F.mv[l] = G.mv[l];
+    F.P = G.P;
+    F.E = G.E;
 }
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,

@@ -67,13 +67,18 @@ def test_one_request_alone_and_in_mix(cuda_ok):
 
 
 def test_split_server_within_tolerance_of_fp64_server(cuda_ok):
+    """<= 1e-6 relative L1 per conserved field.  These flows start at rest
+    and run a few steps, so their momentum is still far below its natural
+    scale, the momentum m c a sound wave carries: the momentum error is
+    normalised by the larger of the momentum L1 norm and sum(m c)."""
     probs = _problems()
     r64, _ = _serve(probs, 0)
     r32, _ = _serve(probs, 1)
     for pr, a, b in zip(probs, r32, r64):
         D = pr.mesh.dim
         den = np.abs(b.Q).sum(0)
-        den[1:D + 1] = np.sqrt((b.Q[:, 1:D + 1] ** 2).sum(1)).sum()
+        c = np.sqrt(pr.gamma * b.W[:, D + 1] / b.W[:, 0])
+        den[1:D + 1] = max(np.sqrt((b.Q[:, 1:D + 1] ** 2).sum(1)).sum(), (b.Q[:, 0] * c).sum())
         err = np.abs(a.Q - b.Q).sum(0) / den
         assert np.all(err <= 1e-6), err
 
