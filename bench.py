@@ -891,16 +891,24 @@ def main():
     names = ["gradients", "faces", "update"]
     per_launch = kms / args.steps
     top = int(np.argmax(per_launch))
-    alg = algorithmic_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz, args.precision)
+    if args.precision == "split":
+        alg = split_kernel_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz)
+        kname = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces",
+                 "update": "k_group_sapply"}[names[top]]
+    else:
+        alg = algorithmic_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz, args.precision)
+        kname = {"gradients": "k_gradients", "faces": "k_faces", "update": "k_apply"}[names[top]]
     peak, peak_kind = peaks()
     achieved = alg[names[top]] / (per_launch[top] / 1e3) / 1e9
     step_bytes = sum(alg.values())
-    roof = {"bound": "hbm", "kernel": f"k_{names[top]}", "achieved": achieved, "peak": peak,
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
             "peak_source": f"hbm_gbs {peak_kind}",
             "algorithmic_bytes_per_launch": alg[names[top]],
             "kernel_ms": {n: float(v) for n, v in zip(names, per_launch)},
-            "step_achieved_gbs": step_bytes / (ms_max / args.steps / 1e3) / 1e9}
+            "step_achieved_gbs": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
+            "step_bytes_per_face": STEP_BYTES[(args.precision, 3)],
+            "step_frac": STEP_BYTES[(args.precision, 3)] * value / 1e9 / peak}
 
     # end to end through the C ABI with host buffers: per step upload W and Q
     # from host memory, one step, download W and Q

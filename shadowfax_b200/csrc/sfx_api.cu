@@ -30,6 +30,12 @@ struct sfx_mesh {
     sfx_ctx* ctx = nullptr;
     sfx_dmesh d;
     std::vector<void*> allocs;
+    /* split pass: the mesh as a one-member launch group, so that a mesh
+     * stepped alone runs the same kernels, and so the same arithmetic, as
+     * in a group with other meshes */
+    sfx_group_entry* self_tab = nullptr;
+    int32_t* self_pre = nullptr;
+    float self_dt = 0.f; /* time step held in self_tab (0: none yet) */
 };
 
 namespace {
@@ -99,17 +105,51 @@ int check_err(sfx_mesh* m, sfx_stats* st) {
 }
 
 /* one phase of a step: 0 gradients, 1 face fluxes, 2 update */
+/* queued slow faces per mesh: 1/32 of the faces, at least 256 (a face that
+ * finds the queue full is solved in place) */
+int32_t slowq_capacity(int64_t n_faces) {
+    const int64_t c = n_faces / 32;
+    return (int32_t)(c < 256 ? 256 : c);
+}
+
+/* device table of a split mesh as a one-member launch group */
+int setup_self(sfx_mesh* m, cudaStream_t s) {
+    SFX_TRY(dalloc(m, &m->self_tab, 1));
+    SFX_TRY(dalloc(m, &m->self_pre, 6));
+    sfx_group_entry e;
+    std::memset(&e, 0, sizeof e);
+    e.m = m->d;
+    m->self_dt = 0.f;
+    SFX_TRY(cuda_ok(cudaMemsetAsync(m->self_pre, 0, 6 * sizeof(int32_t), s)));
+    /* pageable source: staged before the call returns */
+    return h2d(m->self_tab, &e, 1, s);
+}
+
 int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t s) {
     sfx_ctx* c = m->ctx;
-    const bool split = c->cfg.precision == SFX_PREC_SPLIT;
+    if(c->cfg.precision == SFX_PREC_SPLIT) {
+        const float fdt = (float)dt;
+        if(phase == 1 && fdt != m->self_dt) {
+            m->self_dt = fdt;
+            SFX_TRY(h2d(&m->self_tab->dt, &m->self_dt, 1, s));
+        }
+        sfx_group_dev g;
+        std::memset(&g, 0, sizeof g);
+        g.tab = m->self_tab;
+        g.pre = m->self_pre;
+        g.n_meshes = 1;
+        g.dim = m->d.dim;
+        g.lanes = m->d.lanes;
+        sfx_split_blocks(m->d.dim, m->d.lanes, m->d.n_cells, m->d.n_faces, g.blocks);
+        return sfx_split_group_phase(&g, phase, &c->sp, s);
+    }
     switch(phase) {
     case 0:
-        return split ? sfx_split_gradients(&m->d, s) : sfx_fp64_gradients(&m->d, s);
+        return sfx_fp64_gradients(&m->d, s);
     case 1:
-        return split ? sfx_split_faces(&m->d, &c->sp, dt, s)
-                     : sfx_fp64_faces(&m->d, &c->sp, dt, write_branch, s);
+        return sfx_fp64_faces(&m->d, &c->sp, dt, write_branch, s);
     default:
-        return split ? sfx_split_apply(&m->d, &c->sp, s) : sfx_fp64_apply(&m->d, &c->sp, s);
+        return sfx_fp64_apply(&m->d, &c->sp, s);
     }
 }
 
@@ -392,6 +432,9 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         A(&d.an, (size_t)dim * F);
         A(&d.dqm, F);
         A(&d.dqv, (size_t)dim * F);
+        d.slowq_cap = slowq_capacity(F);
+        A(&d.slowq, (size_t)d.slowq_cap);
+        A(&d.slowq_n, 1);
     }
     if(rc != SFX_OK) {
         sfx_mesh_free(m);
@@ -421,7 +464,9 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     if(!rc) rc = cuda_ok(cudaMemsetAsync(d.W, 0, sizeof(double) * n * S, s));
     if(!rc) rc = cuda_ok(cudaMemsetAsync(d.Q, 0, sizeof(double) * n * S, s));
     if(!rc) rc = reset_err(m);
+    if(!rc && split) rc = cuda_ok(cudaMemsetAsync(d.slowq_n, 0, sizeof(int32_t), s));
     if(!rc && split) rc = sfx_split_prepare(&d, s);
+    if(!rc && split) rc = setup_self(m, s);
     /* host staging buffers go out of scope: wait for the copies */
     if(!rc) rc = cuda_ok(cudaStreamSynchronize(s));
     if(rc != SFX_OK) {
@@ -653,17 +698,24 @@ int sfx_mesh_clone(sfx_ctx* ctx, sfx_mesh* base, sfx_mesh** out) {
     A(&d.Q, n * S);
     A(&d.err, 1);
     A(&d.totals_scratch, (size_t)(S + 1) * 1024);
+    d.slowq = d.slowq_n = nullptr;
+    d.slowq_cap = 0;
     if(split) {
         A(&d.cw, 2 * n);
         A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
         A(&d.dqm, F);
         A(&d.dqv, (size_t)dim * F);
+        d.slowq_cap = slowq_capacity(F);
+        A(&d.slowq, (size_t)d.slowq_cap);
+        A(&d.slowq_n, 1);
     } else {
         A(&d.grad, n * dim * S);
         A(&d.dQf, F * S);
         A(&d.branch, F);
     }
     if(!rc) rc = reset_err(m);
+    if(!rc && split) rc = cuda_ok(cudaMemsetAsync(d.slowq_n, 0, sizeof(int32_t), ctx->stream));
+    if(!rc && split) rc = setup_self(m, ctx->stream);
     if(!rc) rc = cuda_ok(cudaStreamSynchronize(ctx->stream));
     if(rc) {
         sfx_mesh_free(m);
@@ -679,7 +731,8 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
     const int64_t n = b.n_cells, F = b.n_faces, S = b.S, D = b.dim;
     int64_t bytes = n * S * 16 + (S + 1) * 1024 * 8 + 64;
     if(precision == SFX_PREC_SPLIT)
-        bytes += n * 32 + n * 16 * ((D * S + 3) / 4) + F * 8 + F * D * 8;
+        bytes += n * 32 + n * 16 * ((D * S + 3) / 4) + F * 8 + F * D * 8 +
+                 4 * (int64_t)slowq_capacity(F) + 4 + (int64_t)sizeof(sfx_group_entry) + 24;
     else
         bytes += n * D * S * 8 + F * S * 8 + F * 4;
     return bytes;

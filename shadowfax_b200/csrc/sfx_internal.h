@@ -75,6 +75,15 @@ struct sfx_dmesh {
     double* an;
     float2* dqm;
     double* dqv;
+    /* exact solver, split pass: faces whose p* iteration falls back to
+     * Brent's method are queued here by the face kernel (face ids, up to
+     * slowq_cap; slowq_n counts them) and solved by a follow-up launch in
+     * which every lane works on a queued face, instead of one lane of a warp
+     * iterating while the other 31 wait.  The gradient kernel resets the
+     * count each step. */
+    int32_t* slowq;
+    int32_t* slowq_n;
+    int32_t slowq_cap;
 };
 
 /* one mesh of a launch group (device table entry); steps_left, when not
@@ -102,6 +111,10 @@ struct sfx_solver_params {
     int32_t kind;
     double gamma, tol, cutoff;
     double gp1d2g, gm1d2g, gm1dgp1, tdgp1, tdgm1, gm1d2, tgdgm1, ginv;
+    /* 2/(g-1) and 2g/(g-1) when they are small integers (3 and 5 for
+     * g = 5/3, 5 and 7 for g = 7/5), else 0: the split pass then raises to
+     * these powers by multiplication (the plain FP64 pass always calls pow) */
+    int32_t k_tdgm1, k_tgdgm1;
 };
 
 void sfx_solver_params_init(sfx_solver_params* p, int kind, double gamma,
@@ -124,10 +137,6 @@ int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n,
 /* FP32/FP64-split kernels (sfx_split.cu) */
 int sfx_split_prepare(const sfx_dmesh* m, void* stream);
 int sfx_split_load_state(const sfx_dmesh* m, void* stream);
-int sfx_split_gradients(const sfx_dmesh* m, void* stream);
-int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
-                    void* stream);
-int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream);
 /* W (FP64 SoA) from the FP32 cell records, for downloads */
 int sfx_split_export_W(const sfx_dmesh* m, void* stream);
 /* per-face dQ (FP32) widened into dQf (FP64 SoA), for parity checks */

@@ -30,6 +30,11 @@ namespace {
 constexpr unsigned kRightBit = 0x80000000u;
 constexpr int kPeriodicBit = 1 << 30;
 constexpr int kIndexMask = (1 << 30) - 1;
+/* exact solver: "this face needs Brent's method", queued instead of solved */
+constexpr int kDefer = 0x7f;
+/* blocks of the group's queued-face launch (two waves of 128-thread blocks
+ * on 148 SMs; the launch strides over each member's queue) */
+constexpr int kSlowGroupBlocks = 296;
 
 __device__ __forceinline__ void report_face(sfx_dev_error* e, int f, int st) {
     atomicMin(&e->face_key, ((unsigned long long)(unsigned)f << 8) | (unsigned)st);
@@ -259,6 +264,7 @@ template <int D, int LPC>
 __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
     constexpr int S = D + 2, G = (D * S + 3) / 4;
     const int i = t / LPC, lane = t % LPC;
+    if(t == 0) *m.slowq_n = 0; /* a new step: empty the slow-face queue */
     /* whole warps stay alive for the shuffles; lanes past the end idle */
     const bool live = i < m.n_cells && !failed(m.err);
     const int ic = live ? i : 0;
@@ -368,11 +374,6 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
         if(lane == q % LPC)
             m.cg[(size_t)G * i + q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2],
                                                   out[4 * q + 3]);
-}
-
-template <int D, int LPC>
-__global__ void __launch_bounds__(256) k_sgrad(sfx_dmesh m) {
-    sgrad_body<D, LPC>(m, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ----------------------------- face physics ----------------------------- */
@@ -695,6 +696,15 @@ __device__ __forceinline__ void shllc(float g, const float* WL, const float* WR,
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
  * 462-546) with the device pow; returns 0 or SFX_ERR_* */
+/* x^y for the exponents 2/(g-1) and 2g/(g-1): by repeated multiplication
+ * when k (the exponent, if a small integer) is nonzero, else pow */
+__device__ __forceinline__ double kpow(double x, int k, double y) {
+    if(k == 0) return pow(x, y);
+    double r = x;
+    for(int i = 1; i < k; ++i) r *= x;
+    return r;
+}
+
 template <int D>
 struct XS {
     const sfx_solver_params& s;
@@ -705,18 +715,29 @@ struct XS {
         }
         return s.tdgm1 * a * (pow(p / Wb[D + 1], s.gm1d2g) - 1.);
     }
-    __device__ double fpb(double p, const double* Wb, double a) const {
+    /* f_K, f_K' and, on the rarefaction side, z = (p/p_K)^((g-1)/(2g)) at
+     * one pressure: f_K' = r^(-(g+1)/(2g)) / (rho_K a_K) = z / (r rho_K a_K)
+     * with r = p/p_K, so one pow serves both */
+    __device__ void side(double p, const double* Wb, double a, double& f, double& fp,
+                         double& z) const {
         if(p > Wb[D + 1]) {
             const double A = s.tdgp1 / Wb[0], B = s.gm1dgp1 * Wb[D + 1];
-            return (1. - 0.5 * (p - Wb[D + 1]) / (B + p)) * sqrt(A / (p + B));
+            const double q = sqrt(A / (p + B));
+            f = (p - Wb[D + 1]) * q;
+            fp = (1. - 0.5 * (p - Wb[D + 1]) / (B + p)) * q;
+            z = 0.;
+        } else {
+            const double r = p / Wb[D + 1];
+            z = pow(r, s.gm1d2g);
+            f = s.tdgm1 * a * (z - 1.);
+            fp = r > 0. ? z / (r * (Wb[0] * a)) : 1. / (Wb[0] * a) * pow(r, -s.gp1d2g);
         }
-        return 1. / (Wb[0] * a) * pow(p / Wb[D + 1], -s.gp1d2g);
     }
 };
 
 template <int D>
 __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const double* n,
-                      bool reflective, double* sol) {
+                      bool reflective, double* sol, bool defer) {
     constexpr int S = D + 2;
     double vL = 0., vR = 0.;
 #pragma unroll
@@ -756,14 +777,14 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         for(int k = 0; k < S; ++k) sol[k] = Ws[k];
         if(side == 2) {
             const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-            sol[0] = WL[0] * pow(base, s.tdgm1);
+            sol[0] = WL[0] * kpow(base, s.k_tdgm1, s.tdgm1);
             vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-            sol[D + 1] = WL[D + 1] * pow(base, s.tgdgm1);
+            sol[D + 1] = WL[D + 1] * kpow(base, s.k_tgdgm1, s.tgdgm1);
         } else if(side == 4) {
             const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-            sol[0] = WR[0] * pow(base, s.tdgm1);
+            sol[0] = WR[0] * kpow(base, s.k_tdgm1, s.tdgm1);
             vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-            sol[D + 1] = WR[D + 1] * pow(base, s.tgdgm1);
+            sol[D + 1] = WR[D + 1] * kpow(base, s.k_tgdgm1, s.tgdgm1);
         }
     } else {
         XS<D> x{s};
@@ -776,9 +797,9 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         if(pmax / pmin <= 2. && pmin <= ppv && ppv <= pmax) {
             pg = ppv;
         } else if(ppv < pmin) {
-            pg = pow((aL + aR - s.gm1d2 * (vR - vL)) /
-                         (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
-                     s.tgdgm1);
+            pg = kpow((aL + aR - s.gm1d2 * (vR - vL)) /
+                          (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
+                      s.k_tgdgm1, s.tgdgm1);
         } else {
             const double gL = sqrt(s.tdgp1 / WL[0] / (ppv + s.gm1dgp1 * pL));
             const double gR = sqrt(s.tdgp1 / WR[0] / (ppv + s.gm1dgp1 * pR));
@@ -786,17 +807,28 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         }
         pg = fmax(floorp, pg);
         auto f = [&](double p) { return x.fb(p, WL, aL) + x.fb(p, WR, aR) + (vR - vL); };
-        auto fp = [&](double p) { return x.fpb(p, WL, aL) + x.fpb(p, WR, aR); };
+        /* f and f' at one pressure, the per-side values kept for the wave
+         * velocity and the sampling below */
+        double fL = 0., fpL = 0., zL = 0., fR = 0., fpR = 0., zR = 0.;
+        auto eval = [&](double p, double& fv, double& fpv) {
+            x.side(p, WL, aL, fL, fpL, zL);
+            x.side(p, WR, aR, fR, fpR, zR);
+            fv = fL + fR + (vR - vL);
+            fpv = fpL + fpR;
+        };
         double p = 0.;
-        const double f0 = f(0.);
-        double fg = f(pg);
+        /* f(0): the rarefaction branch at p = 0 is -2 a_K / (g - 1) */
+        const double f0 = pL > 0. && pR > 0. ? -s.tdgm1 * aL + -s.tdgm1 * aR + (vR - vL) : f(0.);
+        double fg, fpg;
+        eval(pg, fg, fpg);
+        bool at_p = true; /* fL, fR, zL, zR hold the values at the final p */
         int it = 0;
         if(f0 < s.cutoff) {
             while(fabs(p - pg) > s.tol * 0.5 * (p + pg)) {
                 if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
                 p = pg;
-                pg = fmax(0., pg - fg / fp(pg));
-                fg = f(pg);
+                pg = fmax(0., pg - fg / fpg);
+                eval(pg, fg, fpg);
             }
             p = pg;
         } else {
@@ -804,11 +836,13 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                 while(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg < 0.) {
                     if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
                     p = pg;
-                    pg = pg - fg / fp(pg);
-                    fg = f(pg);
+                    pg = pg - fg / fpg;
+                    eval(pg, fg, fpg);
                 }
             }
             if(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg > 0.) {
+                if(defer) return kDefer;
+                at_p = false;
                 /* Brent on [0, pg] */
                 double a = 0., b = pg, c, d = 1e230, fa = f(a), fbv = fg, fc, sv;
                 if(fa * fbv >= 0.) {
@@ -863,7 +897,11 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                 p = pg;
             }
         }
-        const double u = 0.5 * (vL + vR) + 0.5 * (x.fb(p, WR, aR) - x.fb(p, WL, aL));
+        if(!at_p) {
+            double t0, t1;
+            eval(p, t0, t1);
+        }
+        const double u = 0.5 * (vL + vR) + 0.5 * (fR - fL);
         if(u < 0.) {
 #pragma unroll
             for(int k = 0; k < S; ++k) sol[k] = WR[k];
@@ -875,13 +913,14 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                     vhalf = u - vR;
                 }
             } else if(vR + aR > 0.) {
-                if(u + aR * pow(r, s.gm1d2g) <= 0.) {
+                if(u + aR * zR <= 0.) {
                     const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-                    sol[0] = WR[0] * pow(base, s.tdgm1);
+                    sol[0] = WR[0] * kpow(base, s.k_tdgm1, s.tdgm1);
                     vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-                    sol[D + 1] = pR * pow(base, s.tgdgm1);
+                    sol[D + 1] = pR * kpow(base, s.k_tgdgm1, s.tgdgm1);
                 } else {
-                    sol[0] = WR[0] * pow(r, s.ginv);
+                    /* r^(1/g) = z^(2/(g-1)) with z = r^((g-1)/(2g)) */
+                    sol[0] = WR[0] * (s.k_tdgm1 ? kpow(zR, s.k_tdgm1, 0.) : pow(r, s.ginv));
                     sol[D + 1] = p;
                     vhalf = u - vR;
                 }
@@ -897,13 +936,13 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                     vhalf = u - vL;
                 }
             } else if(vL - aL < 0.) {
-                if(u - aL * pow(r, s.gm1d2g) > 0.) {
+                if(u - aL * zL > 0.) {
                     const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-                    sol[0] = WL[0] * pow(base, s.tdgm1);
+                    sol[0] = WL[0] * kpow(base, s.k_tdgm1, s.tdgm1);
                     vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-                    sol[D + 1] = pL * pow(base, s.tgdgm1);
+                    sol[D + 1] = pL * kpow(base, s.k_tgdgm1, s.tgdgm1);
                 } else {
-                    sol[0] = WL[0] * pow(r, s.ginv);
+                    sol[0] = WL[0] * (s.k_tdgm1 ? kpow(zL, s.k_tdgm1, 0.) : pow(r, s.ginv));
                     sol[D + 1] = p;
                     vhalf = u - vL;
                 }
@@ -920,7 +959,7 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
 
 template <int D, int SOLVER>
 __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
-                                            const float dt, const int f) {
+                                            const float dt, const int f, const bool defer) {
     constexpr int S = D + 2;
     if(f >= m.n_faces || failed(m.err)) return;
     float A, c[D], r[D], rn;
@@ -1010,13 +1049,23 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
     } else {
         double dWL[S], dWR[S], dn[D], h[S];
 #pragma unroll
-        for(int k = 0; k < S; ++k) {
-            dWL[k] = WL[k];
-            dWR[k] = WR[k];
-        }
-#pragma unroll
         for(int l = 0; l < D; ++l) dn[l] = nrm[l];
-        status = sexact<D>(sp, dWL, dWR, dn, mirror, h);
+        for(bool d = defer;; d = false) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) {
+                dWL[k] = WL[k];
+                dWR[k] = WR[k];
+            }
+            status = sexact<D>(sp, dWL, dWR, dn, mirror, h, d);
+            if(status != kDefer) break;
+            /* Brent's method: queue the face for the follow-up launch (it
+             * writes this face's dQ); solve it here if the queue is full */
+            const int q = atomicAdd(m.slowq_n, 1);
+            if(q < m.slowq_cap) {
+                m.slowq[q] = f;
+                return;
+            }
+        }
         F.m = 0.f;
         F.P = 0.f;
         F.E = 0.f;
@@ -1081,12 +1130,6 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
     for(int l = 0; l < D; ++l) m.dqv[(size_t)l * FF + f] = dv[l];
     if(status == SFX_OK && F.m != F.m) status = SFX_ERR_NAN_FLUX;
     if(status != SFX_OK) report_face(m.err, f, status);
-}
-
-template <int D, int SOLVER>
-__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
-        k_sfaces(sfx_dmesh m, sfx_solver_params sp, float dt) {
-    sfaces_body<D, SOLVER>(m, sp, dt, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ------------------------------- update ------------------------------- */
@@ -1163,15 +1206,10 @@ __device__ __forceinline__ void sapply_body(const sfx_dmesh& m, const double gam
     store_cell<D>(m.cw, i, Wf, (float)Q[0], (float)m.tarea[i]);
 }
 
-template <int D, int LPC>
-__global__ void __launch_bounds__(256) k_sapply(sfx_dmesh m, double gamma) {
-    sapply_body<D, LPC>(m, gamma, blockIdx.x * blockDim.x + threadIdx.x);
-}
-
 /* ------------------------- grouped (batched) launches -------------------------
  * One launch per phase covers every mesh of a group: block b works on the
- * mesh whose block range [pre[mi], pre[mi+1]) contains b, with the same
- * per-mesh code as the single-mesh kernels. */
+ * mesh whose block range [pre[mi], pre[mi+1]) contains b.  A mesh stepped on
+ * its own is a group of one, so it runs the same kernels. */
 __device__ __forceinline__ int group_mesh_of_block(const int* __restrict__ pre, int nm) {
     __shared__ int s_mesh;
     if(threadIdx.x == 0) {
@@ -1211,7 +1249,21 @@ __global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
     sfaces_body<D, SOLVER>(tab[mi].m, sp, tab[mi].dt,
-                           (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+                           (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x,
+                           SOLVER == SFX_SOLVER_EXACT);
+}
+
+/* the queued exact-solver faces of every member, one per thread */
+template <int D>
+__global__ void __launch_bounds__(128) k_group_sfaces_slow(const sfx_group_entry* tab, int nm,
+                                                          sfx_solver_params sp) {
+    for(int mi = 0; mi < nm; ++mi) {
+        if(member_done(tab, mi)) continue;
+        const sfx_dmesh& m = tab[mi].m;
+        const int n = min(*m.slowq_n, m.slowq_cap);
+        for(int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+            sfaces_body<D, SFX_SOLVER_EXACT>(m, sp, tab[mi].dt, __ldg(m.slowq + j), false);
+    }
 }
 
 template <int D, int LPC>
@@ -1252,12 +1304,15 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
             k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm);
     } else if(phase == 1) {
         if(g->blocks[1]) {
-            if(sp->kind == SFX_SOLVER_EXACT)
+            if(sp->kind == SFX_SOLVER_EXACT) {
                 k_group_sfaces<D, SFX_SOLVER_EXACT><<<g->blocks[1], 256, 0, s>>>(
                         g->tab, g->pre + (nm + 1), nm, *sp);
-            else
+                k_group_sfaces_slow<D><<<kSlowGroupBlocks, 128, 0, s>>>(g->tab, nm, *sp);
+                sfx_count_launches(1);
+            } else {
                 k_group_sfaces<D, SFX_SOLVER_HLLC><<<g->blocks[1], 256, 0, s>>>(
                         g->tab, g->pre + (nm + 1), nm, *sp);
+            }
         }
     } else {
         if(g->blocks[2])
@@ -1320,59 +1375,6 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
     else
         k_export_dQ<2><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
     return launched(1);
-}
-
-/* the per-cell kernels for the mesh's lanes-per-cell setting */
-template <int D>
-int cells_phase(const sfx_dmesh* m, int phase, double gamma, cudaStream_t s) {
-    const int G = grid_for((long long)m->n_cells * m->lanes, 256);
-#define SFX_LANES_CASE(LPC)                                        \
-    case LPC:                                                      \
-        if(phase == 0)                                             \
-            k_sgrad<D, LPC><<<G, 256, 0, s>>>(*m);                 \
-        else                                                       \
-            k_sapply<D, LPC><<<G, 256, 0, s>>>(*m, gamma);         \
-        break;
-    switch(m->lanes) {
-        SFX_LANES_CASE(1)
-        SFX_LANES_CASE(2)
-        SFX_LANES_CASE(4)
-        SFX_LANES_CASE(8)
-        SFX_LANES_CASE(16)
-    default:
-        return SFX_ERR_INVALID;
-    }
-#undef SFX_LANES_CASE
-    return launched(1);
-}
-
-int sfx_split_gradients(const sfx_dmesh* m, void* stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    return m->dim == 3 ? cells_phase<3>(m, 0, 0., s) : cells_phase<2>(m, 0, 0., s);
-}
-
-int sfx_split_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt, void* stream) {
-    if(!m->n_faces) return SFX_OK;
-    cudaStream_t s = (cudaStream_t)stream;
-    const int G = grid_for(m->n_faces, 256);
-    const float fdt = (float)dt;
-    if(m->dim == 3) {
-        if(sp->kind == SFX_SOLVER_EXACT)
-            k_sfaces<3, SFX_SOLVER_EXACT><<<G, 256, 0, s>>>(*m, *sp, fdt);
-        else
-            k_sfaces<3, SFX_SOLVER_HLLC><<<G, 256, 0, s>>>(*m, *sp, fdt);
-    } else {
-        if(sp->kind == SFX_SOLVER_EXACT)
-            k_sfaces<2, SFX_SOLVER_EXACT><<<G, 256, 0, s>>>(*m, *sp, fdt);
-        else
-            k_sfaces<2, SFX_SOLVER_HLLC><<<G, 256, 0, s>>>(*m, *sp, fdt);
-    }
-    return launched(1);
-}
-
-int sfx_split_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    return m->dim == 3 ? cells_phase<3>(m, 2, sp->gamma, s) : cells_phase<2>(m, 2, sp->gamma, s);
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {
