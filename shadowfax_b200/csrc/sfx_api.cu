@@ -751,3 +751,23 @@ int sfx_mesh_totals(sfx_mesh* m, double* totals) {
 }
 
 }  // extern "C"
+
+/* internal transfers for the request server (C++ linkage) */
+int sfx_mesh_upload_W_fieldmajor(sfx_mesh* m, const double* W) {
+    if(!m || !W) return SFX_ERR_INVALID;
+    cudaStream_t s = m->ctx->stream;
+    SFX_TRY(reset_err(m));
+    SFX_TRY(h2d(m->d.W, W, (size_t)m->d.n_cells * m->d.S, s));
+    SFX_TRY(sfx_fp64_init_Q(&m->d, &m->ctx->sp, s));
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_load_state(&m->d, s));
+    return check_err(m, nullptr);
+}
+
+int sfx_mesh_download_fieldmajor_async(sfx_mesh* m, double* W, double* Q, void* stream) {
+    if(!m || !W || !Q) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = sizeof(double) * (size_t)m->d.n_cells * m->d.S;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_export_W(&m->d, s));
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(W, m->d.W, bytes, cudaMemcpyDeviceToHost, s)));
+    return cuda_ok(cudaMemcpyAsync(Q, m->d.Q, bytes, cudaMemcpyDeviceToHost, s));
+}

@@ -1226,12 +1226,6 @@ void sfx_solver_params_init(sfx_solver_params* p, int kind, double g, double tol
     p->gm1d2 = 0.5 * (g - 1.);
     p->tgdgm1 = 2. * g / (g - 1.);
     p->ginv = 1. / g;
-    auto small_int = [](double x) {
-        const double r = nearbyint(x);
-        return r >= 1. && r <= 16. && x == r ? (int32_t)r : 0;
-    };
-    p->k_tdgm1 = small_int(p->tdgm1);
-    p->k_tgdgm1 = small_int(p->tgdgm1);
 }
 
 int sfx_fp64_gradients(const sfx_dmesh* m, void* stream) {

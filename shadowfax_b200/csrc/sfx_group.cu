@@ -26,6 +26,7 @@ struct sfx_group {
     int32_t* d_steps = nullptr; /* per-member step counters (after set_steps) */
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1;
+    int cap = 0; /* members the device buffers hold */
 };
 
 namespace {
@@ -83,6 +84,26 @@ int run_steps(sfx_group* g, int nsteps, cudaStream_t s) {
     return SFX_OK;
 }
 
+/* device buffers for at least n members (contents are not kept) */
+int reserve(sfx_group* g, int n) {
+    if(n <= g->cap) return SFX_OK;
+    const int cap = n > 2 * g->cap ? n : 2 * g->cap;
+    if(g->dev.tab) cudaFree(g->dev.tab);
+    if(g->dev.pre) cudaFree(g->dev.pre);
+    if(g->d_err_out) cudaFree(g->d_err_out);
+    if(g->d_steps) cudaFree(g->d_steps);
+    g->dev.tab = nullptr;
+    g->dev.pre = nullptr;
+    g->d_err_out = nullptr;
+    g->d_steps = nullptr;
+    g->cap = 0;
+    int rc = cuda_ok(cudaMalloc((void**)&g->dev.tab, sizeof(sfx_group_entry) * cap));
+    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.pre, sizeof(int32_t) * 3 * (cap + 1)));
+    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->d_err_out, sizeof(sfx_dev_error) * cap));
+    if(!rc) g->cap = cap;
+    return rc;
+}
+
 bool same_config(const sfx_config* a, const sfx_config* b) {
     return a->dim == b->dim && a->solver == b->solver && a->precision == b->precision &&
            a->gamma == b->gamma && a->tolerance == b->tolerance && a->cutoff == b->cutoff &&
@@ -115,9 +136,7 @@ extern "C" int sfx_group_create(sfx_ctx* ctx, int32_t n, sfx_mesh* const* meshes
     g->dev.dim = cfg->dim;
     g->dev.lanes = 4;
     int rc = cuda_ok(cudaSetDevice(cfg->device));
-    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.tab, sizeof(sfx_group_entry) * n));
-    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->dev.pre, sizeof(int32_t) * 3 * (n + 1)));
-    if(!rc) rc = cuda_ok(cudaMalloc((void**)&g->d_err_out, sizeof(sfx_dev_error) * n));
+    if(!rc) rc = reserve(g, n);
     if(!rc) rc = upload_layout(g);
     if(rc) {
         sfx_group_free(g);
@@ -311,10 +330,10 @@ extern "C" int sfx_group_set_steps(sfx_group* g, const int32_t* steps) {
     for(int i = 0; i < nm; ++i)
         if(steps[i] < 0) return SFX_ERR_INVALID;
     if(!g->d_steps) {
-        int rc = cuda_ok(cudaMalloc((void**)&g->d_steps, sizeof(int32_t) * nm));
+        int rc = cuda_ok(cudaMalloc((void**)&g->d_steps, sizeof(int32_t) * g->cap));
         if(rc) return rc;
-        for(int i = 0; i < nm; ++i) g->host_tab[i].steps_left = g->d_steps + i;
     }
+    for(int i = 0; i < nm; ++i) g->host_tab[i].steps_left = g->d_steps + i;
     cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
     int rc = cuda_ok(cudaMemcpyAsync(g->d_steps, steps, sizeof(int32_t) * nm,
                                      cudaMemcpyHostToDevice, s));
@@ -330,6 +349,34 @@ extern "C" int sfx_group_get_steps(sfx_group* g, int32_t* steps) {
                                      cudaMemcpyDeviceToHost, s));
     if(rc) return rc;
     return cuda_ok(cudaStreamSynchronize(s));
+}
+
+int sfx_group_set_members(sfx_group* g, int32_t n, sfx_mesh* const* meshes, const double* dt,
+                          const int32_t* steps) {
+    if(!g || n <= 0 || !meshes || !dt) return SFX_ERR_INVALID;
+    const sfx_config* cfg = sfx_ctx_config(g->ctx);
+    for(int i = 0; i < n; ++i) {
+        if(!meshes[i] || !(dt[i] > 0.)) return SFX_ERR_INVALID;
+        if(!same_config(sfx_ctx_config(sfx_mesh_ctx(meshes[i])), cfg)) return SFX_ERR_INVALID;
+    }
+    drop_graph(g);
+    const bool had_steps = g->d_steps != nullptr;
+    int rc = reserve(g, n);
+    if(rc) return rc;
+    g->meshes.assign(meshes, meshes + n);
+    g->host_tab.assign(n, sfx_group_entry{});
+    for(int i = 0; i < n; ++i) {
+        std::memset(&g->host_tab[i], 0, sizeof(sfx_group_entry));
+        g->host_tab[i].m = *sfx_mesh_dev(meshes[i]);
+        g->host_tab[i].dt = (float)dt[i];
+    }
+    g->dev.n_meshes = n;
+    if(steps || had_steps) {
+        std::vector<int32_t> zero;
+        if(!steps) zero.assign(n, 0);
+        return sfx_group_set_steps(g, steps ? steps : zero.data());
+    }
+    return upload_layout(g);
 }
 
 extern "C" int sfx_group_free(sfx_group* g) {

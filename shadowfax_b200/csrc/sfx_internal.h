@@ -111,10 +111,6 @@ struct sfx_solver_params {
     int32_t kind;
     double gamma, tol, cutoff;
     double gp1d2g, gm1d2g, gm1dgp1, tdgp1, tdgm1, gm1d2, tgdgm1, ginv;
-    /* 2/(g-1) and 2g/(g-1) when they are small integers (3 and 5 for
-     * g = 5/3, 5 and 7 for g = 7/5), else 0: the split pass then raises to
-     * these powers by multiplication (the plain FP64 pass always calls pow) */
-    int32_t k_tdgm1, k_tgdgm1;
 };
 
 void sfx_solver_params_init(sfx_solver_params* p, int kind, double gamma,
@@ -154,6 +150,17 @@ sfx_ctx* sfx_mesh_ctx(sfx_mesh* m);
 void* sfx_ctx_stream(sfx_ctx* c);
 const sfx_config* sfx_ctx_config(sfx_ctx* c);
 const sfx_solver_params* sfx_ctx_params(sfx_ctx* c);
+
+/* replace a launch group's members (same context), reusing its device
+ * buffers when they are large enough; steps (may be NULL) as in
+ * sfx_group_set_steps (sfx_group.cu) */
+int sfx_group_set_members(sfx_group* g, int32_t n, sfx_mesh* const* meshes, const double* dt,
+                          const int32_t* steps);
+/* state transfers in the device's field-major layout [S][n] (sfx_api.cu):
+ * upload W, derive Q (waits and returns the status, as sfx_state_upload_W);
+ * the download enqueues the copies on `stream` and returns at once */
+int sfx_mesh_upload_W_fieldmajor(sfx_mesh* m, const double* W);
+int sfx_mesh_download_fieldmajor_async(sfx_mesh* m, double* W, double* Q, void* stream);
 
 /* grouped launches (sfx_split.cu) */
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);

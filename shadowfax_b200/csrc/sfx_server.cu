@@ -5,21 +5,28 @@
  * pass into a service.  Meshes are uploaded once into a device pool.  A
  * request (pool mesh, initial state, solver, dt, step count) is queued by
  * sfx_server_submit and admitted by the worker thread in arrival order while
- * the device-memory budget and the slot count allow: its state is cloned
- * onto the pool mesh's geometry (sfx_mesh_clone) and stays resident until it
- * finishes.  Each scheduling round advances every admitted request by up to
- * `chunk_steps` steps:
+ * the device-memory budget and the slot count allow: its state lives in an
+ * instance on the pool mesh's geometry (sfx_mesh_clone) and stays resident
+ * until it finishes.  Each scheduling round advances every admitted request
+ * by up to `chunk_steps` steps:
  *   SFX_PREC_SPLIT  all requests of one (dimension, solver) class share one
- *                   launch group (one launch per phase for all of them,
- *                   captured in a CUDA graph); per-request step counters live
- *                   on the device, so a request that finishes inside a chunk
- *                   stops there while the others go on;
+ *                   launch group (one launch per phase for all of them, a
+ *                   CUDA graph once the membership holds for a round);
+ *                   per-request step counters live on the device, so a
+ *                   request that finishes inside a round stops there while
+ *                   the others go on;
  *   SFX_PREC_FP64   every request is stepped on its own (the per-request
  *                   baseline).
  * The classes run on their own streams and overlap on the device.  Requests
- * that arrive while a round runs join at the next round.  Finished requests
- * are downloaded to host memory, their device state is freed, and they wait
- * for sfx_server_poll.
+ * that arrive while a round runs join at the next round.
+ *
+ * The worker keeps the GPU busy between rounds: finished requests are copied
+ * out on a separate stream into pinned buffers while the next round runs,
+ * and their host-side transposes happen then too; instances of finished
+ * requests are kept per (pool mesh, solver) and reused by later requests,
+ * and launch groups keep their device tables, so a round in steady state
+ * allocates and frees no device memory (cudaFree would wait for the whole
+ * device).  Results wait in host memory until sfx_server_poll collects them.
  */
 #include <cuda_runtime.h>
 
@@ -39,11 +46,18 @@
 
 namespace {
 
+/* pinned host buffer for the asynchronous result copies */
+struct Pinned {
+    double* p = nullptr;
+    size_t cap = 0; /* doubles */
+};
+
 struct Request {
     int64_t id = 0;
     int32_t mesh_id = 0, solver = 0, nsteps = 0;
     double dt = 0.;
-    std::vector<double> W0, W, Q;
+    std::vector<double> W0; /* field-major [S][n], transposed at submit */
+    std::vector<double> W, Q;
     double t_submit = 0., t_admit = 0., t_done = 0.;
     int32_t status = SFX_OK, steps_done = 0;
     int64_t face_steps = 0;
@@ -52,14 +66,16 @@ struct Request {
     int64_t bytes = 0;
     int32_t remaining = 0;
     int32_t chunk = 0; /* steps launched this round (FP64 mode) */
+    Pinned stage;      /* result copy in flight */
 };
 
 struct PoolMesh {
     sfx_mesh* mesh = nullptr;
-    int dim = 0;
+    int dim = 0, S = 0;
     int32_t n_cells = 0;
     int64_t active_faces = 0;
     int64_t clone_bytes = 0;
+    std::vector<sfx_mesh*> cache[2]; /* idle instances per solver */
 };
 
 struct Class {
@@ -67,7 +83,7 @@ struct Class {
     std::vector<Request*> members;
     sfx_group* group = nullptr;
     bool dirty = false;
-    int reused = 0; /* rounds the current group has run unchanged */
+    int reused = 0; /* rounds the current membership has run */
 };
 
 }  // namespace
@@ -84,11 +100,16 @@ struct sfx_server {
     int64_t next_id = 1;
     int64_t n_submitted = 0, n_admitted = 0, n_completed = 0, n_failed = 0;
     int64_t face_steps = 0, rounds = 0;
-    int64_t bytes_in_use = 0;
+    int64_t bytes_in_use = 0; /* instances of admitted requests */
+    int64_t bytes_cached = 0; /* idle instances kept for reuse */
     int active = 0;
     bool stop = false;
     std::thread worker;
     std::chrono::steady_clock::time_point t0;
+    /* worker thread only */
+    cudaStream_t copy_stream = nullptr;
+    std::vector<Pinned> pinned_free;
+    std::vector<Request*> leaving; /* results being copied out */
 };
 
 namespace {
@@ -110,18 +131,33 @@ sfx_config make_cfg(const sfx_server* s, int dim, int solver) {
     return c;
 }
 
-/* worker thread only: request leaves the device */
-void finish(sfx_server* s, Request* r, int status) {
-    if(r->inst) {
-        const int64_t n = sfx_mesh_dev(r->inst)->n_cells;
-        const int S = sfx_mesh_dev(r->inst)->S;
-        r->W.resize((size_t)n * S);
-        r->Q.resize((size_t)n * S);
-        int rc = sfx_state_download(r->inst, r->W.data(), r->Q.data());
-        if(rc && status == SFX_OK) status = rc;
-        sfx_mesh_free(r->inst);
-        r->inst = nullptr;
+Pinned pinned_get(sfx_server* s, size_t n) {
+    size_t best = s->pinned_free.size();
+    for(size_t i = 0; i < s->pinned_free.size(); ++i)
+        if(s->pinned_free[i].cap >= n &&
+           (best == s->pinned_free.size() || s->pinned_free[i].cap < s->pinned_free[best].cap))
+            best = i;
+    if(best < s->pinned_free.size()) {
+        Pinned b = s->pinned_free[best];
+        s->pinned_free.erase(s->pinned_free.begin() + best);
+        return b;
     }
+    Pinned b;
+    if(cudaHostAlloc((void**)&b.p, n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return b;
+    }
+    b.cap = n;
+    return b;
+}
+
+void pinned_put(sfx_server* s, Pinned b) {
+    if(b.p) s->pinned_free.push_back(b);
+}
+
+/* bookkeeping of a request that has left the device (worker thread) */
+void mark_done(sfx_server* s, Request* r, int status) {
     PoolMesh* pm;
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -132,7 +168,6 @@ void finish(sfx_server* s, Request* r, int status) {
     r->status = status;
     r->t_done = now_s(s);
     std::lock_guard<std::mutex> lk(s->mu);
-    s->bytes_in_use -= r->bytes;
     s->active -= 1;
     r->done = true;
     if(status == SFX_OK) {
@@ -144,19 +179,110 @@ void finish(sfx_server* s, Request* r, int status) {
     s->cv_done.notify_all();
 }
 
+/* the instance goes back to its pool mesh's cache */
+void release_instance(sfx_server* s, Request* r) {
+    if(!r->inst) return;
+    PoolMesh* pm;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        pm = s->pool[r->mesh_id].get();
+        s->bytes_in_use -= r->bytes;
+        s->bytes_cached += r->bytes;
+    }
+    pm->cache[r->solver].push_back(r->inst);
+    r->inst = nullptr;
+}
+
+/* a request leaves the device: its final state is copied out on the copy
+ * stream (the class stream has finished with it); finish_leaving completes
+ * it after the next round has been launched */
+void leave(sfx_server* s, Request* r, int status) {
+    r->status = status;
+    if(r->inst) {
+        const size_t n = (size_t)sfx_mesh_dev(r->inst)->n_cells * sfx_mesh_dev(r->inst)->S;
+        r->stage = pinned_get(s, 2 * n);
+        if(r->stage.p) {
+            const int rc = sfx_mesh_download_fieldmajor_async(r->inst, r->stage.p, r->stage.p + n,
+                                                              s->copy_stream);
+            if(rc && r->status == SFX_OK) r->status = rc;
+        } else if(r->status == SFX_OK) {
+            r->status = SFX_ERR_NOMEM;
+        }
+    }
+    s->leaving.push_back(r);
+}
+
+void finish_leaving(sfx_server* s) {
+    if(s->leaving.empty()) return;
+    const bool copy_ok = cudaStreamSynchronize(s->copy_stream) == cudaSuccess;
+    for(Request* r : s->leaving) {
+        int status = r->status;
+        if(r->inst && r->stage.p) {
+            if(!copy_ok && status == SFX_OK) status = SFX_ERR_CUDA;
+            const sfx_dmesh* d = sfx_mesh_dev(r->inst);
+            const int64_t n = d->n_cells;
+            const int S = d->S;
+            r->W.resize((size_t)n * S);
+            r->Q.resize((size_t)n * S);
+            const double* w = r->stage.p;
+            const double* q = r->stage.p + (size_t)n * S;
+            for(int64_t i = 0; i < n; ++i)
+                for(int k = 0; k < S; ++k) {
+                    r->W[(size_t)i * S + k] = w[(size_t)k * n + i];
+                    r->Q[(size_t)i * S + k] = q[(size_t)k * n + i];
+                }
+        }
+        pinned_put(s, r->stage);
+        r->stage = Pinned();
+        release_instance(s, r);
+        mark_done(s, r, status);
+    }
+    s->leaving.clear();
+}
+
+/* free cached instances until `need` more bytes fit the budget (waits for
+ * the device; only when the budget is tight) */
+bool make_room(sfx_server* s, int64_t need) {
+    for(auto& pm : s->pool)
+        for(auto& cache : pm->cache)
+            while(!cache.empty()) {
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    if(s->bytes_in_use + s->bytes_cached + need <= s->cfg.memory_budget)
+                        return true;
+                    s->bytes_cached -= pm->clone_bytes;
+                }
+                sfx_mesh_free(cache.back());
+                cache.pop_back();
+            }
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->bytes_in_use + s->bytes_cached + need <= s->cfg.memory_budget;
+}
+
 /* admit queued requests in arrival order while budget and slots allow */
 void admit(sfx_server* s) {
     for(;;) {
         Request* r;
         PoolMesh* pm;
+        bool reuse;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             if(s->stop || s->queue.empty() || s->active >= s->cfg.max_active) return;
             r = s->queue.front();
             pm = s->pool[r->mesh_id].get();
-            if(s->bytes_in_use + pm->clone_bytes > s->cfg.memory_budget && s->active > 0) return;
+            reuse = !pm->cache[r->solver].empty();
+        }
+        if(!reuse) {
+            bool fits = make_room(s, pm->clone_bytes);
+            std::lock_guard<std::mutex> lk(s->mu);
+            /* one request is always admitted when nothing runs */
+            if(!fits && s->active > 0) return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
             s->queue.pop_front();
             s->bytes_in_use += pm->clone_bytes;
+            if(reuse) s->bytes_cached -= pm->clone_bytes;
             s->active += 1;
             s->n_admitted += 1;
         }
@@ -164,15 +290,22 @@ void admit(sfx_server* s) {
         r->remaining = r->nsteps;
         r->t_admit = now_s(s);
         Class& c = s->cls[pm->dim - 2][r->solver];
-        int rc = sfx_mesh_clone(c.ctx, pm->mesh, &r->inst);
-        if(!rc) rc = sfx_state_upload_W(r->inst, r->W0.data());
-        std::vector<double>().swap(r->W0);
-        if(rc) {
-            finish(s, r, rc);
-            continue;
+        int rc = SFX_OK;
+        if(reuse) {
+            r->inst = pm->cache[r->solver].back();
+            pm->cache[r->solver].pop_back();
+        } else {
+            rc = sfx_mesh_clone(c.ctx, pm->mesh, &r->inst);
+            if(rc) {
+                r->inst = nullptr;
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->bytes_in_use -= r->bytes;
+            }
         }
-        if(r->nsteps == 0) {
-            finish(s, r, SFX_OK);
+        if(!rc) rc = sfx_mesh_upload_W_fieldmajor(r->inst, r->W0.data());
+        std::vector<double>().swap(r->W0);
+        if(rc || r->nsteps == 0) {
+            leave(s, r, rc);
             continue;
         }
         c.members.push_back(r);
@@ -180,11 +313,9 @@ void admit(sfx_server* s) {
     }
 }
 
-int rebuild_group(sfx_server* s, Class& c) {
-    if(c.group) sfx_group_free(c.group);
-    c.group = nullptr;
+int rebuild_group(Class& c) {
     c.dirty = false;
-    if(c.members.empty()) return SFX_OK;
+    c.reused = 0;
     std::vector<sfx_mesh*> ms;
     std::vector<double> dts;
     std::vector<int32_t> steps;
@@ -193,46 +324,40 @@ int rebuild_group(sfx_server* s, Class& c) {
         dts.push_back(r->dt);
         steps.push_back(r->remaining);
     }
-    int rc = sfx_group_create(c.ctx, (int32_t)ms.size(), ms.data(), dts.data(), &c.group);
+    const int32_t n = (int32_t)ms.size();
+    if(c.group) return sfx_group_set_members(c.group, n, ms.data(), dts.data(), steps.data());
+    int rc = sfx_group_create(c.ctx, n, ms.data(), dts.data(), &c.group);
     if(!rc) rc = sfx_group_set_steps(c.group, steps.data());
     return rc;
 }
 
-void round_split(sfx_server* s) {
+void fail_class(sfx_server* s, Class& c, int rc) {
+    for(Request* r : c.members) leave(s, r, rc);
+    c.members.clear();
+    c.dirty = true;
+}
+
+void launch_split(sfx_server* s) {
     const int chunk = std::max(1, s->cfg.chunk_steps);
-    /* rebuild the groups whose membership changed first: freeing device
-     * memory waits for the whole device, so it must not sit between the
-     * launches of the classes */
     for(auto& row : s->cls)
         for(Class& c : row) {
-            if(c.members.empty()) {
-                if(c.group) sfx_group_free(c.group);
-                c.group = nullptr;
-                continue;
-            }
+            if(c.members.empty()) continue;
             if(c.dirty || !c.group) {
-                c.reused = 0;
-                int rc = rebuild_group(s, c);
+                const int rc = rebuild_group(c);
                 if(rc) {
-                    for(Request* r : c.members) finish(s, r, rc);
-                    c.members.clear();
+                    fail_class(s, c, rc);
+                    continue;
                 }
             } else {
                 c.reused += 1;
             }
+            /* a membership that has held for a round is replayed as a graph */
+            const int rc = sfx_group_step(c.group, chunk, c.reused > 0, nullptr);
+            if(rc) fail_class(s, c, rc);
         }
-    /* launch every class, then collect, so the classes overlap; a group
-     * that survives a round is replayed as a CUDA graph from then on */
-    for(auto& row : s->cls)
-        for(Class& c : row) {
-            if(c.members.empty() || !c.group) continue;
-            int rc = sfx_group_step(c.group, chunk, c.reused > 0, nullptr);
-            if(rc) {
-                for(Request* r : c.members) finish(s, r, rc);
-                c.members.clear();
-                c.dirty = true;
-            }
-        }
+}
+
+void collect_split(sfx_server* s) {
     for(auto& row : s->cls)
         for(Class& c : row) {
             if(c.members.empty() || !c.group) continue;
@@ -251,14 +376,14 @@ void round_split(sfx_server* s) {
             for(size_t i = 0; i < nm; ++i) {
                 Request* r = c.members[i];
                 if(rc) {
-                    finish(s, r, rc);
+                    leave(s, r, rc);
                     continue;
                 }
                 r->remaining = left[i];
                 if(st[i] != SFX_OK)
-                    finish(s, r, st[i]);
+                    leave(s, r, st[i]);
                 else if(left[i] == 0)
-                    finish(s, r, SFX_OK);
+                    leave(s, r, SFX_OK);
                 else
                     keep.push_back(r);
             }
@@ -267,7 +392,7 @@ void round_split(sfx_server* s) {
         }
 }
 
-void round_fp64(sfx_server* s) {
+void launch_fp64(sfx_server* s) {
     const int chunk = std::max(1, s->cfg.chunk_steps);
     for(auto& row : s->cls)
         for(Class& c : row)
@@ -275,6 +400,9 @@ void round_fp64(sfx_server* s) {
                 r->chunk = std::min(chunk, r->remaining);
                 if(sfx_step(r->inst, r->dt, r->chunk, nullptr) != SFX_OK) r->chunk = -1;
             }
+}
+
+void collect_fp64(sfx_server* s) {
     for(auto& row : s->cls)
         for(Class& c : row) {
             if(c.members.empty()) continue;
@@ -282,12 +410,12 @@ void round_fp64(sfx_server* s) {
             std::vector<Request*> keep;
             for(Request* r : c.members) {
                 int32_t bad = -1;
-                int st = r->chunk < 0 ? SFX_ERR_CUDA : sfx_mesh_last_status(r->inst, &bad);
+                const int st = r->chunk < 0 ? SFX_ERR_CUDA : sfx_mesh_last_status(r->inst, &bad);
                 if(r->chunk > 0) r->remaining -= r->chunk;
                 if(st != SFX_OK)
-                    finish(s, r, st);
+                    leave(s, r, st);
                 else if(r->remaining == 0)
-                    finish(s, r, SFX_OK);
+                    leave(s, r, SFX_OK);
                 else
                     keep.push_back(r);
             }
@@ -297,30 +425,37 @@ void round_fp64(sfx_server* s) {
 
 void worker_main(sfx_server* s) {
     cudaSetDevice(s->cfg.device);
+    const bool split = s->cfg.precision == SFX_PREC_SPLIT;
     for(;;) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
             if(s->stop) break;
         }
         admit(s);
-        int active;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            active = s->active;
-        }
-        if(active == 0) {
+        bool any = false;
+        for(auto& row : s->cls)
+            for(Class& c : row) any = any || !c.members.empty();
+        if(!any) {
+            finish_leaving(s);
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait_for(lk, std::chrono::milliseconds(20),
                                 [&] { return s->stop || !s->queue.empty(); });
             continue;
         }
-        if(s->cfg.precision == SFX_PREC_SPLIT)
-            round_split(s);
+        if(split)
+            launch_split(s);
         else
-            round_fp64(s);
+            launch_fp64(s);
+        /* the previous round's results, while this round runs */
+        finish_leaving(s);
+        if(split)
+            collect_split(s);
+        else
+            collect_fp64(s);
         std::lock_guard<std::mutex> lk(s->mu);
         s->rounds += 1;
     }
+    finish_leaving(s);
 }
 
 }  // namespace
@@ -335,7 +470,9 @@ extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out)
     if(!s) return SFX_ERR_NOMEM;
     s->cfg = *cfg;
     s->t0 = std::chrono::steady_clock::now();
-    int rc = SFX_OK;
+    int rc = cudaSetDevice(cfg->device) == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+    if(!rc && cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        rc = SFX_ERR_CUDA;
     for(int d = 0; d < 2 && !rc; ++d) {
         sfx_config pc = make_cfg(s, d + 2, SFX_SOLVER_HLLC);
         rc = sfx_ctx_create(&pc, &s->pool_ctx[d]);
@@ -361,6 +498,7 @@ extern "C" int sfx_server_add_mesh(sfx_server* s, const sfx_mesh_desc* desc, int
     int rc = sfx_mesh_upload(s->pool_ctx[desc->dim - 2], desc, &pm->mesh);
     if(rc) return rc;
     pm->dim = desc->dim;
+    pm->S = desc->dim + 2;
     pm->n_cells = desc->n_cells;
     for(int32_t f = 0; f < desc->n_faces; ++f) pm->active_faces += desc->face_area[f] != 0.;
     pm->clone_bytes = sfx_mesh_clone_bytes(pm->mesh, s->cfg.precision);
@@ -390,9 +528,12 @@ extern "C" int sfx_server_submit(sfx_server* s, int32_t mesh_id, const double* W
             return SFX_ERR_INVALID;
         }
         n = s->pool[mesh_id]->n_cells;
-        S = s->pool[mesh_id]->dim + 2;
+        S = s->pool[mesh_id]->S;
     }
-    r->W0.assign(W0, W0 + (size_t)n * S);
+    /* the device layout, transposed here on the caller's thread */
+    r->W0.resize((size_t)n * S);
+    for(int64_t i = 0; i < n; ++i)
+        for(int k = 0; k < S; ++k) r->W0[(size_t)k * n + i] = W0[(size_t)i * S + k];
     r->mesh_id = mesh_id;
     r->solver = solver;
     r->dt = dt;
@@ -479,6 +620,7 @@ extern "C" int sfx_server_shutdown(sfx_server* s) {
     for(auto& row : s->cls)
         for(Class& c : row) {
             if(c.group) sfx_group_free(c.group);
+            c.group = nullptr;
             for(Request* r : c.members)
                 if(r->inst) {
                     sfx_mesh_free(r->inst);
@@ -488,17 +630,24 @@ extern "C" int sfx_server_shutdown(sfx_server* s) {
         }
     for(auto& kv : s->reqs) {
         if(kv.second->inst) sfx_mesh_free(kv.second->inst);
+        if(kv.second->stage.p) cudaFreeHost(kv.second->stage.p);
         delete kv.second;
     }
     s->reqs.clear();
-    for(auto& pm : s->pool)
+    for(auto& pm : s->pool) {
+        for(auto& cache : pm->cache)
+            for(sfx_mesh* m : cache) sfx_mesh_free(m);
         if(pm->mesh) sfx_mesh_free(pm->mesh);
+    }
     s->pool.clear();
+    for(Pinned& b : s->pinned_free) cudaFreeHost(b.p);
+    s->pinned_free.clear();
     for(auto& row : s->cls)
         for(Class& c : row)
             if(c.ctx) sfx_ctx_destroy(c.ctx);
     for(sfx_ctx* c : s->pool_ctx)
         if(c) sfx_ctx_destroy(c);
+    if(s->copy_stream) cudaStreamDestroy(s->copy_stream);
     delete s;
     return SFX_OK;
 }

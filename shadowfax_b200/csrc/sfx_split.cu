@@ -696,15 +696,6 @@ __device__ __forceinline__ void shllc(float g, const float* WL, const float* WR,
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
  * 462-546) with the device pow; returns 0 or SFX_ERR_* */
-/* x^y for the exponents 2/(g-1) and 2g/(g-1): by repeated multiplication
- * when k (the exponent, if a small integer) is nonzero, else pow */
-__device__ __forceinline__ double kpow(double x, int k, double y) {
-    if(k == 0) return pow(x, y);
-    double r = x;
-    for(int i = 1; i < k; ++i) r *= x;
-    return r;
-}
-
 template <int D>
 struct XS {
     const sfx_solver_params& s;
@@ -777,14 +768,14 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         for(int k = 0; k < S; ++k) sol[k] = Ws[k];
         if(side == 2) {
             const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-            sol[0] = WL[0] * kpow(base, s.k_tdgm1, s.tdgm1);
+            sol[0] = WL[0] * pow(base, s.tdgm1);
             vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-            sol[D + 1] = WL[D + 1] * kpow(base, s.k_tgdgm1, s.tgdgm1);
+            sol[D + 1] = WL[D + 1] * pow(base, s.tgdgm1);
         } else if(side == 4) {
             const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-            sol[0] = WR[0] * kpow(base, s.k_tdgm1, s.tdgm1);
+            sol[0] = WR[0] * pow(base, s.tdgm1);
             vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-            sol[D + 1] = WR[D + 1] * kpow(base, s.k_tgdgm1, s.tgdgm1);
+            sol[D + 1] = WR[D + 1] * pow(base, s.tgdgm1);
         }
     } else {
         XS<D> x{s};
@@ -797,9 +788,9 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         if(pmax / pmin <= 2. && pmin <= ppv && ppv <= pmax) {
             pg = ppv;
         } else if(ppv < pmin) {
-            pg = kpow((aL + aR - s.gm1d2 * (vR - vL)) /
-                          (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
-                      s.k_tgdgm1, s.tgdgm1);
+            pg = pow((aL + aR - s.gm1d2 * (vR - vL)) /
+                         (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
+                     s.tgdgm1);
         } else {
             const double gL = sqrt(s.tdgp1 / WL[0] / (ppv + s.gm1dgp1 * pL));
             const double gR = sqrt(s.tdgp1 / WR[0] / (ppv + s.gm1dgp1 * pR));
@@ -915,12 +906,12 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             } else if(vR + aR > 0.) {
                 if(u + aR * zR <= 0.) {
                     const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-                    sol[0] = WR[0] * kpow(base, s.k_tdgm1, s.tdgm1);
+                    sol[0] = WR[0] * pow(base, s.tdgm1);
                     vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-                    sol[D + 1] = pR * kpow(base, s.k_tgdgm1, s.tgdgm1);
+                    sol[D + 1] = pR * pow(base, s.tgdgm1);
                 } else {
                     /* r^(1/g) = z^(2/(g-1)) with z = r^((g-1)/(2g)) */
-                    sol[0] = WR[0] * (s.k_tdgm1 ? kpow(zR, s.k_tdgm1, 0.) : pow(r, s.ginv));
+                    sol[0] = WR[0] * pow(r, s.ginv);
                     sol[D + 1] = p;
                     vhalf = u - vR;
                 }
@@ -938,11 +929,11 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             } else if(vL - aL < 0.) {
                 if(u - aL * zL > 0.) {
                     const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-                    sol[0] = WL[0] * kpow(base, s.k_tdgm1, s.tdgm1);
+                    sol[0] = WL[0] * pow(base, s.tdgm1);
                     vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-                    sol[D + 1] = pL * kpow(base, s.k_tgdgm1, s.tgdgm1);
+                    sol[D + 1] = pL * pow(base, s.tgdgm1);
                 } else {
-                    sol[0] = WL[0] * (s.k_tdgm1 ? kpow(zL, s.k_tdgm1, 0.) : pow(r, s.ginv));
+                    sol[0] = WL[0] * pow(r, s.ginv);
                     sol[D + 1] = p;
                     vhalf = u - vL;
                 }
