@@ -3,7 +3,8 @@
 ``python -m shadowfax_b200.build`` (or ``build_library()``) compiles
 
 * ``csrc/sfx_fp64.cu``   plain-FP64 kernels, ``-fmad=false`` (bit parity)
-* ``csrc/sfx_split.cu``  FP32/FP64-split and batched kernels (FMA allowed)
+* ``csrc/sfx_split.cu``  FP32/FP64-split and batched kernels (FMA allowed, FP32
+  division and square root approximate)
 * ``csrc/sfx_api.cu``    C ABI (include/sfxflux.h)
 * ``csrc/sfx_voronoi.cpp`` host face-list builder
 
@@ -33,7 +34,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp-con
 # per-source extra flags
 UNITS = {
     "sfx_fp64.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
-    "sfx_split.cu": ["-fmad=true"],
+    # FP32 division and square root by the hardware approximations (about
+    # 2 ulp); FP64 operations stay IEEE
+    "sfx_split.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"],
     "sfx_api.cu": [],
     "sfx_noalloc.cu": [],
     "sfx_group.cu": [],

@@ -696,6 +696,13 @@ __device__ __forceinline__ void shllc(float g, const float* WL, const float* WR,
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
  * 462-546) with the device pow; returns 0 or SFX_ERR_* */
+/* pow for the exact solver, out of line: one copy of its code instead of one
+ * per call site keeps the face kernel's instruction footprint small (the
+ * kernel stalled on instruction fetch with the copies inlined) */
+__device__ __noinline__ double xpow(double x, double y) {
+    return pow(x, y);
+}
+
 template <int D>
 struct XS {
     const sfx_solver_params& s;
@@ -704,7 +711,7 @@ struct XS {
             const double A = s.tdgp1 / Wb[0], B = s.gm1dgp1 * Wb[D + 1];
             return (p - Wb[D + 1]) * sqrt(A / (p + B));
         }
-        return s.tdgm1 * a * (pow(p / Wb[D + 1], s.gm1d2g) - 1.);
+        return s.tdgm1 * a * (xpow(p / Wb[D + 1], s.gm1d2g) - 1.);
     }
     /* f_K, f_K' and, on the rarefaction side, z = (p/p_K)^((g-1)/(2g)) at
      * one pressure: f_K' = r^(-(g+1)/(2g)) / (rho_K a_K) = z / (r rho_K a_K)
@@ -719,9 +726,9 @@ struct XS {
             z = 0.;
         } else {
             const double r = p / Wb[D + 1];
-            z = pow(r, s.gm1d2g);
+            z = xpow(r, s.gm1d2g);
             f = s.tdgm1 * a * (z - 1.);
-            fp = r > 0. ? z / (r * (Wb[0] * a)) : 1. / (Wb[0] * a) * pow(r, -s.gp1d2g);
+            fp = r > 0. ? z / (r * (Wb[0] * a)) : 1. / (Wb[0] * a) * xpow(r, -s.gp1d2g);
         }
     }
 };
@@ -768,14 +775,14 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         for(int k = 0; k < S; ++k) sol[k] = Ws[k];
         if(side == 2) {
             const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-            sol[0] = WL[0] * pow(base, s.tdgm1);
+            sol[0] = WL[0] * xpow(base, s.tdgm1);
             vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-            sol[D + 1] = WL[D + 1] * pow(base, s.tgdgm1);
+            sol[D + 1] = WL[D + 1] * xpow(base, s.tgdgm1);
         } else if(side == 4) {
             const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-            sol[0] = WR[0] * pow(base, s.tdgm1);
+            sol[0] = WR[0] * xpow(base, s.tdgm1);
             vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-            sol[D + 1] = WR[D + 1] * pow(base, s.tgdgm1);
+            sol[D + 1] = WR[D + 1] * xpow(base, s.tgdgm1);
         }
     } else {
         XS<D> x{s};
@@ -788,8 +795,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         if(pmax / pmin <= 2. && pmin <= ppv && ppv <= pmax) {
             pg = ppv;
         } else if(ppv < pmin) {
-            pg = pow((aL + aR - s.gm1d2 * (vR - vL)) /
-                         (aL / pow(pL, s.gm1d2g) + aR / pow(pR, s.gm1d2g)),
+            pg = xpow((aL + aR - s.gm1d2 * (vR - vL)) /
+                         (aL / xpow(pL, s.gm1d2g) + aR / xpow(pR, s.gm1d2g)),
                      s.tgdgm1);
         } else {
             const double gL = sqrt(s.tdgp1 / WL[0] / (ppv + s.gm1dgp1 * pL));
@@ -906,12 +913,12 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             } else if(vR + aR > 0.) {
                 if(u + aR * zR <= 0.) {
                     const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-                    sol[0] = WR[0] * pow(base, s.tdgm1);
+                    sol[0] = WR[0] * xpow(base, s.tdgm1);
                     vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-                    sol[D + 1] = pR * pow(base, s.tgdgm1);
+                    sol[D + 1] = pR * xpow(base, s.tgdgm1);
                 } else {
                     /* r^(1/g) = z^(2/(g-1)) with z = r^((g-1)/(2g)) */
-                    sol[0] = WR[0] * pow(r, s.ginv);
+                    sol[0] = WR[0] * xpow(r, s.ginv);
                     sol[D + 1] = p;
                     vhalf = u - vR;
                 }
@@ -929,11 +936,11 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             } else if(vL - aL < 0.) {
                 if(u - aL * zL > 0.) {
                     const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-                    sol[0] = WL[0] * pow(base, s.tdgm1);
+                    sol[0] = WL[0] * xpow(base, s.tdgm1);
                     vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-                    sol[D + 1] = pL * pow(base, s.tgdgm1);
+                    sol[D + 1] = pL * xpow(base, s.tgdgm1);
                 } else {
-                    sol[0] = WL[0] * pow(r, s.ginv);
+                    sol[0] = WL[0] * xpow(r, s.ginv);
                     sol[D + 1] = p;
                     vhalf = u - vL;
                 }
