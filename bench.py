@@ -472,7 +472,7 @@ def run_served(pool, reqs, precision, chunk, sample_every, device=0):
     return [results[j] for j in range(len(reqs))], launches, st
 
 
-def served_summary(res, reqs):
+def served_summary(res, reqs, st=None):
     ok = [r for r in res if r.status == 0]
     lat = np.array([r.t_done - r.t_submit for r in ok]) if ok else np.zeros(1)
     t0 = min(r.t_submit for r in res)
@@ -482,7 +482,11 @@ def served_summary(res, reqs):
             "failed": len(res) - len(ok), "face_steps": int(fs), "makespan_s": t1 - t0,
             "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)),
-            "mean_latency_s": float(lat.mean())}
+            "mean_latency_s": float(lat.mean()),
+            "rounds": int(st.rounds) if st is not None else None,
+            "worker_s": {k: round(float(v), 3) for k, v in
+                         zip(("admit", "launch", "finish", "collect"), st.worker_s)}
+            if st is not None else None}
 
 
 def run_resident(pool, reqs, chunk, torch, local):
@@ -679,9 +683,10 @@ def bench_serve(args, rank, world, local, torch):
                                            sample_every, local)
         clk.mark("t1")
         time.sleep(0.3)
-    res64, launches64, _ = run_served(pool, reqs, L.PREC_FP64, args.chunk, sample_every, local)
-    split = served_summary(res32, reqs)
-    fp64 = served_summary(res64, reqs)
+    res64, launches64, st64 = run_served(pool, reqs, L.PREC_FP64, args.chunk, sample_every,
+                                         local)
+    split = served_summary(res32, reqs, st32)
+    fp64 = served_summary(res64, reqs, st64)
     # accuracy and conservation on the sampled requests
     errs, drift = [], []
     for j in range(0, len(reqs), sample_every):

@@ -315,6 +315,8 @@ typedef struct sfx_server_stats {
     int64_t bytes_in_use;   /* device bytes of admitted request states        */
     int64_t rounds;         /* scheduling rounds run                          */
     double now;             /* server clock, seconds                          */
+    double worker_s[4];     /* worker thread time in admission, launches,
+                               completing results, and waiting for rounds    */
 } sfx_server_stats;
 
 int sfx_server_create(const sfx_server_config* cfg, sfx_server** out);

@@ -87,6 +87,8 @@ class Oracle:
                                    _ip]
         L.sfxo_pow.argtypes = [C.c_double, C.c_double]
         L.sfxo_pow.restype = C.c_double
+        L.sfxo_pow_fast.argtypes = [C.c_double, C.c_double]
+        L.sfxo_pow_fast.restype = C.c_double
         self.L = L
 
     @staticmethod
@@ -169,6 +171,9 @@ class Oracle:
 
     def pow(self, x: float, y: float) -> float:
         return self.L.sfxo_pow(x, y)
+
+    def pow_fast(self, x: float, y: float) -> float:
+        return self.L.sfxo_pow_fast(x, y)
 
 
 # ---------------------------------------------------------------- reference

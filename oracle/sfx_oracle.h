@@ -67,6 +67,7 @@ int sfxo_riemann(int dim, const sfxo_params* p, int n, const double* WL,
                  const double* WR, const double* normal, int reflective,
                  double* half, double* flux, int* code);
 double sfxo_pow(double x, double y);
+double sfxo_pow_fast(double x, double y);
 
 #ifdef __cplusplus
 }

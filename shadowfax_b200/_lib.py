@@ -92,7 +92,7 @@ class sfx_server_stats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
                 ("failed", C.c_int64), ("active", C.c_int64), ("queued", C.c_int64),
                 ("face_steps", C.c_int64), ("bytes_in_use", C.c_int64), ("rounds", C.c_int64),
-                ("now", C.c_double)]
+                ("now", C.c_double), ("worker_s", C.c_double * 4)]
 
 
 class sfx_stats(C.Structure):

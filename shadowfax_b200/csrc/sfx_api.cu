@@ -105,17 +105,16 @@ int check_err(sfx_mesh* m, sfx_stats* st) {
 }
 
 /* one phase of a step: 0 gradients, 1 face fluxes, 2 update */
-/* queued slow faces per mesh: 1/32 of the faces, at least 256 (a face that
- * finds the queue full is solved in place) */
+/* queued slow faces per mesh: room for every face, so the face kernel never
+ * has to run Brent's method itself (and carries none of its code) */
 int32_t slowq_capacity(int64_t n_faces) {
-    const int64_t c = n_faces / 32;
-    return (int32_t)(c < 256 ? 256 : c);
+    return (int32_t)(n_faces > 0 ? n_faces : 1);
 }
 
 /* device table of a split mesh as a one-member launch group */
 int setup_self(sfx_mesh* m, cudaStream_t s) {
-    SFX_TRY(dalloc(m, &m->self_tab, 1));
-    SFX_TRY(dalloc(m, &m->self_pre, 6));
+    if(!m->self_tab) SFX_TRY(dalloc(m, &m->self_tab, 1));
+    if(!m->self_pre) SFX_TRY(dalloc(m, &m->self_pre, 6));
     sfx_group_entry e;
     std::memset(&e, 0, sizeof e);
     e.m = m->d;
@@ -153,12 +152,92 @@ int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t 
     }
 }
 
-int reset_err(sfx_mesh* m) {
+int reset_err_on(sfx_mesh* m, cudaStream_t s) {
     sfx_dev_error e;
     e.face_key = ~0ull;
     e.cell_key = ~0ull;
-    return cuda_ok(cudaMemcpyAsync(m->d.err, &e, sizeof e, cudaMemcpyHostToDevice,
-                                   m->ctx->stream));
+    /* pageable source: staged before the call returns */
+    return cuda_ok(cudaMemcpyAsync(m->d.err, &e, sizeof e, cudaMemcpyHostToDevice, s));
+}
+
+int reset_err(sfx_mesh* m) {
+    return reset_err_on(m, m->ctx->stream);
+}
+
+/* a state on base's geometry: one device block carved into the arrays,
+ * set up on stream s (waited for when `wait`) */
+int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh** out) {
+    if(!ctx || !base || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    const sfx_dmesh& b = base->d;
+    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
+    if(ctx->cfg.dim != b.dim || ctx->closing) return SFX_ERR_INVALID;
+    if(split && !b.fg) return SFX_ERR_INVALID; /* base has no split geometry */
+    if(cudaSetDevice(ctx->cfg.device) != cudaSuccess) return SFX_ERR_CUDA;
+    sfx_mesh* m = new(std::nothrow) sfx_mesh;
+    if(!m) return SFX_ERR_NOMEM;
+    m->ctx = ctx;
+    ctx->live_meshes++;
+    m->d = b; /* geometry pointers shared with the base */
+    sfx_dmesh& d = m->d;
+    const int64_t n = d.n_cells, F = d.n_faces;
+    const int S = d.S, dim = d.dim;
+    d.W = d.Q = d.grad = d.dQf = nullptr;
+    d.branch = nullptr;
+    d.err = nullptr;
+    d.totals_scratch = nullptr;
+    d.cw = d.cg = nullptr;
+    d.dqm = nullptr;
+    d.dqv = nullptr;
+    d.slowq = d.slowq_n = nullptr;
+    d.slowq_cap = 0;
+    struct Slot {
+        void** p;
+        size_t bytes;
+    };
+    std::vector<Slot> slots;
+    auto A = [&](auto** p, size_t c) { slots.push_back({(void**)p, c * sizeof(**p)}); };
+    A(&d.W, n * S);
+    A(&d.Q, n * S);
+    A(&d.err, 1);
+    A(&d.totals_scratch, (size_t)(S + 1) * 1024);
+    if(split) {
+        A(&d.cw, 2 * n);
+        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
+        A(&d.dqm, F);
+        A(&d.dqv, (size_t)dim * F);
+        d.slowq_cap = slowq_capacity(F);
+        A(&d.slowq, (size_t)d.slowq_cap);
+        A(&d.slowq_n, 1);
+        A(&m->self_tab, 1);
+        A(&m->self_pre, 6);
+    } else {
+        A(&d.grad, n * dim * S);
+        A(&d.dQf, F * S);
+        A(&d.branch, F);
+    }
+    size_t total = 0;
+    for(const Slot& sl : slots) total = ((total + 255) & ~(size_t)255) + sl.bytes;
+    uint8_t* block = nullptr;
+    int rc = dalloc(m, &block, total);
+    if(!rc) {
+        size_t off = 0;
+        for(const Slot& sl : slots) {
+            off = (off + 255) & ~(size_t)255;
+            *sl.p = block + off;
+            off += sl.bytes;
+        }
+    }
+    if(!rc) rc = reset_err_on(m, s);
+    if(!rc && split) rc = cuda_ok(cudaMemsetAsync(d.slowq_n, 0, sizeof(int32_t), s));
+    if(!rc && split) rc = setup_self(m, s);
+    if(!rc && wait) rc = cuda_ok(cudaStreamSynchronize(s));
+    if(rc) {
+        sfx_mesh_free(m);
+        return rc;
+    }
+    *out = m;
+    return SFX_OK;
 }
 
 }  // namespace
@@ -268,11 +347,17 @@ int sfx_ctx_synchronize(sfx_ctx* ctx) {
 
 int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
                               int64_t nnz, int32_t precision) {
-    (void)precision;
     const int64_t S = dim + 2, n = n_cells, F = n_faces;
     int64_t cells = n * (8 * (2 * dim + 2 + 2 * S + dim * S) + 4) + 4;
     int64_t faces = F * (8 * (1 + 3 * dim + S) + 4 * 4);
-    return cells + faces + nnz * 4 + 8 * 8 * 1024 + 4096;
+    int64_t bytes = cells + faces + nnz * 4 + 8 * 8 * 1024 + 4096;
+    if(precision == SFX_PREC_SPLIT) {
+        /* fg, fi, fsh, an, dqm, dqv, queue; cw, cg, cx, self table; nbe */
+        bytes += F * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + 4 * slowq_capacity(F) + 4;
+        bytes += n * (32 + 16 * ((dim * S + 3) / 4) + 16) + 256;
+        bytes += nnz * 4;
+    }
+    return bytes;
 }
 
 int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
@@ -429,6 +514,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         A(&d.cw, 2 * n);
         A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
         A(&d.cx, n);
+        A(&d.nbe, nnz);
         A(&d.an, (size_t)dim * F);
         A(&d.dqm, F);
         A(&d.dqv, (size_t)dim * F);
@@ -453,6 +539,19 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     if(!rc) rc = h2d(d.tarea, desc->cell_total_area, n, s);
     if(!rc) rc = h2d(d.off, off, n + 1, s);
     if(!rc) rc = h2d(d.idx, split ? idx_split.data() : idx.data(), nnz, s);
+    std::vector<int32_t> nbe;
+    if(split) {
+        /* the neighbour of each CSR entry, so the gradient kernel loads it
+         * beside the face id instead of after it */
+        nbe.resize(nnz);
+        for(int64_t j = 0; j < nnz; ++j) {
+            const uint32_t e = (uint32_t)idx_split[j];
+            const int32_t f = (int32_t)(e & 0x7fffffffu);
+            nbe[j] = (e >> 31) ? desc->face_left[f]
+                               : (desc->face_kind[f] == SFX_FACE_MIRROR ? -1 : desc->face_right[f]);
+        }
+        if(!rc) rc = h2d(d.nbe, nbe.data(), nnz, s);
+    }
     if(!rc && split) rc = h2d(d.fsh, skip.data(), F, s);
     if(!rc) rc = h2d(d.area, desc->face_area, F, s);
     if(!rc) rc = h2d(d.mid, t3.data(), t3.size(), s);
@@ -668,61 +767,7 @@ int sfx_riemann_eval(sfx_ctx* c, int32_t n, const double* WL, const double* WR,
 }
 
 int sfx_mesh_clone(sfx_ctx* ctx, sfx_mesh* base, sfx_mesh** out) {
-    if(!ctx || !base || !out) return SFX_ERR_INVALID;
-    *out = nullptr;
-    const sfx_dmesh& b = base->d;
-    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
-    if(ctx->cfg.dim != b.dim || ctx->closing) return SFX_ERR_INVALID;
-    if(split && !b.fg) return SFX_ERR_INVALID; /* base has no split geometry */
-    if(cudaSetDevice(ctx->cfg.device) != cudaSuccess) return SFX_ERR_CUDA;
-    sfx_mesh* m = new(std::nothrow) sfx_mesh;
-    if(!m) return SFX_ERR_NOMEM;
-    m->ctx = ctx;
-    ctx->live_meshes++;
-    m->d = b; /* geometry pointers shared with the base */
-    sfx_dmesh& d = m->d;
-    const int64_t n = d.n_cells, F = d.n_faces;
-    const int S = d.S, dim = d.dim;
-    d.W = d.Q = d.grad = d.dQf = nullptr;
-    d.branch = nullptr;
-    d.err = nullptr;
-    d.totals_scratch = nullptr;
-    d.cw = d.cg = nullptr;
-    d.dqm = nullptr;
-    d.dqv = nullptr;
-    int rc = SFX_OK;
-    auto A = [&](auto** p, size_t c) {
-        if(rc == SFX_OK) rc = dalloc(m, p, c);
-    };
-    A(&d.W, n * S);
-    A(&d.Q, n * S);
-    A(&d.err, 1);
-    A(&d.totals_scratch, (size_t)(S + 1) * 1024);
-    d.slowq = d.slowq_n = nullptr;
-    d.slowq_cap = 0;
-    if(split) {
-        A(&d.cw, 2 * n);
-        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
-        A(&d.dqm, F);
-        A(&d.dqv, (size_t)dim * F);
-        d.slowq_cap = slowq_capacity(F);
-        A(&d.slowq, (size_t)d.slowq_cap);
-        A(&d.slowq_n, 1);
-    } else {
-        A(&d.grad, n * dim * S);
-        A(&d.dQf, F * S);
-        A(&d.branch, F);
-    }
-    if(!rc) rc = reset_err(m);
-    if(!rc && split) rc = cuda_ok(cudaMemsetAsync(d.slowq_n, 0, sizeof(int32_t), ctx->stream));
-    if(!rc && split) rc = setup_self(m, ctx->stream);
-    if(!rc) rc = cuda_ok(cudaStreamSynchronize(ctx->stream));
-    if(rc) {
-        sfx_mesh_free(m);
-        return rc;
-    }
-    *out = m;
-    return SFX_OK;
+    return clone_impl(ctx, base, ctx ? ctx->stream : nullptr, true, out);
 }
 
 int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
@@ -770,4 +815,18 @@ int sfx_mesh_download_fieldmajor_async(sfx_mesh* m, double* W, double* Q, void* 
     if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_export_W(&m->d, s));
     SFX_TRY(cuda_ok(cudaMemcpyAsync(W, m->d.W, bytes, cudaMemcpyDeviceToHost, s)));
     return cuda_ok(cudaMemcpyAsync(Q, m->d.Q, bytes, cudaMemcpyDeviceToHost, s));
+}
+
+int sfx_mesh_clone_async(sfx_ctx* ctx, sfx_mesh* base, void* stream, sfx_mesh** out) {
+    return clone_impl(ctx, base, (cudaStream_t)stream, false, out);
+}
+
+int sfx_mesh_upload_W_fieldmajor_async(sfx_mesh* m, const double* W, void* stream) {
+    if(!m || !W) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    SFX_TRY(reset_err_on(m, s));
+    SFX_TRY(h2d(m->d.W, W, (size_t)m->d.n_cells * m->d.S, s));
+    SFX_TRY(sfx_fp64_init_Q(&m->d, &m->ctx->sp, s));
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_load_state(&m->d, s));
+    return SFX_OK;
 }

@@ -72,12 +72,13 @@ struct sfx_dmesh {
     float4* cw;
     float4* cg;
     float4* cx;
+    int32_t* nbe; /* [nnz] neighbour cell of each CSR entry (-1 mirror) */
     double* an;
     float2* dqm;
     double* dqv;
     /* exact solver, split pass: faces whose p* iteration falls back to
-     * Brent's method are queued here by the face kernel (face ids, up to
-     * slowq_cap; slowq_n counts them) and solved by a follow-up launch in
+     * Brent's method are queued here by the face kernel (face ids; room for
+     * every face; slowq_n counts them) and solved by a follow-up launch in
      * which every lane works on a queued face, instead of one lane of a warp
      * iterating while the other 31 wait.  The gradient kernel resets the
      * count each step. */
@@ -161,6 +162,12 @@ int sfx_group_set_members(sfx_group* g, int32_t n, sfx_mesh* const* meshes, cons
  * the download enqueues the copies on `stream` and returns at once */
 int sfx_mesh_upload_W_fieldmajor(sfx_mesh* m, const double* W);
 int sfx_mesh_download_fieldmajor_async(sfx_mesh* m, double* W, double* Q, void* stream);
+/* the same without waiting, all device work on `stream` (W must stay valid
+ * until the stream has run it); errors of the upload land in the mesh's
+ * error record (sfx_mesh_last_status after the stream has finished) */
+int sfx_mesh_upload_W_fieldmajor_async(sfx_mesh* m, const double* W, void* stream);
+/* sfx_mesh_clone with its device setup on `stream`, not waited for */
+int sfx_mesh_clone_async(sfx_ctx* ctx, sfx_mesh* base, void* stream, sfx_mesh** out);
 
 /* grouped launches (sfx_split.cu) */
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);

@@ -54,6 +54,7 @@ struct Pinned {
 
 struct Request {
     int64_t id = 0;
+    int32_t admit_status = SFX_OK;
     int32_t mesh_id = 0, solver = 0, nsteps = 0;
     double dt = 0.;
     std::vector<double> W0; /* field-major [S][n], transposed at submit */
@@ -104,12 +105,15 @@ struct sfx_server {
     int64_t bytes_cached = 0; /* idle instances kept for reuse */
     int active = 0;
     bool stop = false;
+    double worker_s[4] = {0., 0., 0., 0.}; /* admit, launch, finish, collect */
     std::thread worker;
     std::chrono::steady_clock::time_point t0;
     /* worker thread only */
-    cudaStream_t copy_stream = nullptr;
+    cudaStream_t copy_stream = nullptr; /* results out */
+    cudaStream_t up_stream = nullptr;   /* admitted states in */
     std::vector<Pinned> pinned_free;
-    std::vector<Request*> leaving; /* results being copied out */
+    std::vector<Request*> leaving;  /* results being copied out */
+    std::vector<Request*> arriving; /* admitted, states being copied in */
 };
 
 namespace {
@@ -259,7 +263,10 @@ bool make_room(sfx_server* s, int64_t need) {
     return s->bytes_in_use + s->bytes_cached + need <= s->cfg.memory_budget;
 }
 
-/* admit queued requests in arrival order while budget and slots allow */
+/* admit queued requests in arrival order while budget and slots allow: take
+ * an instance (cached, or a new clone) and start copying the state in on the
+ * upload stream; join_arrivals adds them to their classes once it has run.
+ * Called while a round runs, so the host work overlaps the GPU. */
 void admit(sfx_server* s) {
     for(;;) {
         Request* r;
@@ -295,22 +302,55 @@ void admit(sfx_server* s) {
             r->inst = pm->cache[r->solver].back();
             pm->cache[r->solver].pop_back();
         } else {
-            rc = sfx_mesh_clone(c.ctx, pm->mesh, &r->inst);
+            rc = sfx_mesh_clone_async(c.ctx, pm->mesh, s->up_stream, &r->inst);
             if(rc) {
                 r->inst = nullptr;
                 std::lock_guard<std::mutex> lk(s->mu);
                 s->bytes_in_use -= r->bytes;
             }
         }
-        if(!rc) rc = sfx_mesh_upload_W_fieldmajor(r->inst, r->W0.data());
+        if(!rc) {
+            r->stage = pinned_get(s, r->W0.size());
+            if(r->stage.p) {
+                std::memcpy(r->stage.p, r->W0.data(), r->W0.size() * sizeof(double));
+                rc = sfx_mesh_upload_W_fieldmajor_async(r->inst, r->stage.p, s->up_stream);
+            } else {
+                rc = SFX_ERR_NOMEM;
+            }
+        }
         std::vector<double>().swap(r->W0);
+        r->admit_status = rc;
+        s->arriving.push_back(r);
+    }
+}
+
+/* admitted requests whose states have arrived join their classes */
+void join_arrivals(sfx_server* s) {
+    if(s->arriving.empty()) return;
+    const bool up_ok = cudaStreamSynchronize(s->up_stream) == cudaSuccess;
+    for(Request* r : s->arriving) {
+        pinned_put(s, r->stage);
+        r->stage = Pinned();
+        int rc = r->admit_status;
+        if(!rc && !up_ok) rc = SFX_ERR_CUDA;
+        if(!rc) {
+            int32_t bad = -1;
+            rc = sfx_mesh_last_status(r->inst, &bad);
+        }
         if(rc || r->nsteps == 0) {
             leave(s, r, rc);
             continue;
         }
+        PoolMesh* pm;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            pm = s->pool[r->mesh_id].get();
+        }
+        Class& c = s->cls[pm->dim - 2][r->solver];
         c.members.push_back(r);
         c.dirty = true;
     }
+    s->arriving.clear();
 }
 
 int rebuild_group(Class& c) {
@@ -426,35 +466,59 @@ void collect_fp64(sfx_server* s) {
 void worker_main(sfx_server* s) {
     cudaSetDevice(s->cfg.device);
     const bool split = s->cfg.precision == SFX_PREC_SPLIT;
+    double tw[4] = {0., 0., 0., 0.};
+    auto lap = [&](double& t0, int k) {
+        const double t1 = now_s(s);
+        tw[k] += t1 - t0;
+        t0 = t1;
+    };
     for(;;) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
             if(s->stop) break;
+            for(int k = 0; k < 4; ++k) s->worker_s[k] = tw[k];
         }
-        admit(s);
+        double t = now_s(s);
         bool any = false;
         for(auto& row : s->cls)
             for(Class& c : row) any = any || !c.members.empty();
-        if(!any) {
-            finish_leaving(s);
-            std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait_for(lk, std::chrono::milliseconds(20),
-                                [&] { return s->stop || !s->queue.empty(); });
+        /* launch the round first; admissions and finished results are
+         * handled while it runs */
+        if(any) {
+            if(split)
+                launch_split(s);
+            else
+                launch_fp64(s);
+        }
+        lap(t, 1);
+        admit(s);
+        lap(t, 0);
+        finish_leaving(s);
+        lap(t, 2);
+        if(any) {
+            if(split)
+                collect_split(s);
+            else
+                collect_fp64(s);
+        }
+        lap(t, 3);
+        join_arrivals(s);
+        lap(t, 0);
+        if(any) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->rounds += 1;
             continue;
         }
-        if(split)
-            launch_split(s);
-        else
-            launch_fp64(s);
-        /* the previous round's results, while this round runs */
-        finish_leaving(s);
-        if(split)
-            collect_split(s);
-        else
-            collect_fp64(s);
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->rounds += 1;
+        bool more = !s->leaving.empty();
+        for(auto& row : s->cls)
+            for(Class& c : row) more = more || !c.members.empty();
+        if(more) continue;
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(20),
+                            [&] { return s->stop || !s->queue.empty(); });
     }
+    finish_leaving(s);
+    join_arrivals(s);
     finish_leaving(s);
 }
 
@@ -472,6 +536,8 @@ extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out)
     s->t0 = std::chrono::steady_clock::now();
     int rc = cudaSetDevice(cfg->device) == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
     if(!rc && cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        rc = SFX_ERR_CUDA;
+    if(!rc && cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking) != cudaSuccess)
         rc = SFX_ERR_CUDA;
     for(int d = 0; d < 2 && !rc; ++d) {
         sfx_config pc = make_cfg(s, d + 2, SFX_SOLVER_HLLC);
@@ -606,6 +672,7 @@ extern "C" int sfx_server_stats_get(sfx_server* s, sfx_server_stats* st) {
     st->bytes_in_use = s->bytes_in_use;
     st->rounds = s->rounds;
     st->now = now_s(s);
+    for(int k = 0; k < 4; ++k) st->worker_s[k] = s->worker_s[k];
     return SFX_OK;
 }
 
@@ -648,6 +715,7 @@ extern "C" int sfx_server_shutdown(sfx_server* s) {
     for(sfx_ctx* c : s->pool_ctx)
         if(c) sfx_ctx_destroy(c);
     if(s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    if(s->up_stream) cudaStreamDestroy(s->up_stream);
     delete s;
     return SFX_OK;
 }

@@ -25,6 +25,15 @@
 
 #include "sfx_internal.h"
 
+/* sfx_pow for the arguments outside sfx_pow_fast's domain, out of line so
+ * that its code is not inlined into the exact solver */
+__host__ __device__ __noinline__ double sfx_pow_rare(double x, double y);
+#define SFX_POW_FAST_RARE sfx_pow_rare
+#include "sfx_pow.h"
+__host__ __device__ __noinline__ double sfx_pow_rare(double x, double y) {
+    return sfx_pow(x, y);
+}
+
 namespace {
 
 constexpr unsigned kRightBit = 0x80000000u;
@@ -293,9 +302,9 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
 #pragma unroll
             for(int l = 0; l < D; ++l) r[l] = -r[l];
         }
-        const int2 fi = __ldg(m.fi + f);
+        const int nb = __ldg(m.nbe + j);
         float Wj[S];
-        if(!right && fi.y < 0) {
+        if(nb < 0) {
             /* reflective mirror: flip the velocity component along the face
              * normal (VorFace::transform / invtransform, VorFace.cpp:417-542) */
             float vn = 0.f;
@@ -307,7 +316,6 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
 #pragma unroll
             for(int l = 0; l < D; ++l) Wj[1 + l] = W[1 + l] - vn * r[l];
         } else {
-            const int nb = right ? fi.x : (fi.y & kIndexMask);
             const Cell<D> cn = load_cell<D>(m.cw, nb);
 #pragma unroll
             for(int k = 0; k < S; ++k) Wj[k] = cn.W[k];
@@ -696,11 +704,12 @@ __device__ __forceinline__ void shllc(float g, const float* WL, const float* WR,
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
  * 462-546) with the device pow; returns 0 or SFX_ERR_* */
-/* pow for the exact solver, out of line: one copy of its code instead of one
- * per call site keeps the face kernel's instruction footprint small (the
- * kernel stalled on instruction fetch with the copies inlined) */
+/* pow for the exact solver: the library's plain-double power (sfx_pow.h,
+ * a few ulp, which the p* iteration's 1e-8 tolerance needs far less than),
+ * out of line so that the face kernel carries one copy of its code (the
+ * kernel stalled on instruction fetch with copies inlined at every site) */
 __device__ __noinline__ double xpow(double x, double y) {
-    return pow(x, y);
+    return sfx_pow_fast(x, y);
 }
 
 template <int D>
@@ -733,9 +742,9 @@ struct XS {
     }
 };
 
-template <int D>
+template <int D, bool DEFER>
 __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const double* n,
-                      bool reflective, double* sol, bool defer) {
+                      bool reflective, double* sol) {
     constexpr int S = D + 2;
     double vL = 0., vR = 0.;
 #pragma unroll
@@ -839,7 +848,7 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                 }
             }
             if(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg > 0.) {
-                if(defer) return kDefer;
+                if(DEFER) return kDefer;
                 at_p = false;
                 /* Brent on [0, pg] */
                 double a = 0., b = pg, c, d = 1e230, fa = f(a), fbv = fg, fc, sv;
@@ -955,9 +964,9 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
     return bad ? SFX_ERR_RIEMANN : SFX_OK;
 }
 
-template <int D, int SOLVER>
+template <int D, int SOLVER, bool DEFER>
 __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
-                                            const float dt, const int f, const bool defer) {
+                                            const float dt, const int f) {
     constexpr int S = D + 2;
     if(f >= m.n_faces || failed(m.err)) return;
     float A, c[D], r[D], rn;
@@ -1048,21 +1057,17 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
         double dWL[S], dWR[S], dn[D], h[S];
 #pragma unroll
         for(int l = 0; l < D; ++l) dn[l] = nrm[l];
-        for(bool d = defer;; d = false) {
 #pragma unroll
-            for(int k = 0; k < S; ++k) {
-                dWL[k] = WL[k];
-                dWR[k] = WR[k];
-            }
-            status = sexact<D>(sp, dWL, dWR, dn, mirror, h, d);
-            if(status != kDefer) break;
-            /* Brent's method: queue the face for the follow-up launch (it
-             * writes this face's dQ); solve it here if the queue is full */
-            const int q = atomicAdd(m.slowq_n, 1);
-            if(q < m.slowq_cap) {
-                m.slowq[q] = f;
-                return;
-            }
+        for(int k = 0; k < S; ++k) {
+            dWL[k] = WL[k];
+            dWR[k] = WR[k];
+        }
+        status = sexact<D, DEFER>(sp, dWL, dWR, dn, mirror, h);
+        if(DEFER && status == kDefer) {
+            /* Brent's method: the face goes to the queue (room for every face)
+             * and the follow-up launch writes its dQ */
+            m.slowq[atomicAdd(m.slowq_n, 1)] = f;
+            return;
         }
         F.m = 0.f;
         F.P = 0.f;
@@ -1241,14 +1246,13 @@ __global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab,
 }
 
 template <int D, int SOLVER>
-__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 2)
+__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 3)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
-    sfaces_body<D, SOLVER>(tab[mi].m, sp, tab[mi].dt,
-                           (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x,
-                           SOLVER == SFX_SOLVER_EXACT);
+    sfaces_body<D, SOLVER, SOLVER == SFX_SOLVER_EXACT>(
+            tab[mi].m, sp, tab[mi].dt, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
 /* the queued exact-solver faces of every member, one per thread */
@@ -1260,7 +1264,7 @@ __global__ void __launch_bounds__(128) k_group_sfaces_slow(const sfx_group_entry
         const sfx_dmesh& m = tab[mi].m;
         const int n = min(*m.slowq_n, m.slowq_cap);
         for(int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-            sfaces_body<D, SFX_SOLVER_EXACT>(m, sp, tab[mi].dt, __ldg(m.slowq + j), false);
+            sfaces_body<D, SFX_SOLVER_EXACT, false>(m, sp, tab[mi].dt, __ldg(m.slowq + j));
     }
 }
 
