@@ -541,6 +541,7 @@ def run_resident(pool, reqs, chunk, torch, local):
         n0 = L.lib().sfx_launch_count()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("resident")  # the timed region, for profilers
         e0.record(main)
         for c in classes:
             cstream[c].wait_event(e0)
@@ -576,6 +577,7 @@ def run_resident(pool, reqs, chunk, torch, local):
             ev.record(cstream[c])
             main.wait_event(ev)
         e1.record(main)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
         launches += L.lib().sfx_launch_count() - n0

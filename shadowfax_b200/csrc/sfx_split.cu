@@ -41,6 +41,9 @@ constexpr int kPeriodicBit = 1 << 30;
 constexpr int kIndexMask = (1 << 30) - 1;
 /* exact solver: "this face needs Brent's method", queued instead of solved */
 constexpr int kDefer = 0x7f;
+/* how the exact solver treats a face whose p* needs a bracketing search:
+ * search in this lane, or queue the face (kDefer) for a follow-up launch */
+constexpr int kSolveInline = 0, kSolveDefer = 1;
 /* blocks of the group's queued-face launch (two waves of 128-thread blocks
  * on 148 SMs; the launch strides over each member's queue) */
 constexpr int kSlowGroupBlocks = 296;
@@ -742,7 +745,7 @@ struct XS {
     }
 };
 
-template <int D, bool DEFER>
+template <int D, int MODE>
 __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const double* n,
                       bool reflective, double* sol) {
     constexpr int S = D + 2;
@@ -848,57 +851,37 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                 }
             }
             if(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg > 0.) {
-                if(DEFER) return kDefer;
-                at_p = false;
-                /* Brent on [0, pg] */
-                double a = 0., b = pg, c, d = 1e230, fa = f(a), fbv = fg, fc, sv;
-                if(fa * fbv >= 0.) {
-                    p = fa < fbv ? a : b;
+                if(MODE == kSolveDefer) return kDefer;
+                /* f(0) < 0 < f(pg).  The reference runs Brent's method on
+                 * [0, pg] (ExactRiemannSolver.cpp:462-546), tens of
+                 * iterations in one lane.  f is increasing and concave, so a
+                 * Newton step from the right of the root lands on its left,
+                 * and Newton iterates started on the left rise monotonically
+                 * to it: a few iterations to the same root and tolerance
+                 * (bisection keeps the iterate inside (0, pg)). */
+                if(!(f0 < 0.)) {
+                    /* no bracket (Brent's fa * fb >= 0 exit) */
+                    p = f0 < fg ? 0. : pg;
+                    at_p = false;
                 } else {
-                    if(fabs(fa) < fabs(fbv)) {
-                        double t = a; a = b; b = t;
-                        t = fa; fa = fbv; fbv = t;
-                    }
-                    c = a;
-                    fc = fa;
-                    bool mflag = true;
-                    const double tol = s.tol;
-                    while(fbv != 0. && fabs(a - b) > tol * (a + b) * 0.5) {
-                        if(++it > 2 * SFX_MAX_ITER) return SFX_ERR_NOCONV;
-                        if(fa != fc && fbv != fc)
-                            sv = a * fbv * fc / (fa - fbv) / (fa - fc) +
-                                 b * fa * fc / (fbv - fa) / (fbv - fc) +
-                                 c * fa * fbv / (fc - fa) / (fc - fbv);
-                        else
-                            sv = b - fbv * (b - a) / (fbv - fa);
-                        const double t2 = (3. * a + b) / 4.;
-                        if(!((sv > t2 && sv < b) || (sv < t2 && sv > b)) ||
-                           (mflag && fabs(sv - b) >= fabs(b - c) / 2.) ||
-                           (!mflag && fabs(sv - b) >= fabs(c - d) / 2.) ||
-                           (mflag && fabs(b - c) < tol * (b + c) * 0.5) ||
-                           (!mflag && fabs(c - d) < tol * (c + d) * 0.5)) {
-                            sv = (a + b) / 2.;
-                            mflag = true;
-                        } else {
-                            mflag = false;
-                        }
-                        const double fs = f(sv);
-                        d = c;
-                        c = b;
-                        fc = fbv;
-                        if(fa * fs < 0.) {
-                            b = sv;
-                            fbv = fs;
-                        } else {
-                            a = sv;
-                            fa = fs;
-                        }
-                        if(fabs(fa) < fabs(fbv)) {
-                            double t = a; a = b; b = t;
-                            t = fa; fa = fbv; fbv = t;
-                        }
-                    }
-                    p = b;
+                double lo = 0., hi = pg, x = pg - fg / fpg, fx, fpx;
+                if(!(x > lo && x < hi)) x = 0.5 * (lo + hi);
+                eval(x, fx, fpx);
+                while(fx > 0.) {
+                    if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
+                    hi = x;
+                    x = x - fx / fpx;
+                    if(!(x > lo && x < hi)) x = 0.5 * (lo + hi);
+                    eval(x, fx, fpx);
+                }
+                double xp;
+                do {
+                    if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
+                    xp = x;
+                    x = fx < 0. ? x - fx / fpx : x;
+                    eval(x, fx, fpx);
+                } while(fabs(x - xp) > s.tol * 0.5 * (x + xp));
+                p = x;
                 }
             } else {
                 p = pg;
@@ -964,7 +947,7 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
     return bad ? SFX_ERR_RIEMANN : SFX_OK;
 }
 
-template <int D, int SOLVER, bool DEFER>
+template <int D, int SOLVER, int MODE>
 __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
                                             const float dt, const int f) {
     constexpr int S = D + 2;
@@ -1062,8 +1045,8 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
             dWL[k] = WL[k];
             dWR[k] = WR[k];
         }
-        status = sexact<D, DEFER>(sp, dWL, dWR, dn, mirror, h);
-        if(DEFER && status == kDefer) {
+        status = sexact<D, MODE>(sp, dWL, dWR, dn, mirror, h);
+        if(MODE == kSolveDefer && status == kDefer) {
             /* Brent's method: the face goes to the queue (room for every face)
              * and the follow-up launch writes its dQ */
             m.slowq[atomicAdd(m.slowq_n, 1)] = f;
@@ -1251,7 +1234,7 @@ __global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 3)
                        sfx_solver_params sp) {
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
-    sfaces_body<D, SOLVER, SOLVER == SFX_SOLVER_EXACT>(
+    sfaces_body<D, SOLVER, SOLVER == SFX_SOLVER_EXACT ? kSolveDefer : kSolveInline>(
             tab[mi].m, sp, tab[mi].dt, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
@@ -1264,7 +1247,8 @@ __global__ void __launch_bounds__(128) k_group_sfaces_slow(const sfx_group_entry
         const sfx_dmesh& m = tab[mi].m;
         const int n = min(*m.slowq_n, m.slowq_cap);
         for(int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-            sfaces_body<D, SFX_SOLVER_EXACT, false>(m, sp, tab[mi].dt, __ldg(m.slowq + j));
+            sfaces_body<D, SFX_SOLVER_EXACT, kSolveInline>(m, sp, tab[mi].dt,
+                                                            __ldg(m.slowq + j));
     }
 }
 
