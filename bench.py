@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=None,
                     help="serve: take every arrival of this many seconds of the stream "
                          "instead of the first --steps requests (the full config is 60)")
-    ap.add_argument("--chunk", type=int, default=8, help="serve: steps per scheduling round")
+    ap.add_argument("--chunk", type=int, default=4, help="serve: steps per scheduling round")
     a = ap.parse_args()
     if a.steps is None:
         a.steps = {"serve": 400, "sedov3d": 50, "batch2d": 20}[a.workload]
@@ -597,47 +597,81 @@ def run_resident(pool, reqs, chunk, torch, local):
     return face_steps, total_ms, launches, roof, len(waves), len(failed)
 
 
+# DRAM bytes (read + write) per face of one launch, from the ncu capture of a
+# 300,000-cell periodic random-field mesh (2,396,113 faces) in
+# profiles/split_kernels_random3d.md; the gathers and the per-face records
+# scale with the faces, so a launch over F faces moves about F times these
+TRAFFIC_B_PER_FACE = {("k_group_sfaces", 3, "Exact"): 106.2, ("k_group_sfaces", 3, "HLLC"): 103.7,
+                      ("k_group_sgrad", 3): 59.5, ("k_group_sapply", 3): 52.5}
+KERNELS = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces", "update": "k_group_sapply"}
+
+
 def resident_roofline(pool, reqs, inst, classes, cctx):
-    """per-kernel device times of the class with the most face work, all of
-    its requests in one launch group, CUDA events around each launch"""
+    """per-kernel device times of every class (all of its requests in one
+    launch group, CUDA events around each launch): the dominant kernel of the
+    class with the most face work, and each class's figures"""
     from shadowfax_b200.hydro import Group
+    peak, peak_kind = peaks()
+    names = ["gradients", "faces", "update"]
     work = {c: 0 for c in classes}
     for j, (c, fp) in inst.items():
         work[c] += pool.meshes[reqs[j].mesh].n_active_faces * reqs[j].nsteps
-    top_c = max(classes, key=lambda c: work[c])
-    js = [j for j, (c, _) in inst.items() if c == top_c]
-    g = Group(cctx[top_c], [inst[j][1] for j in js],
-              [pool.dts[reqs[j].mesh][reqs[j].state] for j in js])
-    g.step_timed(1)
-    steps = 3
-    ms, nl = g.step_timed(steps)
-    g.close()
-    per_launch = ms / steps
-    names = ["gradients", "faces", "update"]
-    alg = {k: 0 for k in names}
-    faces = 0
-    for j in js:
-        m = pool.meshes[reqs[j].mesh]
-        b = split_kernel_bytes(m.dim, m.n_cells, m.n_faces, m.nnz)
-        for k in names:
-            alg[k] += b[k]
-        faces += m.n_active_faces
-    top = int(np.argmax(per_launch))
-    peak, peak_kind = peaks()
-    achieved = alg[names[top]] / (per_launch[top] / 1e3) / 1e9
-    D = top_c[0]
-    step_rate = faces / (per_launch.sum() / 1e3)
-    kname = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces",
-             "update": "k_group_sapply"}[names[top]]
-    return {"bound": "hbm", "kernel": kname,
-            "class": f"{D}D {top_c[1]}, {len(js)} requests, {faces} faces",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": f"hbm_gbs {peak_kind}",
-            "algorithmic_bytes_per_launch": alg[names[top]],
+    per_class = {}
+    for c in classes:
+        js = [j for j, (cc, _) in inst.items() if cc == c]
+        if not js:
+            continue
+        g = Group(cctx[c], [inst[j][1] for j in js],
+                  [pool.dts[reqs[j].mesh][reqs[j].state] for j in js])
+        g.step_timed(1)
+        steps = 3
+        ms, nl = g.step_timed(steps)
+        g.close()
+        per_launch = ms / steps
+        alg = {k: 0 for k in names}
+        faces = 0
+        for j in js:
+            m = pool.meshes[reqs[j].mesh]
+            b = split_kernel_bytes(m.dim, m.n_cells, m.n_faces, m.nnz)
+            for k in names:
+                alg[k] += b[k]
+            faces += m.n_active_faces
+        D = c[0]
+        per_class[c] = {
+            "requests": len(js), "faces": faces, "face_work_share": work[c] / sum(work.values()),
             "kernel_ms": {k: float(v) for k, v in zip(names, per_launch)},
+            "achieved_gbs": {k: alg[k] / (per_launch[i] / 1e3) / 1e9 for i, k in enumerate(names)},
+            "algorithmic_bytes": alg,
+            "step_face_steps_per_s": faces / (per_launch.sum() / 1e3),
+            "step_frac": STEP_BYTES[("split", D)] * faces / (per_launch.sum() / 1e3) / 1e9 / peak}
+    top_c = max(per_class, key=lambda c: work[c])
+    pc = per_class[top_c]
+    kms = pc["kernel_ms"]
+    top = max(names, key=lambda k: kms[k])
+    kname = KERNELS[top]
+    D = top_c[0]
+    tkey = (kname, D, top_c[1]) if kname == "k_group_sfaces" else (kname, D)
+    traffic = TRAFFIC_B_PER_FACE[tkey] * pc["faces"] if tkey in TRAFFIC_B_PER_FACE else None
+    roof = {"bound": "hbm", "kernel": kname,
+            "class": f"{D}D {top_c[1]}, {pc['requests']} requests, {pc['faces']} faces",
+            "achieved": pc["achieved_gbs"][top], "peak": peak, "unit": "GB/s",
+            "frac": pc["achieved_gbs"][top] / peak, "traffic": traffic,
+            "traffic_note": "bytes per face from the ncu capture of a 300k-cell mesh "
+                            "(profiles/split_kernels_random3d.md) x faces of this launch",
+            "peak_source": f"hbm_gbs {peak_kind} (of measured)",
+            "algorithmic_bytes_per_launch": pc["algorithmic_bytes"][top],
+            "kernel_ms": kms,
+            "note": "the exact-solver face kernel is bound by the FP64 pipe (p* iteration), "
+                    "not by HBM; its FP64 pipe utilisation is in profiles/",
             "step_bytes_per_face": STEP_BYTES[("split", D)],
-            "step_achieved_gbs": STEP_BYTES[("split", D)] * step_rate / 1e9,
-            "step_frac": STEP_BYTES[("split", D)] * step_rate / 1e9 / peak}
+            "step_frac": pc["step_frac"],
+            "classes": {f"{c[0]}D {c[1]}": v for c, v in per_class.items()}}
+    hllc = per_class.get((3, "HLLC")) or per_class.get((2, "HLLC"))
+    if hllc is not None:
+        roof["hllc_pass"] = {"faces_kernel_achieved_gbs": hllc["achieved_gbs"]["faces"],
+                             "faces_kernel_frac": hllc["achieved_gbs"]["faces"] / peak,
+                             "step_frac": hllc["step_frac"]}
+    return roof
 
 
 def serve_cpu_sample(pool, reqs, steps: int = 2):

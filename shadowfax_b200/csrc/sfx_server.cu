@@ -46,11 +46,21 @@
 
 namespace {
 
-/* pinned host buffer for the asynchronous result copies */
-struct Pinned {
-    double* p = nullptr;
-    size_t cap = 0; /* doubles */
+/* pinned host staging for the asynchronous copies: one fixed block used as
+ * a bump allocator and emptied once every copy it holds has completed
+ * (cudaHostAlloc costs milliseconds per call, far more than the copies) */
+struct Ring {
+    uint8_t* base = nullptr;
+    size_t cap = 0, used = 0;
+    double* take(size_t n_doubles) {
+        const size_t b = (n_doubles * sizeof(double) + 255) & ~(size_t)255;
+        if(!base || used + b > cap) return nullptr;
+        double* p = (double*)(base + used);
+        used += b;
+        return p;
+    }
 };
+constexpr size_t kRingBytes = (size_t)256 << 20;
 
 struct Request {
     int64_t id = 0;
@@ -67,7 +77,8 @@ struct Request {
     int64_t bytes = 0;
     int32_t remaining = 0;
     int32_t chunk = 0; /* steps launched this round (FP64 mode) */
-    Pinned stage;      /* result copy in flight */
+    double* stage = nullptr; /* pinned staging of the copy in flight */
+    bool stage_own = false;  /* staging allocated for this request alone */
 };
 
 struct PoolMesh {
@@ -111,7 +122,7 @@ struct sfx_server {
     /* worker thread only */
     cudaStream_t copy_stream = nullptr; /* results out */
     cudaStream_t up_stream = nullptr;   /* admitted states in */
-    std::vector<Pinned> pinned_free;
+    Ring up, down; /* staging of admitted states and of results */
     std::vector<Request*> leaving;  /* results being copied out */
     std::vector<Request*> arriving; /* admitted, states being copied in */
 };
@@ -135,30 +146,28 @@ sfx_config make_cfg(const sfx_server* s, int dim, int solver) {
     return c;
 }
 
-Pinned pinned_get(sfx_server* s, size_t n) {
-    size_t best = s->pinned_free.size();
-    for(size_t i = 0; i < s->pinned_free.size(); ++i)
-        if(s->pinned_free[i].cap >= n &&
-           (best == s->pinned_free.size() || s->pinned_free[i].cap < s->pinned_free[best].cap))
-            best = i;
-    if(best < s->pinned_free.size()) {
-        Pinned b = s->pinned_free[best];
-        s->pinned_free.erase(s->pinned_free.begin() + best);
-        return b;
-    }
-    Pinned b;
-    if(cudaHostAlloc((void**)&b.p, n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+/* staging for n doubles: from the ring, or (larger than the ring) a block of
+ * its own */
+double* stage_take(Ring& ring, size_t n, bool* own) {
+    *own = false;
+    if(double* p = ring.take(n)) return p;
+    if(ring.used > 0) return nullptr;
+    double* p = nullptr;
+    if(cudaHostAlloc((void**)&p, n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
-        b.p = nullptr;
-        return b;
+        return nullptr;
     }
-    b.cap = n;
-    return b;
+    *own = true;
+    return p;
 }
 
-void pinned_put(sfx_server* s, Pinned b) {
-    if(b.p) s->pinned_free.push_back(b);
+void stage_release(Request* r) {
+    if(r->stage_own && r->stage) cudaFreeHost(r->stage);
+    r->stage = nullptr;
+    r->stage_own = false;
 }
+
+void finish_leaving(sfx_server* s);
 
 /* bookkeeping of a request that has left the device (worker thread) */
 void mark_done(sfx_server* s, Request* r, int status) {
@@ -204,9 +213,14 @@ void leave(sfx_server* s, Request* r, int status) {
     r->status = status;
     if(r->inst) {
         const size_t n = (size_t)sfx_mesh_dev(r->inst)->n_cells * sfx_mesh_dev(r->inst)->S;
-        r->stage = pinned_get(s, 2 * n);
-        if(r->stage.p) {
-            const int rc = sfx_mesh_download_fieldmajor_async(r->inst, r->stage.p, r->stage.p + n,
+        r->stage = stage_take(s->down, 2 * n, &r->stage_own);
+        if(!r->stage) {
+            /* the ring is full: complete the results already in it first */
+            finish_leaving(s);
+            r->stage = stage_take(s->down, 2 * n, &r->stage_own);
+        }
+        if(r->stage) {
+            const int rc = sfx_mesh_download_fieldmajor_async(r->inst, r->stage, r->stage + n,
                                                               s->copy_stream);
             if(rc && r->status == SFX_OK) r->status = rc;
         } else if(r->status == SFX_OK) {
@@ -221,27 +235,27 @@ void finish_leaving(sfx_server* s) {
     const bool copy_ok = cudaStreamSynchronize(s->copy_stream) == cudaSuccess;
     for(Request* r : s->leaving) {
         int status = r->status;
-        if(r->inst && r->stage.p) {
+        if(r->inst && r->stage) {
             if(!copy_ok && status == SFX_OK) status = SFX_ERR_CUDA;
             const sfx_dmesh* d = sfx_mesh_dev(r->inst);
             const int64_t n = d->n_cells;
             const int S = d->S;
             r->W.resize((size_t)n * S);
             r->Q.resize((size_t)n * S);
-            const double* w = r->stage.p;
-            const double* q = r->stage.p + (size_t)n * S;
+            const double* w = r->stage;
+            const double* q = r->stage + (size_t)n * S;
             for(int64_t i = 0; i < n; ++i)
                 for(int k = 0; k < S; ++k) {
                     r->W[(size_t)i * S + k] = w[(size_t)k * n + i];
                     r->Q[(size_t)i * S + k] = q[(size_t)k * n + i];
                 }
         }
-        pinned_put(s, r->stage);
-        r->stage = Pinned();
+        stage_release(r);
         release_instance(s, r);
         mark_done(s, r, status);
     }
     s->leaving.clear();
+    s->down.used = 0;
 }
 
 /* free cached instances until `need` more bytes fit the budget (waits for
@@ -285,6 +299,9 @@ void admit(sfx_server* s) {
             /* one request is always admitted when nothing runs */
             if(!fits && s->active > 0) return;
         }
+        /* staging for the state; a full ring waits for the next round */
+        r->stage = stage_take(s->up, r->W0.size(), &r->stage_own);
+        if(!r->stage && s->up.used > 0) return;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->queue.pop_front();
@@ -310,10 +327,9 @@ void admit(sfx_server* s) {
             }
         }
         if(!rc) {
-            r->stage = pinned_get(s, r->W0.size());
-            if(r->stage.p) {
-                std::memcpy(r->stage.p, r->W0.data(), r->W0.size() * sizeof(double));
-                rc = sfx_mesh_upload_W_fieldmajor_async(r->inst, r->stage.p, s->up_stream);
+            if(r->stage) {
+                std::memcpy(r->stage, r->W0.data(), r->W0.size() * sizeof(double));
+                rc = sfx_mesh_upload_W_fieldmajor_async(r->inst, r->stage, s->up_stream);
             } else {
                 rc = SFX_ERR_NOMEM;
             }
@@ -329,8 +345,7 @@ void join_arrivals(sfx_server* s) {
     if(s->arriving.empty()) return;
     const bool up_ok = cudaStreamSynchronize(s->up_stream) == cudaSuccess;
     for(Request* r : s->arriving) {
-        pinned_put(s, r->stage);
-        r->stage = Pinned();
+        stage_release(r);
         int rc = r->admit_status;
         if(!rc && !up_ok) rc = SFX_ERR_CUDA;
         if(!rc) {
@@ -351,6 +366,7 @@ void join_arrivals(sfx_server* s) {
         c.dirty = true;
     }
     s->arriving.clear();
+    s->up.used = 0;
 }
 
 int rebuild_group(Class& c) {
@@ -539,6 +555,16 @@ extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out)
         rc = SFX_ERR_CUDA;
     if(!rc && cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking) != cudaSuccess)
         rc = SFX_ERR_CUDA;
+    for(Ring* g : {&s->up, &s->down}) {
+        if(rc) break;
+        if(cudaHostAlloc((void**)&g->base, kRingBytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            g->base = nullptr;
+            rc = SFX_ERR_NOMEM;
+        } else {
+            g->cap = kRingBytes;
+        }
+    }
     for(int d = 0; d < 2 && !rc; ++d) {
         sfx_config pc = make_cfg(s, d + 2, SFX_SOLVER_HLLC);
         rc = sfx_ctx_create(&pc, &s->pool_ctx[d]);
@@ -697,7 +723,7 @@ extern "C" int sfx_server_shutdown(sfx_server* s) {
         }
     for(auto& kv : s->reqs) {
         if(kv.second->inst) sfx_mesh_free(kv.second->inst);
-        if(kv.second->stage.p) cudaFreeHost(kv.second->stage.p);
+        stage_release(kv.second);
         delete kv.second;
     }
     s->reqs.clear();
@@ -707,8 +733,8 @@ extern "C" int sfx_server_shutdown(sfx_server* s) {
         if(pm->mesh) sfx_mesh_free(pm->mesh);
     }
     s->pool.clear();
-    for(Pinned& b : s->pinned_free) cudaFreeHost(b.p);
-    s->pinned_free.clear();
+    for(Ring* g : {&s->up, &s->down})
+        if(g->base) cudaFreeHost(g->base);
     for(auto& row : s->cls)
         for(Class& c : row)
             if(c.ctx) sfx_ctx_destroy(c.ctx);

@@ -46,7 +46,7 @@ class Result:
 class Server:
     def __init__(self, precision: int = L.PREC_SPLIT, gamma: float = 5.0 / 3.0,
                  tolerance: float = 1e-8, cutoff: float = -5.0, memory_budget: int = 150 << 30,
-                 max_active: int = 4096, chunk_steps: int = 8, device: int = 0):
+                 max_active: int = 4096, chunk_steps: int = 4, device: int = 0):
         cfg = L.sfx_server_config(device, precision, gamma, tolerance, cutoff, memory_budget,
                                   max_active, chunk_steps)
         h = C.c_void_p()
