@@ -71,11 +71,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
-    ap.add_argument("--n", type=int, default=N_GEN, help="generators (default: config size)")
+    ap.add_argument("--n", type=int, default=None,
+                    help="generators of sedov3d / random3d (default: the config's size)")
+    ap.add_argument("--solver", default=None, choices=["Exact", "HLLC"],
+                    help="sedov3d / random3d solver (default: HLLC / Exact, as the configs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="serve", choices=["serve", "sedov3d", "batch2d"],
+    ap.add_argument("--workload", default="serve",
+                    choices=["serve", "sedov3d", "random3d", "batch2d"],
                     help="serve: config-5 request stream (default); sedov3d: config 2 on "
-                         "one mesh; batch2d: config 4, 1,024 meshes")
+                         "one mesh; random3d: config 3 (periodic random field, exact "
+                         "solver); batch2d: config 4, 1,024 meshes")
     ap.add_argument("--meshes", type=int, default=1024, help="batch2d: number of meshes")
     ap.add_argument("--duration", type=float, default=None,
                     help="serve: take every arrival of this many seconds of the stream "
@@ -83,7 +88,11 @@ def parse():
     ap.add_argument("--chunk", type=int, default=4, help="serve: steps per scheduling round")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = {"serve": 400, "sedov3d": 50, "batch2d": 20}[a.workload]
+        a.steps = {"serve": 400, "sedov3d": 50, "random3d": 10, "batch2d": 20}[a.workload]
+    if a.n is None:
+        a.n = {"random3d": 2_097_152}.get(a.workload, N_GEN)
+    if a.solver is None:
+        a.solver = "Exact" if a.workload == "random3d" else "HLLC"
     return a
 
 
@@ -215,9 +224,22 @@ def split_kernel_bytes(dim: int, n_cells: int, n_faces: int, nnz: int):
 STEP_BYTES = {("fp64", 2): 144, ("fp64", 3): 120, ("split", 2): 92, ("split", 3): 70}
 
 
-def build_problem(n: int):
+def build_problem(args):
+    """config 2 (Sedov 3D, reflective cube, seed 2) or config 3 (random field
+    3D, periodic cube, seed 3) with the chosen solver"""
     from shadowfax_b200 import workloads as wl
-    return wl.sedov3d(n=n, seed=SEED, solver="HLLC")
+    if args.workload == "random3d":
+        return wl.random_field3d(n=args.n, seed=3, solver=args.solver)
+    return wl.sedov3d(n=args.n, seed=SEED, solver=args.solver)
+
+
+def problem_text(args, pr):
+    m = pr.mesh
+    if args.workload == "random3d":
+        return (f"random3d {pr.solver}, {m.n_cells} generators (seed 3), {m.n_active_faces} "
+                f"faces, periodic unit cube, log-normal density, Gaussian velocities, CFL-0.4 dt")
+    return (f"sedov3d {pr.solver}, {m.n_cells} generators (seed {SEED}), {m.n_active_faces} "
+            f"faces, reflective unit cube, CFL-0.4 dt")
 
 
 def cpu_baseline(pr, steps: int = 3):
@@ -301,9 +323,11 @@ def bench_batch(args, rank, world, local, torch):
         grp.step(args.steps, graph=True, status=False)   # capture the K-step graph
         torch.cuda.synchronize()
         clk.mark("t0")
+        n_launch0 = L.lib().sfx_launch_count()
         e0.record(stream)
         grp.step(args.steps, graph=True, status=False)
         e1.record(stream)
+        n_launches = L.lib().sfx_launch_count() - n_launch0
         torch.cuda.synchronize()
         clk.mark("t1")
         time.sleep(0.3)
@@ -381,7 +405,7 @@ def bench_batch(args, rank, world, local, torch):
                          "achieved": 92 * value / 1e9, "frac": 92 * value / 1e9 / peak,
                          "note": "bytes per face-step of the split pass, 2D (algorithmic)"},
             "cpu_baseline": cb,
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": int(n_launches),
         }
     grp.close()
     for fp in members:
@@ -808,7 +832,7 @@ def run_reference_arm(args, rank, world):
         return
     if args.workload == "serve":
         return run_reference_serve(args)
-    pr = build_problem(args.n)
+    pr = build_problem(args)
     steps = max(1, min(args.steps, 5))
     from oracle.oracle import ref_binary
     if not ref_binary(3, "libm").exists():
@@ -820,9 +844,8 @@ def run_reference_arm(args, rank, world):
             "steps": steps, "warmup": 1, "ms_per_step": 1e3 * pr.mesh.n_active_faces / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"sedov3d HLLC, {pr.mesh.n_cells} generators, "
-                                   f"{pr.mesh.n_active_faces} faces, reflective unit cube",
-                       "solver": "HLLC", "precision": "fp64"},
+            "config": {"workload": problem_text(args, pr), "solver": pr.solver,
+                       "precision": "fp64"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -883,7 +906,7 @@ def main():
         return
     from shadowfax_b200 import _lib as L
     from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
-    pr = build_problem(args.n)
+    pr = build_problem(args)
     mesh = pr.mesh
     prec = L.PREC_FP64 if args.precision == "fp64" else L.PREC_SPLIT
     ctx = Context(3, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec, device=local)
@@ -894,7 +917,7 @@ def main():
     faces = mesh.n_active_faces
     dt = pr.dt
     lanes = None
-    if args.precision == "split":
+    if args.precision == "split" and args.workload == "sedov3d":
         lanes = fp.tune(dt, 3)     # lanes per cell for the gradient/update kernels
         fp.set_primitive(pr.W0)
 
@@ -902,6 +925,9 @@ def main():
         clk.wait_first_sample()
         for _ in range(args.warmup):
             fp.step(dt, 1, stats=False)
+        # every measured segment starts from the initial state (the supersonic
+        # random field reaches negative energies after some tens of steps)
+        fp.set_primitive(pr.W0)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -909,10 +935,12 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         clk.mark("t0")
+        n_launch0 = L.lib().sfx_launch_count()
         e0.record(stream)
         for _ in range(args.steps):
             fp.step(dt, 1, stats=False)
         e1.record(stream)
+        n_launches = L.lib().sfx_launch_count() - n_launch0
         torch.cuda.synchronize()
         clk.mark("t1")
         time.sleep(0.3)
@@ -928,6 +956,7 @@ def main():
     value = faces * args.steps * world / (ms_max / 1e3)
 
     # per-kernel device times (events around every launch) for the roofline
+    fp.set_primitive(pr.W0)
     kms, launches = fp.step_timed(dt, args.steps)
     names = ["gradients", "faces", "update"]
     per_launch = kms / args.steps
@@ -953,6 +982,7 @@ def main():
 
     # end to end through the C ABI with host buffers: per step upload W and Q
     # from host memory, one step, download W and Q
+    fp.set_primitive(pr.W0)
     W0, Q0 = fp.state()
     W = W0.copy()
     Q = Q0.copy()
@@ -982,8 +1012,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32/f64",
             "data": "synthetic",
-            "config": {"workload": f"sedov3d HLLC, {mesh.n_cells} generators (seed {SEED}), "
-                                   f"{faces} faces, reflective unit cube, CFL-0.4 dt",
+            "config": {"workload": problem_text(args, pr),
                        "solver": pr.solver, "precision": args.precision,
                        "lanes_per_cell": lanes,
                        "l2": "working set > L2 (no flush)",
@@ -993,7 +1022,7 @@ def main():
             "cpu_baseline": cb,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": int(n_launches),
         }
         print(json.dumps(line))
     fp.close()
