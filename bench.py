@@ -176,6 +176,20 @@ class ClockSampler:
                 "samples": len(sm), "window_s": round(t1 - t0, 4), "pad_s": pad}
 
 
+def reduce_over_ranks(ms: float, work: float, device, world: int):
+    """whole-job throughput over ranks: the work of all ranks (SUM) divided by
+    the slowest rank's device time (MAX); returns (value, ms_max, work_total).
+    Every rank makes the same two collective calls."""
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+    ms_max, work_total = float(t.item()), float(w.item())
+    return work_total / (ms_max / 1e3), ms_max, work_total
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -334,11 +348,7 @@ def bench_batch(args, rank, world, local, torch):
         ms = e0.elapsed_time(e1)
         st = grp.step(1, graph=False)
         assert np.all(st == 0), st
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = faces * args.steps * world / (ms_max / 1e3)
+    value, ms_max, _ = reduce_over_ranks(ms, faces * args.steps, f"cuda:{local}", world)
     # FP64 baseline: one launch sequence per mesh
     ctx64 = Context(2, solver, L.PREC_FP64, device=local)
     ctx64.set_stream(stream.cuda_stream)
@@ -767,12 +777,7 @@ def bench_serve(args, rank, world, local, torch):
                       abs(b.Q[:, D + 1].sum() - e0) / e0])
     errs = np.max(errs, 0) if errs else np.full(3, np.nan)
     drift = np.max(drift, 0) if drift else np.full(4, np.nan)
-    t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-    tf = torch.tensor([float(fs)], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(tf, op=torch.distributed.ReduceOp.SUM)
-    value = float(tf.item()) / (float(t.item()) / 1e3)
+    value, ms_max, _ = reduce_over_ranks(ms, fs, f"cuda:{local}", world)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = serve_cpu_sample(pool, reqs)
@@ -784,7 +789,7 @@ def bench_serve(args, rank, world, local, torch):
         line = {
             "metric": METRIC_SERVE, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": len(reqs), "warmup": args.warmup,
-            "ms_per_step": float(t.item()) / len(reqs),
+            "ms_per_step": ms_max / len(reqs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64", "data": "synthetic",
             "config": {"workload": f"serve: config-5 request stream, {len(reqs)} Poisson arrivals "
@@ -824,6 +829,53 @@ def bench_serve(args, rank, world, local, torch):
             "gpu_launches_served": int(launches),
         }
     return line
+
+
+def flux_error_by_branch(pr, device):
+    """one flux pass from the initial state in FP64 and in split precision:
+    relative L1 error of the per-face dQ (mass, momentum, energy) over all
+    faces and over the faces of each FP64 wave pattern (shock, rarefaction,
+    near-vacuum), and the largest per-face error relative to the largest
+    |dQ| of its field"""
+    from shadowfax_b200 import _lib as L
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    out = {}
+    for prec in (L.PREC_FP64, L.PREC_SPLIT):
+        ctx = Context(pr.mesh.dim, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec,
+                      device=device)
+        fp = FluxPass(ctx, pr.mesh)
+        fp.set_primitive(pr.W0)
+        grad, dQ, br, rc, _ = fp.flux_pass(pr.dt)
+        fp.close()
+        ctx.close()
+        if rc:
+            return {"status": int(rc)}
+        out[prec] = (dQ, br)
+    dQ64, br = out[L.PREC_FP64]
+    dQ32 = out[L.PREC_SPLIT][0]
+    D = pr.mesh.dim
+    region = (br >> 5) & 15
+    vac = ((br & 7) != 0) | (region == 11)
+    masks = {"all": np.ones(len(br), bool)}
+    if pr.solver == "Exact":
+        masks.update({"shock": np.isin(region, [1, 2, 6, 7]) & ~vac,
+                      "rarefaction": np.isin(region, [3, 4, 5, 8, 9, 10]) & ~vac,
+                      "near_vacuum": vac})
+    res = {}
+    for name, m in masks.items():
+        if not m.any():
+            res[name] = {"faces": 0}
+            continue
+        a, b = dQ32[m], dQ64[m]
+        den = np.abs(b).sum(0)
+        den[1:D + 1] = np.sqrt((b[:, 1:D + 1] ** 2).sum(1)).sum()
+        e = np.abs(a - b).sum(0) / np.maximum(den, 1e-300)
+        mx = (np.abs(a - b) / np.maximum(np.abs(dQ64).max(0), 1e-300)).max(0)
+        res[name] = {"faces": int(m.sum()), "rel_l1": {"mass": float(e[0]),
+                                                       "momentum": float(e[1:D + 1].max()),
+                                                       "energy": float(e[D + 1])},
+                     "max_rel": float(mx.max())}
+    return res
 
 
 def run_reference_arm(args, rank, world):
@@ -949,11 +1001,7 @@ def main():
             dist.barrier()
         st = fp.step(dt, 1)  # status check after the timed region
         assert st.status == 0, st.status
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = faces * args.steps * world / (ms_max / 1e3)
+    value, ms_max, _ = reduce_over_ranks(ms, faces * args.steps, f"cuda:{local}", world)
 
     # per-kernel device times (events around every launch) for the roofline
     fp.set_primitive(pr.W0)
@@ -1005,6 +1053,7 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pr)
+    flux_err = flux_error_by_branch(pr, local) if args.precision == "split" and rank == 0 else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -1023,6 +1072,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": int(n_launches),
+            "split_vs_fp64_face_flux_error": flux_err,
         }
         print(json.dumps(line))
     fp.close()
