@@ -334,6 +334,41 @@ __device__ __forceinline__ double ff(const sfx_solver_params& s, double p,
     return fb<D>(s, p, WL, aL) + fb<D>(s, p, WR, aR) + (vR - vL);
 }
 
+/* The last f(p) of the iteration, per side, with its power
+ * sfx_pow(p / p_K, (g-1)/(2g)) on a rarefaction side.  The reference
+ * evaluates f_K(p) again for the wave velocity and that power again for the
+ * sampling at the same p (ExactRiemannSolver.cpp:207-265): the kept values
+ * are the same operations on the same operands, so reusing them changes no
+ * bit and saves the double-double powers. */
+struct FLast {
+    double p, fL, fR, zL, zR;
+    bool ok;
+};
+
+template <int D>
+__device__ __forceinline__ double fbz(const sfx_solver_params& s, double p, const double* Wb,
+                                      double a, double* z) {
+    if(p > Wb[D + 1]) {
+        double A = s.tdgp1 / Wb[0];
+        double B = s.gm1dgp1 * Wb[D + 1];
+        *z = 0.;
+        return (p - Wb[D + 1]) * sqrt(A / (p + B));
+    }
+    *z = sfx_pow(p / Wb[D + 1], s.gm1d2g);
+    return s.tdgm1 * a * (*z - 1.);
+}
+
+template <int D>
+__device__ __forceinline__ double ffl(const sfx_solver_params& s, double p, const double* WL,
+                                      const double* WR, double vL, double vR, double aL,
+                                      double aR, FLast& c) {
+    c.p = p;
+    c.fL = fbz<D>(s, p, WL, aL, &c.zL);
+    c.fR = fbz<D>(s, p, WR, aR, &c.zR);
+    c.ok = true;
+    return c.fL + c.fR + (vR - vL);
+}
+
 template <int D>
 __device__ __forceinline__ double fprime(const sfx_solver_params& s, double p,
                                          const double* WL, const double* WR,
@@ -582,8 +617,14 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
     const double tol = s.tol;
     double p = 0.;
     double pguess = guess_p<D>(s, WL, WR, vL, vR, aL, aR);
-    const double fp = ff<D>(s, p, WL, WR, vL, vR, aL, aR);
-    double fpguess = ff<D>(s, pguess, WL, WR, vL, vR, aL, aR);
+    /* f(0): on both sides the rarefaction branch with sfx_pow(0, e) = +0
+     * (e > 0), i.e. (2/(g-1) a_K) * (0 - 1) exactly */
+    const double fp = WL[D + 1] > 0. && WR[D + 1] > 0.
+                              ? s.tdgm1 * aL * (0. - 1.) + s.tdgm1 * aR * (0. - 1.) + (vR - vL)
+                              : ff<D>(s, p, WL, WR, vL, vR, aL, aR);
+    FLast last;
+    last.ok = false;
+    double fpguess = ffl<D>(s, pguess, WL, WR, vL, vR, aL, aR, last);
     int newton = 0, brent_it = 0, errexit = 0, noconv = 0, mode;
     if(fp < s.cutoff) {
         mode = 1 << 3;
@@ -596,7 +637,7 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
             p = pguess;
             pguess = pguess - fpguess / fprime<D>(s, pguess, WL, WR, aL, aR);
             if(pguess < 0.) pguess = 0.;
-            fpguess = ff<D>(s, pguess, WL, WR, vL, vR, aL, aR);
+            fpguess = ffl<D>(s, pguess, WL, WR, vL, vR, aL, aR, last);
         }
         p = pguess;
     } else {
@@ -610,7 +651,7 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
                 ++newton;
                 p = pguess;
                 pguess = pguess - fpguess / fprime<D>(s, pguess, WL, WR, aL, aR);
-                fpguess = ff<D>(s, pguess, WL, WR, vL, vR, aL, aR);
+                fpguess = ffl<D>(s, pguess, WL, WR, vL, vR, aL, aR, last);
             }
         }
         if(!noconv && fabs(p - pguess) > tol * 0.5 * (p + pguess) && fpguess > 0.) {
@@ -621,7 +662,9 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
             p = pguess;
         }
     }
-    const double u = 0.5 * (vL + vR) + 0.5 * (fb<D>(s, p, WR, aR) - fb<D>(s, p, WL, aL));
+    const bool at_p = last.ok && last.p == p;
+    const double u = 0.5 * (vL + vR) + 0.5 * ((at_p ? last.fR : fb<D>(s, p, WR, aR)) -
+                                             (at_p ? last.fL : fb<D>(s, p, WL, aL)));
     double vhalf;
     int region;
     if(u < 0) {
@@ -642,7 +685,7 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
         } else {
             const double SHR = vR + aR;
             if(SHR > 0) {
-                const double STR = u + aR * sfx_pow(pdpR, s.gm1d2g);
+                const double STR = u + aR * (at_p ? last.zR : sfx_pow(pdpR, s.gm1d2g));
                 if(STR <= 0) {
                     sol[0] = WR[0] * sfx_pow(s.tdgp1 - s.gm1dgp1 / aR * vR, s.tdgm1);
                     vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
@@ -677,7 +720,7 @@ __device__ ExactOut exact_solve(const sfx_solver_params& s, double* WL, double* 
         } else {
             const double SHL = vL - aL;
             if(SHL < 0) {
-                const double STL = u - aL * sfx_pow(pdpL, s.gm1d2g);
+                const double STL = u - aL * (at_p ? last.zL : sfx_pow(pdpL, s.gm1d2g));
                 if(STL > 0) {
                     sol[0] = WL[0] * sfx_pow(s.tdgp1 + s.gm1dgp1 / aL * vL, s.tdgm1);
                     vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
