@@ -725,11 +725,13 @@ struct XS {
         }
         return s.tdgm1 * a * (xpow(p / Wb[D + 1], s.gm1d2g) - 1.);
     }
-    /* f_K, f_K' and, on the rarefaction side, z = (p/p_K)^((g-1)/(2g)) at
-     * one pressure: f_K' = r^(-(g+1)/(2g)) / (rho_K a_K) = z / (r rho_K a_K)
-     * with r = p/p_K, so one pow serves both */
-    __device__ void side(double p, const double* Wb, double a, double& f, double& fp,
-                         double& z) const {
+    /* f_K, f_K' and, on the rarefaction side, z = (p/p_K)^e, e = (g-1)/(2g),
+     * at one pressure: f_K' = r^(-(g+1)/(2g)) / (rho_K a_K) = z / (r rho_K a_K)
+     * with r = p/p_K, so one power serves both; z = q ik with q = p^e shared
+     * by the two sides and ik = p_K^-e computed once per face (ik = 0: the
+     * power of the ratio instead) */
+    __device__ void side(double p, const double* Wb, double a, double ik, double q,
+                         double& f, double& fp, double& z) const {
         if(p > Wb[D + 1]) {
             const double A = s.tdgp1 / Wb[0], B = s.gm1dgp1 * Wb[D + 1];
             const double q = sqrt(A / (p + B));
@@ -738,7 +740,7 @@ struct XS {
             z = 0.;
         } else {
             const double r = p / Wb[D + 1];
-            z = xpow(r, s.gm1d2g);
+            z = ik > 0. ? q * ik : xpow(r, s.gm1d2g);
             f = s.tdgm1 * a * (z - 1.);
             fp = r > 0. ? z / (r * (Wb[0] * a)) : 1. / (Wb[0] * a) * xpow(r, -s.gp1d2g);
         }
@@ -799,6 +801,11 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
     } else {
         XS<D> x{s};
         const double pL = WL[D + 1], pR = WR[D + 1];
+        /* p_K^-e (e = (g-1)/(2g)): (p/p_K)^e = p^e p_K^-e, one pow per
+         * evaluation for both sides (0: not finite, pow of the ratio) */
+        double iL = xpow(pL, -s.gm1d2g), iR = xpow(pR, -s.gm1d2g);
+        if(!(iL > 0. && iL < 1e300)) iL = 0.;
+        if(!(iR > 0. && iR < 1e300)) iR = 0.;
         const double pmin = fmin(pL, pR), pmax = fmax(pL, pR);
         double ppv = 0.5 * (pL + pR) - 0.125 * (vR - vL) * (WL[0] + WR[0]) * (aL + aR);
         const double floorp = s.tol * 0.5 * (pL + pR);
@@ -808,7 +815,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             pg = ppv;
         } else if(ppv < pmin) {
             pg = xpow((aL + aR - s.gm1d2 * (vR - vL)) /
-                         (aL / xpow(pL, s.gm1d2g) + aR / xpow(pR, s.gm1d2g)),
+                         (iL > 0. && iR > 0. ? aL * iL + aR * iR
+                                             : aL / xpow(pL, s.gm1d2g) + aR / xpow(pR, s.gm1d2g)),
                      s.tgdgm1);
         } else {
             const double gL = sqrt(s.tdgp1 / WL[0] / (ppv + s.gm1dgp1 * pL));
@@ -821,8 +829,10 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
          * velocity and the sampling below */
         double fL = 0., fpL = 0., zL = 0., fR = 0., fpR = 0., zR = 0.;
         auto eval = [&](double p, double& fv, double& fpv) {
-            x.side(p, WL, aL, fL, fpL, zL);
-            x.side(p, WR, aR, fR, fpR, zR);
+            const bool need = (!(p > pL) && iL > 0.) || (!(p > pR) && iR > 0.);
+            const double q = need ? xpow(p, s.gm1d2g) : 0.;
+            x.side(p, WL, aL, iL, q, fL, fpL, zL);
+            x.side(p, WR, aR, iR, q, fR, fpR, zR);
             fv = fL + fR + (vR - vL);
             fpv = fpL + fpR;
         };
