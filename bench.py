@@ -769,7 +769,7 @@ def bench_serve(args, rank, world, local, torch):
                                         f"cuda:{local}", world)
     # accuracy and conservation on the sampled requests
     errs, drift = [], []
-    for j in range(0, len(reqs), sample_every if fp64_serve else len(reqs) + 1):
+    for j in (range(0, len(reqs), sample_every) if fp64_serve else ()):
         a, b = res32[j], res64[j]
         if a.status or b.status:
             continue

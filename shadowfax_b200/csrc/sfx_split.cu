@@ -39,6 +39,9 @@ namespace {
 constexpr unsigned kRightBit = 0x80000000u;
 constexpr int kPeriodicBit = 1 << 30;
 constexpr int kIndexMask = (1 << 30) - 1;
+/* faces per lane whose midpoint - centroid the gradient kernel keeps in
+ * shared memory between its two passes */
+constexpr int kGradSlots = 6;
 /* exact solver: "this face needs Brent's method", queued instead of solved */
 constexpr int kDefer = 0x7f;
 /* how the exact solver treats a face whose p* needs a bracketing search:
@@ -294,16 +297,29 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
     }
     const int beg = live ? __ldg(m.off + ic) : 0;
     const int end = live ? __ldg(m.off + ic + 1) : 0;
-    for(int j = beg + lane; j < end; j += LPC) {
+    /* the limiter pass below needs each face's midpoint - centroid again:
+     * the first kGradSlots faces of each lane keep it in shared memory (NaN:
+     * a face of zero area), the rest are loaded again */
+    __shared__ float sd[kGradSlots * D][256];
+    int k0 = 0;
+    for(int j = beg + lane; j < end; j += LPC, ++k0) {
         const unsigned e = (unsigned)__ldg(m.idx + j);
         const int f = (int)(e & ~kRightBit);
         const bool right = e & kRightBit;
         float A, c[D], r[D], rn;
         geom<D>(m.fg, f, A, c, r, rn);
-        if(A == 0.f) continue;
+        if(A == 0.f) {
+            if(k0 < kGradSlots) sd[k0 * D][threadIdx.x] = __int_as_float(0x7fc00000);
+            continue;
+        }
         if(right) {
 #pragma unroll
             for(int l = 0; l < D; ++l) r[l] = -r[l];
+        }
+        if(k0 < kGradSlots) {
+            /* midpoint - centroid = c + (x - centroid) - r_cell / 2 */
+#pragma unroll
+            for(int l = 0; l < D; ++l) sd[k0 * D + l][threadIdx.x] = c[l] + xmc[l] - 0.5f * r[l];
         }
         const int nb = __ldg(m.nbe + j);
         float Wj[S];
@@ -345,17 +361,24 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
     float alpha[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) alpha[k] = 1.f;
-    for(int j = beg + lane; j < end; j += LPC) {
-        const unsigned e = (unsigned)__ldg(m.idx + j);
-        const int f = (int)(e & ~kRightBit);
-        const bool right = e & kRightBit;
-        float A, c[D], r[D], rn;
-        geom<D>(m.fg, f, A, c, r, rn);
-        if(A == 0.f) continue;
-        /* midpoint - centroid = c + (x - centroid) - r_cell / 2 */
+    int k1 = 0;
+    for(int j = beg + lane; j < end; j += LPC, ++k1) {
         float d[D];
+        if(k1 < kGradSlots) {
+            d[0] = sd[k1 * D][threadIdx.x];
+            if(d[0] != d[0]) continue;
 #pragma unroll
-        for(int l = 0; l < D; ++l) d[l] = c[l] + xmc[l] + (right ? 0.5f : -0.5f) * r[l];
+            for(int l = 1; l < D; ++l) d[l] = sd[k1 * D + l][threadIdx.x];
+        } else {
+            const unsigned e = (unsigned)__ldg(m.idx + j);
+            const int f = (int)(e & ~kRightBit);
+            const bool right = e & kRightBit;
+            float A, c[D], r[D], rn;
+            geom<D>(m.fg, f, A, c, r, rn);
+            if(A == 0.f) continue;
+#pragma unroll
+            for(int l = 0; l < D; ++l) d[l] = c[l] + xmc[l] + (right ? 0.5f : -0.5f) * r[l];
+        }
 #pragma unroll
         for(int k = 0; k < S; ++k) {
             float dp = 0.f;
