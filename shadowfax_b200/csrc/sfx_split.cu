@@ -866,24 +866,34 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         eval(pg, fg, fpg);
         bool at_p = true; /* fL, fR, zL, zR hold the values at the final p */
         int it = 0;
+        /* Newton stops when its next step is below the tolerance: the
+         * current iterate, whose f values are at hand, is then within the
+         * tolerance of the root (the reference takes that step and
+         * evaluates f once more) */
+        bool conv = false;
         if(f0 < s.cutoff) {
-            while(fabs(p - pg) > s.tol * 0.5 * (p + pg)) {
+            for(;;) {
+                const double pn = fmax(0., pg - fg / fpg);
+                if(!(fabs(pn - pg) > s.tol * 0.5 * (pn + pg))) break;
                 if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
-                p = pg;
-                pg = fmax(0., pg - fg / fpg);
+                pg = pn;
                 eval(pg, fg, fpg);
             }
             p = pg;
         } else {
             if(f0 * fg >= 0.) {
-                while(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg < 0.) {
+                while(fg < 0.) {
+                    const double pn = pg - fg / fpg;
+                    if(!(fabs(pn - pg) > s.tol * 0.5 * (pn + pg))) {
+                        conv = true;
+                        break;
+                    }
                     if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
-                    p = pg;
-                    pg = pg - fg / fpg;
+                    pg = pn;
                     eval(pg, fg, fpg);
                 }
             }
-            if(fabs(p - pg) > s.tol * 0.5 * (p + pg) && fg > 0.) {
+            if(!conv && fg > 0.) {
                 if(MODE == kSolveDefer) return kDefer;
                 /* f(0) < 0 < f(pg).  The reference runs Brent's method on
                  * [0, pg] (ExactRiemannSolver.cpp:462-546), tens of
@@ -907,13 +917,13 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
                     if(!(x > lo && x < hi)) x = 0.5 * (lo + hi);
                     eval(x, fx, fpx);
                 }
-                double xp;
-                do {
+                for(;;) {
+                    const double xn = fx < 0. ? x - fx / fpx : x;
+                    if(!(fabs(xn - x) > s.tol * 0.5 * (xn + x))) break;
                     if(++it > SFX_MAX_ITER) return SFX_ERR_NOCONV;
-                    xp = x;
-                    x = fx < 0. ? x - fx / fpx : x;
+                    x = xn;
                     eval(x, fx, fpx);
-                } while(fabs(x - xp) > s.tol * 0.5 * (x + xp));
+                }
                 p = x;
                 }
             } else {
