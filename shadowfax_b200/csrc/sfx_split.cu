@@ -1272,7 +1272,7 @@ __global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab,
 }
 
 template <int D, int SOLVER>
-__global__ void __launch_bounds__(256, SOLVER == SFX_SOLVER_HLLC ? 4 : 3)
+__global__ void __launch_bounds__(256, 4)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
     const int mi = group_mesh_of_block(pre, nm);
