@@ -295,7 +295,7 @@ typedef struct sfx_server_config {
     double cutoff;
     int64_t memory_budget;  /* device bytes for admitted request states       */
     int32_t max_active;     /* admitted requests at most                      */
-    int32_t chunk_steps;    /* steps per scheduling round                     */
+    int32_t chunk_steps;    /* steps per scheduling round (4 measured best)    */
 } sfx_server_config;
 
 typedef struct sfx_request_info {
