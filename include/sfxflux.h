@@ -221,8 +221,8 @@ int sfx_mesh_clone(sfx_ctx* ctx, sfx_mesh* base, sfx_mesh** out);
 int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision);
 
 /* split pass: lanes of a warp that share one cell in the gradient and update
- * kernels (1, 2, 4, 8 or 16; default 4).  Changes the summation tree of the
- * per-cell sums, not the algorithm. */
+ * kernels (1, 2, 4, 8 or 16; default 1 in 2D, 4 in 3D).  Changes the summation
+ * tree of the per-cell sums, not the algorithm. */
 int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
 
 /* ---- launch groups: many meshes per launch (SFX_PREC_SPLIT) ----
@@ -240,8 +240,8 @@ int sfx_group_create(sfx_ctx* ctx, int32_t n_meshes, sfx_mesh* const* meshes,
 int sfx_group_set_dt(sfx_group* group, const double* dt);
 int sfx_group_step(sfx_group* group, int32_t nsteps, int32_t use_graph,
                    int32_t* mesh_status);
-/* time each lanes-per-cell variant (4, 8, 16) of the gradient kernel on this
- * group (reads the states, changes none) and keep the fastest for the
+/* time each lanes-per-cell variant (1, 2, 4, 8, 16) of the gradient kernel on
+ * this group (reads the states, changes none) and keep the fastest for the
  * gradient and update kernels; *lanes receives it */
 int sfx_group_tune(sfx_group* group, int32_t reps, int32_t* lanes);
 int sfx_group_set_lanes(sfx_group* group, int32_t lanes);

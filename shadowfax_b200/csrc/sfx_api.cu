@@ -476,7 +476,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     d.n_faces = (int32_t)F;
     d.nnz = nnz;
     d.has_velocity = desc->face_velocity != nullptr;
-    d.lanes = 4;
+    d.lanes = sfx_default_lanes(dim);
     const int S = d.S;
     int rc = SFX_OK;
     auto A = [&](auto** p, size_t c) {

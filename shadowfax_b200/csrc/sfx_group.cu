@@ -134,7 +134,7 @@ extern "C" int sfx_group_create(sfx_ctx* ctx, int32_t n, sfx_mesh* const* meshes
     }
     g->dev.n_meshes = n;
     g->dev.dim = cfg->dim;
-    g->dev.lanes = 4;
+    g->dev.lanes = sfx_default_lanes(cfg->dim);
     int rc = cuda_ok(cudaSetDevice(cfg->device));
     if(!rc) rc = reserve(g, n);
     if(!rc) rc = upload_layout(g);

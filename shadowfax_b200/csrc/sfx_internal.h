@@ -169,6 +169,14 @@ int sfx_mesh_upload_W_fieldmajor_async(sfx_mesh* m, const double* W, void* strea
 /* sfx_mesh_clone with its device setup on `stream`, not waited for */
 int sfx_mesh_clone_async(sfx_ctx* ctx, sfx_mesh* base, void* stream, sfx_mesh** out);
 
+/* lanes per cell of the split gradient and update kernels before any
+ * tuning, the same for a mesh alone and in a group: one in 2D (about six
+ * faces per cell), four in 3D (about sixteen); measured fastest on 300,000-cell
+ * meshes */
+inline int sfx_default_lanes(int dim) {
+    return dim == 2 ? 1 : 4;
+}
+
 /* grouped launches (sfx_split.cu) */
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);
 int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,

@@ -77,7 +77,7 @@ def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
         fp.set_primitive(pr.W0)
     g = Group(ctx, members, [pr.dt for pr in probs])
     lanes = g.tune(2)
-    assert lanes in (4, 8, 16)
+    assert lanes in (1, 2, 4, 8, 16)
     st = g.step(probs[0].nsteps)
     assert np.all(st == 0)
     for pr, fp in zip(probs, members):
