@@ -490,16 +490,28 @@ def run_served(pool, reqs, precision, chunk, sample_every, device=0):
 
         th = threading.Thread(target=feeder, daemon=True)
         th.start()
+        # collect results only when the server reports new completions: one
+        # poll per pending request every millisecond would contend with the
+        # worker thread for the server's lock (latencies are the server's
+        # timestamps, so the collection rate does not enter them)
+        seen, last = -1, 0.0
         while len(results) < len(reqs):
-            with lock:
-                items = list(pending.items())
-            for rid, j in items:
-                res = srv.poll(rid, want_state=(j % sample_every == 0))
-                if res is not None:
-                    results[j] = res
-                    with lock:
-                        del pending[rid]
-            time.sleep(0.001)
+            st = srv.stats()
+            done = st.completed + st.failed
+            now = time.perf_counter()
+            # (and every 50 ms: a request may finish before the feeder has
+            # recorded its id)
+            if done != seen or now - last > 0.05:
+                seen, last = done, now
+                with lock:
+                    items = list(pending.items())
+                for rid, j in items:
+                    res = srv.poll(rid, want_state=(j % sample_every == 0))
+                    if res is not None:
+                        results[j] = res
+                        with lock:
+                            del pending[rid]
+            time.sleep(0.002)
         th.join()
         launches = L.lib().sfx_launch_count() - n0
         st = srv.stats()
