@@ -1,6 +1,6 @@
 """Benchmark of the B200 flux pass (one JSON line on rank 0).
 
-Default workload (--workload serve): the config-5 request stream -- Poisson
+Default workload (--workload serve): the serving request stream -- Poisson
 arrivals at 200 requests/s (seed 5), 70% 2D / 30% 3D static Voronoi meshes
 (periodic unit box) with generator counts log-uniform in [1e3, 1e6] served
 from a pre-tessellated pool (10 log-size bins per dimension), random-field
@@ -18,12 +18,14 @@ gradient and update work).
          request latency; beside it the same stream served with the plain
          FP64 pass one request at a time, and the split-vs-FP64 error.
 
-Other workloads: --workload sedov3d (config 2: 262,144 generators, HLLC, one
-mesh; --precision fp64|split) and --workload batch2d (config 4: 1,024 2D
-meshes in one launch group vs one FP64 launch sequence per mesh).
+Other workloads: --workload sedov3d (Sedov 3D blast, 262,144 generators,
+HLLC, one mesh; --precision fp64|split), --workload random3d (3D supersonic
+random field, 2,097,152 generators, exact solver) and --workload batch2d
+(1,024 2D step-state meshes in one launch group vs one FP64 launch sequence
+per mesh).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload serve|sedov3d|batch2d] [--precision fp64|split]
+                    [--workload serve|sedov3d|random3d|batch2d] [--precision fp64|split]
 
 Timing: CUDA events on the library's streams, barrier + synchronize on both
 sides, max over ranks; untimed warm-up before the timed region.  Working
@@ -72,19 +74,19 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     ap.add_argument("--n", type=int, default=None,
-                    help="generators of sedov3d / random3d (default: the config's size)")
+                    help="generators of sedov3d / random3d (default: 262,144 / 2,097,152)")
     ap.add_argument("--solver", default=None, choices=["Exact", "HLLC"],
-                    help="sedov3d / random3d solver (default: HLLC / Exact, as the configs)")
+                    help="sedov3d / random3d solver (default: HLLC / Exact)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="serve",
                     choices=["serve", "sedov3d", "random3d", "batch2d"],
-                    help="serve: config-5 request stream (default); sedov3d: config 2 on "
-                         "one mesh; random3d: config 3 (periodic random field, exact "
-                         "solver); batch2d: config 4, 1,024 meshes")
+                    help="serve: the request stream (default); sedov3d: Sedov 3D blast "
+                         "on one mesh; random3d: periodic 3D random field, exact solver; "
+                         "batch2d: 1,024 2D meshes")
     ap.add_argument("--meshes", type=int, default=1024, help="batch2d: number of meshes")
     ap.add_argument("--duration", type=float, default=None,
                     help="serve: take every arrival of this many seconds of the stream "
-                         "instead of the first --steps requests (the full config is 60)")
+                         "instead of the first --steps requests (the whole stream is 60)")
     ap.add_argument("--chunk", type=int, default=4, help="serve: steps per scheduling round")
     ap.add_argument("--no-fp64-serve", action="store_true",
                     help="serve: skip serving the stream with the plain FP64 pass")
@@ -241,8 +243,8 @@ STEP_BYTES = {("fp64", 2): 144, ("fp64", 3): 120, ("split", 2): 92, ("split", 3)
 
 
 def build_problem(args):
-    """config 2 (Sedov 3D, reflective cube, seed 2) or config 3 (random field
-    3D, periodic cube, seed 3) with the chosen solver"""
+    """Sedov 3D (reflective cube, seed 2) or the 3D random field (periodic
+    cube, seed 3) with the chosen solver"""
     from shadowfax_b200 import workloads as wl
     if args.workload == "random3d":
         return wl.random_field3d(n=args.n, seed=3, solver=args.solver)
@@ -303,7 +305,7 @@ def cpu_baseline_many(probs, steps: int = 2):
 
 
 def bench_batch(args, rank, world, local, torch):
-    """config 4: many independent 2D meshes, HLLC, each at its own CFL dt.
+    """batch2d: many independent 2D meshes, HLLC, each at its own CFL dt.
     Ours: FP32/FP64-split pass, all meshes in one launch group (one launch per
     phase per step, the steps captured in a CUDA graph, lanes per cell tuned).
     Baseline on the same GPU: the plain-FP64 pass launched mesh by mesh."""
@@ -433,7 +435,7 @@ SERVE_CPU_PROCS = 48
 
 
 def serve_requests(args, rank):
-    """the config-5 stream: first --steps arrivals, or --duration seconds"""
+    """the request stream: first --steps arrivals, or --duration seconds"""
     from shadowfax_b200 import workloads as wl
     seed = 5 + 1000 * rank
     if args.duration:
@@ -742,7 +744,7 @@ def serve_cpu_sample(pool, reqs, steps: int = 2):
 
 
 def bench_serve(args, rank, world, local, torch):
-    """config 5: the request stream served by the continuous-batching server
+    """the request stream served by the continuous-batching server
     (FP32/FP64 split, co-batched) against the same stream served with the
     plain FP64 pass one request at a time"""
     from shadowfax_b200 import _lib as L
@@ -814,7 +816,7 @@ def bench_serve(args, rank, world, local, torch):
             "ms_per_step": ms_max / len(reqs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": f"serve: config-5 request stream, {len(reqs)} Poisson arrivals "
+            "config": {"workload": f"serve: request stream, {len(reqs)} Poisson arrivals "
                                    f"at 200/s (seed 5; {'%.1f s' % reqs[-1].t} of the 60 s stream), "
                                    f"{n2} 2D / {len(reqs) - n2} 3D, N log-uniform in [1e3, 1e6] "
                                    f"from a pool of {len(used)} periodic meshes (10 log bins per "
@@ -946,7 +948,7 @@ def run_reference_serve(args):
             "steps": steps, "warmup": 1, "ms_per_step": 1e3 * faces / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "serve: config-5 request stream (first requests, one "
+            "config": {"workload": "serve: request stream (first requests, one "
                                    "reference process each)", "precision": "fp64"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,

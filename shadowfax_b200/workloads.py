@@ -1,14 +1,14 @@
-"""Synthetic workloads: the five configurations the flux pass is measured on.
+"""Synthetic workloads the flux pass is measured and tested on.
 
 Inputs are seeded synthetic stand-ins (numpy PCG64 streams): generators
 uniform in the unit square/cube, tessellated by the host face-list builder,
-with the initial states of each configuration.  Nothing here reads files.
+with each workload's initial states.  Nothing here reads files.
 
-  c1  2D Sod tube, reflective unit square, exact solver, dt = 1e-4, 100 steps
-  c2  3D Sedov-type blast, reflective unit cube, HLLC, global CFL 0.4, 50 steps
-  c3  3D supersonic random field, periodic unit cube, exact solver, one pass
-  c4  1,024 independent 2D step-state meshes, HLLC, 20 steps at own CFL dt
-  c5  Poisson request stream of static meshes (serving)
+  sod2d           2D Sod tube, reflective unit square, exact solver, dt = 1e-4, 100 steps
+  sedov3d         3D Sedov-type blast, reflective unit cube, HLLC, global CFL 0.4, 50 steps
+  random_field3d  3D supersonic random field, periodic unit cube, exact solver, one pass
+  batch2d         1,024 independent 2D step-state meshes, HLLC, 20 steps at own CFL dt
+  serve_stream    Poisson request stream of static meshes (serving)
 """
 from __future__ import annotations
 
@@ -89,7 +89,7 @@ def random_field3d(n: int = 2_097_152, seed: int = 3, solver: str = "Exact",
 
 
 def step_state2d(n: int, seed: int, solver: str = "HLLC", nsteps: int = 20) -> Problem:
-    """one c4 mesh: left/right constant states split by a line through the
+    """one mesh of batch2d: left/right constant states split by a line through the
     centre with a random normal angle"""
     rng = np.random.Generator(np.random.PCG64(seed))
     pos = random_generators(n, 2, int(rng.integers(1 << 62)))
@@ -110,7 +110,7 @@ def batch_sizes(count: int = 1024, lo: int = 1_000, hi: int = 100_000, seed: int
 
 def batch2d(count: int = 1024, seed: int = 4, solver: str = "HLLC", nsteps: int = 20,
             workers: int = 0) -> list[Problem]:
-    """config 4: `count` independent 2D step-state meshes with generator
+    """`count` independent 2D step-state meshes with generator
     counts log-uniform in [1e3, 1e5]; meshes are tessellated concurrently
     (the builder releases the interpreter lock)"""
     import os
@@ -138,7 +138,7 @@ def serve_pool_sizes(k: int = 10, lo: int = SERVE_LO, hi: int = SERVE_HI) -> np.
 
 
 def random_field_state(mesh: Mesh, seed: int) -> np.ndarray:
-    """the c3 state on any mesh: ln rho ~ N(-1/2, 1) (mean rho 1), p = 1,
+    """the random_field3d state on any mesh: ln rho ~ N(-1/2, 1) (mean rho 1), p = 1,
     each velocity component ~ N(0, 1)"""
     n, D = mesh.n_cells, mesh.dim
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -199,7 +199,7 @@ def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
 def serve_stream(k: int = 10, rate: float = 200.0, duration: float = 60.0, seed: int = 5,
                  frac2d: float = 0.7, steps: tuple = (10, 200), states_per_mesh: int = 2,
                  count: int | None = None) -> list:
-    """config 5: Poisson arrivals at `rate` per second for `duration`
+    """the serving stream: Poisson arrivals at `rate` per second for `duration`
     seconds (or the first `count` arrivals); 70% 2D / 30% 3D; N log-uniform
     in [1e3, 1e6] (served by the pool mesh of its bin); step count uniform on
     {10..200}; exact or HLLC 50/50"""

@@ -94,7 +94,7 @@ def test_riemann_toro_half_states(cuda_ok, dim):
 
 
 def test_sod2d_c1_full_config_vs_oracle(cuda_ok, oracle):
-    """config 1 exactly: 10,000 generators (seed 1), exact solver, dt 1e-4,
+    """the 2D Sod tube in full: 10,000 generators (seed 1), exact solver, dt 1e-4,
     100 steps; GPU == oracle (sfx_pow) bitwise, <= 1e-12 vs glibc pow"""
     from shadowfax_b200 import workloads as wl
     from shadowfax_b200.hydro import FluxPass
@@ -119,7 +119,7 @@ def test_sod2d_c1_full_config_vs_oracle(cuda_ok, oracle):
                                                   ("sedov3d", "Exact", 6000, 4),
                                                   ("random_field3d", "Exact", 20000, 1),
                                                   ("random_field3d", "HLLC", 20000, 2)])
-def test_scaled_configs_bitwise_vs_oracle(cuda_ok, oracle, maker, solver, n, steps):
+def test_scaled_workloads_bitwise_vs_oracle(cuda_ok, oracle, maker, solver, n, steps):
     from shadowfax_b200 import workloads as wl
     from shadowfax_b200.hydro import FluxPass
     pr = getattr(wl, maker)(n=n, solver=solver, nsteps=steps)

@@ -63,7 +63,7 @@ def test_split_reruns_are_bitwise_identical(cuda_ok):
 
 
 def test_split_single_pass_face_flux_error_by_branch(cuda_ok):
-    """config-3 style: per-face flux error of the split pass vs FP64 for the
+    """random field: per-face flux error of the split pass vs FP64 for the
     exact solver, grouped by the FP64 branch (shock / rarefaction / vacuum)"""
     from shadowfax_b200 import workloads as wl
     from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
