@@ -187,7 +187,7 @@ int sfx_state_download(sfx_mesh* mesh, double* W, double* Q);
  * reports it in stats (may be NULL).  Asynchronous unless stats != NULL. */
 int sfx_step(sfx_mesh* mesh, double dt, int32_t nsteps, sfx_stats* stats);
 
-/* sfx_step with CUDA events around every launch: kernel_ms[0..2] receive
+/* sfx_step with CUDA events around every phase: kernel_ms[0..2] receive
  * the summed device time (ms) of the gradient, face and update kernels over
  * the nsteps, *launches the number of kernels launched.  For profiling. */
 int sfx_step_timed(sfx_mesh* mesh, double dt, int32_t nsteps, float* kernel_ms,

@@ -182,7 +182,7 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     sfx_dmesh& d = m->d;
     const int64_t n = d.n_cells, F = d.n_faces;
     const int S = d.S, dim = d.dim;
-    d.W = d.Q = d.grad = d.dQf = nullptr;
+    d.W = d.Q = d.grad = d.dQf = d.gterm = nullptr;
     d.branch = nullptr;
     d.err = nullptr;
     d.totals_scratch = nullptr;
@@ -213,7 +213,10 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
         A(&m->self_pre, 6);
     } else {
         A(&d.grad, n * dim * S);
-        A(&d.dQf, F * S);
+        if(d.gshare)
+            A(&d.gterm, F * sfx_grad_term_stride(dim));
+        else
+            A(&d.dQf, F * S);
         A(&d.branch, F);
     }
     size_t total = 0;
@@ -227,6 +230,7 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
             *sl.p = block + off;
             off += sl.bytes;
         }
+        if(d.gterm) d.dQf = d.gterm;
     }
     if(!rc) rc = reset_err_on(m, s);
     if(!rc && split) rc = cuda_ok(cudaMemsetAsync(d.slowq_n, 0, sizeof(int32_t), s));
@@ -351,6 +355,8 @@ int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
     int64_t cells = n * (8 * (2 * dim + 2 + 2 * S + dim * S) + 4) + 4;
     int64_t faces = F * (8 * (1 + 3 * dim + S) + 4 * 4);
     int64_t bytes = cells + faces + nnz * 4 + 8 * 8 * 1024 + 4096;
+    if(precision != SFX_PREC_SPLIT) /* the gradient terms, dQf inside them */
+        bytes += F * 8 * (sfx_grad_term_stride(dim) - S);
     if(precision == SFX_PREC_SPLIT) {
         /* fg, fi, fsh, an, dqm, dqv, queue; cw, cg, cx, self table; nbe */
         bytes += F * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + 4 * slowq_capacity(F) + 4;
@@ -477,6 +483,16 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     d.nnz = nnz;
     d.has_velocity = desc->face_velocity != nullptr;
     d.lanes = sfx_default_lanes(dim);
+    /* the plain-FP64 gradients compute a face's terms once for both of its
+     * cells when the right cell of every local face sits at the face's right
+     * position, bit for bit */
+    d.gshare = 1;
+    for(int64_t f = 0; f < F && d.gshare; ++f)
+        if(desc->face_kind[f] == SFX_FACE_REAL &&
+           std::memcmp(desc->face_right_pos + f * dim,
+                       desc->cell_pos + (int64_t)desc->face_right[f] * dim,
+                       sizeof(double) * dim) != 0)
+            d.gshare = 0;
     const int S = d.S;
     int rc = SFX_OK;
     auto A = [&](auto** p, size_t c) {
@@ -498,11 +514,16 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     A(&d.kind, F);
     A(&d.rpos, F * dim);
     if(d.has_velocity) A(&d.vel, F * dim);
-    A(&d.dQf, F * S);
+    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
+    if(!split && d.gshare) {
+        A(&d.gterm, F * sfx_grad_term_stride(dim));
+        d.dQf = d.gterm;
+    } else {
+        A(&d.dQf, F * S);
+    }
     A(&d.branch, F);
     A(&d.err, 1);
     A(&d.totals_scratch, (size_t)(S + 1) * 1024);
-    const bool split = ctx->cfg.precision == SFX_PREC_SPLIT;
     if(split) {
         if(d.has_velocity) {
             sfx_mesh_free(m);
@@ -661,7 +682,7 @@ int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
         if(cudaEventCreate(&e) != cudaSuccess) return SFX_ERR_CUDA;
     double acc[3] = {0., 0., 0.};
     int rc = reset_err(m);
-    int nl = 0;
+    const int64_t l0 = sfx_launch_count();
     for(int t = 0; t < nsteps && rc == SFX_OK; ++t) {
         cudaEventRecord(ev[0], s);
         rc = run_phase(m, 0, dt, 0, s);
@@ -670,7 +691,6 @@ int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
         cudaEventRecord(ev[2], s);
         if(!rc) rc = run_phase(m, 2, dt, 0, s);
         cudaEventRecord(ev[3], s);
-        nl += 3;
         if(!rc) rc = cuda_ok(cudaEventSynchronize(ev[3]));
         for(int k = 0; k < 3 && !rc; ++k) {
             float ms = 0.f;
@@ -680,7 +700,7 @@ int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
     }
     for(auto& e : ev) cudaEventDestroy(e);
     for(int k = 0; k < 3; ++k) kernel_ms[k] = (float)acc[k];
-    if(launches) *launches = nl;
+    if(launches) *launches = (int32_t)(sfx_launch_count() - l0);
     if(rc) return rc;
     return check_err(m, nullptr);
 }
@@ -779,7 +799,8 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
         bytes += n * 32 + n * 16 * ((D * S + 3) / 4) + F * 8 + F * D * 8 +
                  4 * (int64_t)slowq_capacity(F) + 4 + (int64_t)sizeof(sfx_group_entry) + 24;
     else
-        bytes += n * D * S * 8 + F * S * 8 + F * 4;
+        bytes += n * D * S * 8 + F * 4 +
+                 F * 8 * (b.gshare ? sfx_grad_term_stride((int)D) : S) + 256;
     return bytes;
 }
 

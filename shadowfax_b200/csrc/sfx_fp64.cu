@@ -8,9 +8,11 @@
  * is sfx_pow (sfx_pow.h), shared with the CPU oracle, because glibc's and
  * CUDA's pow differ in the last bit.
  *
- * Kernels (one step = three launches):
+ * Kernels (one step = three or four launches):
  *   k_gradients  one thread per cell: VorCell::estimate_gradient
- *                (src/VorCell.cpp:464-530)
+ *                (src/VorCell.cpp:464-530); or k_grad_terms (one thread
+ *                per face) + k_grad_sum (one per cell and variable), the
+ *                same values with each face's terms computed once
  *   k_faces      one thread per face: VorFace::calculate_flux
  *                (src/VorFace.cpp:670-1024) with the Exact or HLLC solver;
  *                writes the limited dQ of the left cell once per face
@@ -284,6 +286,169 @@ __global__ void __launch_bounds__(128) k_gradients(sfx_dmesh m) {
 #pragma unroll
         for(int k = 0; k < S; ++k)
             m.grad[((size_t)l * S + k) * n + i] = delta[l][k] * alpha[k];
+}
+
+constexpr int kGradBlock = 128;
+
+/* The same gradients in two kernels, when every local face's right position
+ * is its right cell's position (gshare).  The first loop's term of a face,
+ *   t = A ((W_j - W_i) c / |r| - (W_i + W_j) / 2 r / |r|),
+ * is then exactly negated between the face's two cells: c is the same for
+ * both (the midpoint sum commutes), r and W_j - W_i change sign, and IEEE
+ * rounding is symmetric under negation, so the right cell's term equals -t
+ * bit for bit, except that a zero term may carry the other sign, which no
+ * sum starting at +0 can tell apart.  k_grad_terms evaluates t once per face
+ * (its 2 D S divisions, the bulk of the gradients' cost, are no longer done
+ * twice); k_grad_sum adds the terms in each cell's face order exactly as the
+ * one-kernel loop does, and runs the limiter. */
+template <int D>
+__global__ void __launch_bounds__(128) k_grad_terms(sfx_dmesh m) {
+    constexpr int S = D + 2, TS = D == 3 ? 16 : 8;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= m.n_faces || failed(m.err)) return;
+    const double A = m.area[f];
+    if(A == 0.) return; /* skipped by both cells */
+    const int n = m.n_cells, F = m.n_faces;
+    const int i = m.left[f];
+    double W[S], Wj[S], xi[D], xj[D], c[D], rij[D];
+#pragma unroll
+    for(int k = 0; k < S; ++k) W[k] = m.W[(size_t)k * n + i];
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        xi[l] = m.pos[(size_t)l * n + i];
+        xj[l] = m.rpos[(size_t)l * F + f];
+    }
+    if(m.kind[f] == SFX_FACE_MIRROR) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) Wj[k] = W[k];
+        mirror_state<D>(Wj, xi, xj);
+    } else {
+        const int r = m.right[f];
+#pragma unroll
+        for(int k = 0; k < S; ++k) Wj[k] = m.W[(size_t)k * n + r];
+    }
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        c[l] = m.mid[(size_t)l * F + f] - 0.5 * (xi[l] + xj[l]);
+        rij[l] = xi[l] - xj[l];
+    }
+    const double rnorm = norm<D>(rij);
+    double t[TS];
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+#pragma unroll
+        for(int k = 0; k < S; ++k)
+            t[l * S + k] =
+                A * ((Wj[k] - W[k]) * c[l] / rnorm - 0.5 * (W[k] + Wj[k]) * rij[l] / rnorm);
+#pragma unroll
+    for(int q = D * S; q < TS; ++q) t[q] = 0.;
+    double2* out = reinterpret_cast<double2*>(m.gterm + (size_t)f * TS);
+#pragma unroll
+    for(int q = 0; q < TS / 2; ++q) out[q] = make_double2(t[2 * q], t[2 * q + 1]);
+}
+
+/* the limiter quotient of one face (VorCell.cpp:486-530):
+ * mx = max(q1, q2) in the reference's select order, q1 = a / dp, q2 = b / dp,
+ * with a = W_max - W >= 0 >= b = W_min - W.  For finite operands the signs
+ * decide the select without one of the divisions: dp > 0 gives
+ * q1 >= +0 >= q2, so mx = q1; dp < 0 gives q1 <= -0 and q2 >= -0, so mx = q2
+ * unless both are zero, where the select keeps q1.  Anything else (dp = 0,
+ * a non-finite operand) takes the reference's two divisions. */
+__device__ __forceinline__ double limiter_ratio(double a, double b, double dp) {
+    constexpr double big = 1.7976931348623157e308;
+    const bool fin = a >= 0. && a <= big && b <= 0. && b >= -big && fabs(dp) <= big;
+    if(fin && dp > 0.) return a / dp;
+    if(fin && dp < 0.) {
+        const double q2 = b / dp;
+        if(q2 != 0.) return q2;
+        const double q1 = a / dp;
+        return (q1 < q2) ? q2 : q1;
+    }
+    double q1 = a, q2 = b;
+    if(dp != 0.) {
+        q1 = q1 / dp;
+        q2 = q2 / dp;
+    } else {
+        q1 = 1.;
+        q2 = 1.;
+    }
+    return (q1 < q2) ? q2 : q1;
+}
+
+/* one thread per (cell, primitive variable): the first loop adds the
+ * faces' terms (subtracts them where the cell is the face's right one) in
+ * the cell's face order, the second is the limiter; the variables are
+ * independent in both loops, so each thread rounds exactly as the
+ * one-kernel loop does */
+template <int D>
+__global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
+    constexpr int S = D + 2, TS = D == 3 ? 16 : 8;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / S), k = (int)(t % S);
+    if(i >= m.n_cells || failed(m.err)) return;
+    const int n = m.n_cells, F = m.n_faces;
+    const double W = m.W[(size_t)k * n + i];
+    double delta[D];
+    double Wmax = W, Wmin = W;
+#pragma unroll
+    for(int l = 0; l < D; ++l) delta[l] = 0.;
+    const int beg = m.off[i], end = m.off[i + 1];
+    for(int j = end - 1; j >= beg; --j) {
+        const unsigned e = (unsigned)m.idx[j];
+        const int f = (int)(e & ~kRightBit);
+        if(m.area[f] == 0.) continue;
+        const double* tf = m.gterm + (size_t)f * TS + k;
+        double Wj;
+        if(!(e & kRightBit)) {
+#pragma unroll
+            for(int l = 0; l < D; ++l) delta[l] = delta[l] + tf[l * S];
+            if(m.kind[f] == SFX_FACE_MIRROR) {
+                double Wm[S], xi[D], xj[D];
+#pragma unroll
+                for(int q = 0; q < S; ++q) Wm[q] = m.W[(size_t)q * n + i];
+#pragma unroll
+                for(int l = 0; l < D; ++l) {
+                    xi[l] = m.pos[(size_t)l * n + i];
+                    xj[l] = m.rpos[(size_t)l * F + f];
+                }
+                mirror_state<D>(Wm, xi, xj);
+                Wj = Wm[0];
+#pragma unroll
+                for(int q = 1; q < S; ++q)
+                    if(q == k) Wj = Wm[q];
+            } else {
+                Wj = m.W[(size_t)k * n + m.right[f]];
+            }
+        } else {
+#pragma unroll
+            for(int l = 0; l < D; ++l) delta[l] = delta[l] - tf[l * S];
+            Wj = m.W[(size_t)k * n + m.left[f]];
+        }
+        Wmax = (Wmax < Wj) ? Wj : Wmax;
+        Wmin = (Wj < Wmin) ? Wj : Wmin;
+    }
+    const double V = m.vol[i];
+    double cen[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        delta[l] = delta[l] / V;
+        cen[l] = m.cen[(size_t)l * n + i];
+    }
+    const double a = Wmax - W, b = Wmin - W;
+    double alpha = 1.;
+    for(int j = end - 1; j >= beg; --j) {
+        const int f = (int)((unsigned)m.idx[j] & ~kRightBit);
+        if(m.area[f] == 0.) continue;
+        double d[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) d[l] = m.mid[(size_t)l * F + f] - cen[l];
+        double dp = delta[0] * d[0] + delta[1] * d[1];
+        if(D == 3) dp = dp + delta[2] * d[2];
+        const double mx = limiter_ratio(a, b, dp);
+        alpha = (mx < alpha) ? mx : alpha;
+    }
+#pragma unroll
+    for(int l = 0; l < D; ++l) m.grad[((size_t)l * S + k) * n + i] = delta[l] * alpha;
 }
 
 /* --------------------------- exact solver --------------------------- */
@@ -1275,6 +1440,18 @@ int sfx_fp64_gradients(const sfx_dmesh* m, void* stream) {
     if(m->n_cells == 0) return SFX_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int B = 128;
+    if(m->gterm && m->gshare) {
+        const long long cs = (long long)m->n_cells * m->S;
+        if(m->dim == 3) {
+            if(m->n_faces) k_grad_terms<3><<<grid_for(m->n_faces, B), B, 0, s>>>(*m);
+            k_grad_sum<3><<<grid_for(cs, kGradBlock), kGradBlock, 0, s>>>(*m);
+        } else {
+            if(m->n_faces) k_grad_terms<2><<<grid_for(m->n_faces, B), B, 0, s>>>(*m);
+            k_grad_sum<2><<<grid_for(cs, kGradBlock), kGradBlock, 0, s>>>(*m);
+        }
+        sfx_count_launches(m->n_faces ? 2 : 1);
+        return cuda_status(cudaGetLastError());
+    }
     if(m->dim == 3)
         k_gradients<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m);
     else

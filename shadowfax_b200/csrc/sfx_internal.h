@@ -48,6 +48,13 @@ struct sfx_dmesh {
     double* rpos;   /* [dim][F]  */
     double* vel;    /* [dim][F] or NULL */
     double* dQf;    /* [S][F] scratch: limited dQ received by the left cell */
+    /* plain-FP64 pass: the first gradient loop's terms as seen from each
+     * face's left cell, [F][sfx_grad_term_stride(dim)] (the right cell of a
+     * local face takes their negation).  NULL: one kernel computes the
+     * gradients without it.  The array is dead between the gradient and the
+     * face kernels, so dQf lives inside it. */
+    double* gterm;
+    int32_t gshare; /* every local face's right position equals its right cell's */
     int32_t* branch; /* [F] scratch or NULL */
     sfx_dev_error* err;
     double* totals_scratch; /* [S * 1024] */
@@ -118,6 +125,7 @@ void sfx_solver_params_init(sfx_solver_params* p, int kind, double gamma,
                             double tol, double cutoff);
 
 /* FP64 kernels (sfx_fp64.cu) */
+inline int64_t sfx_grad_term_stride(int dim) { return dim == 3 ? 16 : 8; }
 int sfx_fp64_gradients(const sfx_dmesh* m, void* stream);
 int sfx_fp64_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
                    int write_branch, void* stream);

@@ -52,6 +52,29 @@ def test_single_pass_bitwise_vs_oracle(cuda_ok, oracle, name):
     np.testing.assert_array_equal(br, ocode)   # branch choices bit-exact on every face
 
 
+@pytest.mark.parametrize("name", ["sod2d_exact", "sedov3d_hllc", "random2d_periodic_exact"])
+def test_face_off_its_right_cell_bitwise_vs_oracle(cuda_ok, oracle, name):
+    """a local face whose right position is not bit for bit its right cell's
+    position: the two cells of that face see different geometry, so the
+    gradients are formed cell by cell instead of from shared face terms, and
+    still equal the oracle's"""
+    import dataclasses
+    mesh, meta, _ = load_case(name)
+    rpos = mesh.face_right_pos.copy()
+    f = int(np.flatnonzero(mesh.face_kind == 0)[len(rpos) // 3])
+    rpos[f, 0] = np.nextafter(rpos[f, 0], np.inf)
+    mesh = dataclasses.replace(mesh, face_right_pos=rpos)
+    ctx, fp = _pass(mesh, meta)
+    p = Params(solver=meta["solver"], gamma=meta["gamma"])
+    Qo = oracle.init_Q(mesh, p, meta["W0"])
+    grad, dQ, br, rc, bad = fp.flux_pass(meta["dt"])
+    og, odQ, ocode, orc, obad = oracle.flux_pass(mesh, p, meta["dt"], meta["W0"], Qo)
+    assert rc == orc == 0
+    np.testing.assert_array_equal(grad, og)
+    np.testing.assert_array_equal(dQ, odQ)
+    np.testing.assert_array_equal(br, ocode)
+
+
 @pytest.mark.parametrize("name", MESH_CASES)
 def test_steps_bitwise_vs_reference(cuda_ok, name):
     """n steps on the GPU == the reference's CPU pass (sfx_pow build), bit for
