@@ -770,6 +770,91 @@ struct XS {
     }
 };
 
+/* p* for the face kernel: Newton's method in FP32 from the reference's
+ * initial guess, then one FP64 Newton step from the FP32 root.  The face's
+ * states are FP32 values; the FP32 root is within about 1e-6 of p*, and the
+ * FP64 step (quadratic convergence) takes it to about 1e-12, inside the
+ * iteration's 1e-8 tolerance.  f_K and the rarefaction powers z_K at the
+ * final pressure are the FP64 values at the FP32 root carried along the
+ * step to first order (error of the order of the step squared).  Two FP64
+ * powers at most instead of one per FP64 iteration plus two per face.
+ * Returns false, and the FP64 iteration runs from the start, outside the
+ * range where FP32 is safe, when the FP32 iteration does not converge or
+ * takes a Newton step to (nearly) zero pressure (where the reference's
+ * iteration can stop at p = 0), when the FP64 step is not small, or when it
+ * moves a side between shock and rarefaction. */
+template <int D>
+__device__ __forceinline__ bool fast_root(const sfx_solver_params& s, const double* WL,
+                                          const double* WR, double aL, double aR, double vL,
+                                          double vR, double& p, double& fL, double& fR,
+                                          double& zL, double& zR) {
+    const double pL = WL[D + 1], pR = WR[D + 1];
+    constexpr double lo = 1e-12, hi = 1e12;
+    if(!(pL > lo && pL < hi && pR > lo && pR < hi && WL[0] > lo && WL[0] < hi && WR[0] > lo &&
+         WR[0] < hi && fabs(vR - vL) < hi))
+        return false;
+    const float e = (float)s.gm1d2g, tdgm1 = (float)s.tdgm1;
+    const float fpL = (float)pL, fpR = (float)pR, frL = (float)WL[0], frR = (float)WR[0];
+    const float faL = (float)aL, faR = (float)aR, dv = (float)(vR - vL);
+    const float AL = (float)s.tdgp1 / frL, BL = (float)s.gm1dgp1 * fpL;
+    const float AR = (float)s.tdgp1 / frR, BR = (float)s.gm1dgp1 * fpR;
+    auto side = [&](float q, float pK, float A, float B, float a, float rho, float& f,
+                    float& fp) {
+        if(q > pK) {
+            const float w = sqrtf(A / (q + B));
+            f = (q - pK) * w;
+            fp = (1.f - 0.5f * (q - pK) / (B + q)) * w;
+        } else {
+            const float r = q / pK;
+            const float z = exp2f(e * __log2f(r));
+            f = tdgm1 * a * (z - 1.f);
+            fp = z / (r * rho * a);
+        }
+    };
+    /* the reference's guess (two-rarefaction, two-shock or PVRS) */
+    const float pmin = fminf(fpL, fpR), pmax = fmaxf(fpL, fpR);
+    const float floorp = (float)s.tol * 0.5f * (fpL + fpR);
+    const float ppv = fmaxf(floorp, 0.5f * (fpL + fpR) - 0.125f * dv * (frL + frR) * (faL + faR));
+    float pg;
+    if(pmax / pmin <= 2.f && pmin <= ppv && ppv <= pmax) {
+        pg = ppv;
+    } else if(ppv < pmin) {
+        const float num = faL + faR - (float)s.gm1d2 * dv;
+        const float den = faL * exp2f(-e * __log2f(fpL)) + faR * exp2f(-e * __log2f(fpR));
+        pg = exp2f(__log2f(num / den) / e);
+    } else {
+        const float gL = sqrtf(AL / (ppv + BL)), gR = sqrtf(AR / (ppv + BR));
+        pg = (gL * fpL + gR * fpR - dv) / (gL + gR);
+    }
+    pg = fmaxf(floorp, pg);
+    if(!(pg > 0.f && pg < 3e38f)) return false;
+    for(int it = 0;; ++it) {
+        float f1, g1, f2, g2;
+        side(pg, fpL, AL, BL, faL, frL, f1, g1);
+        side(pg, fpR, AR, BR, faR, frR, f2, g2);
+        const float pn = pg - (f1 + f2 + dv) / (g1 + g2);
+        if(!(pn > 1e-3f * pg && pn < 3e38f) || it >= 16) return false;
+        const bool conv = fabsf(pn - pg) <= 1e-6f * pg;
+        pg = pn;
+        if(conv) break;
+    }
+    XS<D> x{s};
+    const double p0 = (double)pg;
+    double fpl, fpr;
+    x.side(p0, WL, aL, 0., 0., fL, fpl, zL);
+    x.side(p0, WR, aR, 0., 0., fR, fpr, zR);
+    const double dp = -(fL + fR + (vR - vL)) / (fpl + fpr);
+    const double p1 = p0 + dp;
+    if(!(fabs(dp) <= 1e-5 * p0) || (p0 > pL) != (p1 > pL) || (p0 > pR) != (p1 > pR))
+        return false;
+    fL += fpl * dp;
+    fR += fpr * dp;
+    zL *= 1. + s.gm1d2g * dp / p0;
+    zR *= 1. + s.gm1d2g * dp / p0;
+    p = p1;
+    return true;
+}
+
 template <int D, int MODE>
 __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const double* n,
                       bool reflective, double* sol) {
@@ -824,6 +909,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
     } else {
         XS<D> x{s};
         const double pL = WL[D + 1], pR = WR[D + 1];
+        double p = 0., fL = 0., zL = 0., fR = 0., zR = 0.;
+        if(MODE != kSolveDefer || !fast_root<D>(s, WL, WR, aL, aR, vL, vR, p, fL, fR, zL, zR)) {
         /* p_K^-e (e = (g-1)/(2g)): (p/p_K)^e = p^e p_K^-e, one pow per
          * evaluation for both sides (0: not finite, pow of the ratio) */
         double iL = xpow(pL, -s.gm1d2g), iR = xpow(pR, -s.gm1d2g);
@@ -850,7 +937,7 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         auto f = [&](double p) { return x.fb(p, WL, aL) + x.fb(p, WR, aR) + (vR - vL); };
         /* f and f' at one pressure, the per-side values kept for the wave
          * velocity and the sampling below */
-        double fL = 0., fpL = 0., zL = 0., fR = 0., fpR = 0., zR = 0.;
+        double fpL = 0., fpR = 0.;
         auto eval = [&](double p, double& fv, double& fpv) {
             const bool need = (!(p > pL) && iL > 0.) || (!(p > pR) && iR > 0.);
             const double q = need ? xpow(p, s.gm1d2g) : 0.;
@@ -859,7 +946,6 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
             fv = fL + fR + (vR - vL);
             fpv = fpL + fpR;
         };
-        double p = 0.;
         /* f(0): the rarefaction branch at p = 0 is -2 a_K / (g - 1) */
         const double f0 = pL > 0. && pR > 0. ? -s.tdgm1 * aL + -s.tdgm1 * aR + (vR - vL) : f(0.);
         double fg, fpg;
@@ -933,6 +1019,7 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         if(!at_p) {
             double t0, t1;
             eval(p, t0, t1);
+        }
         }
         const double u = 0.5 * (vL + vR) + 0.5 * (fR - fL);
         if(u < 0.) {
