@@ -651,7 +651,7 @@ def run_resident(pool, reqs, chunk, torch, local):
 # 300,000-cell periodic random-field mesh (2,396,113 faces) in
 # profiles/split_kernels_random3d.md; the gathers and the per-face records
 # scale with the faces, so a launch over F faces moves about F times these
-TRAFFIC_B_PER_FACE = {("k_group_sfaces", 3, "Exact"): 108.8, ("k_group_sfaces", 3, "HLLC"): 104.3,
+TRAFFIC_B_PER_FACE = {("k_group_sfaces", 3, "Exact"): 106.1, ("k_group_sfaces", 3, "HLLC"): 104.3,
                       ("k_group_sgrad", 3): 59.4, ("k_group_sapply", 3): 53.0}
 KERNELS = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces", "update": "k_group_sapply"}
 
