@@ -396,33 +396,41 @@ __global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
     for(int j = end - 1; j >= beg; --j) {
         const unsigned e = (unsigned)m.idx[j];
         const int f = (int)(e & ~kRightBit);
-        if(m.area[f] == 0.) continue;
+        const bool rside = (e & kRightBit) != 0;
+        /* the face's loads all issued before the area test (the record of a
+         * face of zero area holds stale values, never used) */
+        const double A = m.area[f];
+        const int kd = m.kind[f];
+        const int nb = rside ? m.left[f] : m.right[f];
         const double* tf = m.gterm + (size_t)f * TS + k;
+        double tv[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) tv[l] = tf[l * S];
+        if(A == 0.) continue;
         double Wj;
-        if(!(e & kRightBit)) {
+        if(!rside && kd == SFX_FACE_MIRROR) {
+            double Wm[S], xi[D], xj[D];
 #pragma unroll
-            for(int l = 0; l < D; ++l) delta[l] = delta[l] + tf[l * S];
-            if(m.kind[f] == SFX_FACE_MIRROR) {
-                double Wm[S], xi[D], xj[D];
+            for(int q = 0; q < S; ++q) Wm[q] = m.W[(size_t)q * n + i];
 #pragma unroll
-                for(int q = 0; q < S; ++q) Wm[q] = m.W[(size_t)q * n + i];
-#pragma unroll
-                for(int l = 0; l < D; ++l) {
-                    xi[l] = m.pos[(size_t)l * n + i];
-                    xj[l] = m.rpos[(size_t)l * F + f];
-                }
-                mirror_state<D>(Wm, xi, xj);
-                Wj = Wm[0];
-#pragma unroll
-                for(int q = 1; q < S; ++q)
-                    if(q == k) Wj = Wm[q];
-            } else {
-                Wj = m.W[(size_t)k * n + m.right[f]];
+            for(int l = 0; l < D; ++l) {
+                xi[l] = m.pos[(size_t)l * n + i];
+                xj[l] = m.rpos[(size_t)l * F + f];
             }
+            mirror_state<D>(Wm, xi, xj);
+            Wj = Wm[0];
+#pragma unroll
+            for(int q = 1; q < S; ++q)
+                if(q == k) Wj = Wm[q];
+        } else {
+            Wj = m.W[(size_t)k * n + nb];
+        }
+        if(!rside) {
+#pragma unroll
+            for(int l = 0; l < D; ++l) delta[l] = delta[l] + tv[l];
         } else {
 #pragma unroll
-            for(int l = 0; l < D; ++l) delta[l] = delta[l] - tf[l * S];
-            Wj = m.W[(size_t)k * n + m.left[f]];
+            for(int l = 0; l < D; ++l) delta[l] = delta[l] - tv[l];
         }
         Wmax = (Wmax < Wj) ? Wj : Wmax;
         Wmin = (Wj < Wmin) ? Wj : Wmin;
@@ -438,10 +446,11 @@ __global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
     double alpha = 1.;
     for(int j = end - 1; j >= beg; --j) {
         const int f = (int)((unsigned)m.idx[j] & ~kRightBit);
-        if(m.area[f] == 0.) continue;
+        const double A = m.area[f];
         double d[D];
 #pragma unroll
         for(int l = 0; l < D; ++l) d[l] = m.mid[(size_t)l * F + f] - cen[l];
+        if(A == 0.) continue;
         double dp = delta[0] * d[0] + delta[1] * d[1];
         if(D == 3) dp = dp + delta[2] * d[2];
         const double mx = limiter_ratio(a, b, dp);
