@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include "sfx_internal.h"
+#include "sfx_limiter.h"
 #include "sfx_pow.h"
 
 namespace {
@@ -347,34 +348,6 @@ __global__ void __launch_bounds__(128) k_grad_terms(sfx_dmesh m) {
     for(int q = 0; q < TS / 2; ++q) out[q] = make_double2(t[2 * q], t[2 * q + 1]);
 }
 
-/* the limiter quotient of one face (VorCell.cpp:486-530):
- * mx = max(q1, q2) in the reference's select order, q1 = a / dp, q2 = b / dp,
- * with a = W_max - W >= 0 >= b = W_min - W.  For finite operands the signs
- * decide the select without one of the divisions: dp > 0 gives
- * q1 >= +0 >= q2, so mx = q1; dp < 0 gives q1 <= -0 and q2 >= -0, so mx = q2
- * unless both are zero, where the select keeps q1.  Anything else (dp = 0,
- * a non-finite operand) takes the reference's two divisions. */
-__device__ __forceinline__ double limiter_ratio(double a, double b, double dp) {
-    constexpr double big = 1.7976931348623157e308;
-    const bool fin = a >= 0. && a <= big && b <= 0. && b >= -big && fabs(dp) <= big;
-    if(fin && dp > 0.) return a / dp;
-    if(fin && dp < 0.) {
-        const double q2 = b / dp;
-        if(q2 != 0.) return q2;
-        const double q1 = a / dp;
-        return (q1 < q2) ? q2 : q1;
-    }
-    double q1 = a, q2 = b;
-    if(dp != 0.) {
-        q1 = q1 / dp;
-        q2 = q2 / dp;
-    } else {
-        q1 = 1.;
-        q2 = 1.;
-    }
-    return (q1 < q2) ? q2 : q1;
-}
-
 /* one thread per (cell, primitive variable): the first loop adds the
  * faces' terms (subtracts them where the cell is the face's right one) in
  * the cell's face order, the second is the limiter; the variables are
@@ -453,7 +426,7 @@ __global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
         if(A == 0.) continue;
         double dp = delta[0] * d[0] + delta[1] * d[1];
         if(D == 3) dp = dp + delta[2] * d[2];
-        const double mx = limiter_ratio(a, b, dp);
+        const double mx = sfx_limiter_ratio(a, b, dp);
         alpha = (mx < alpha) ? mx : alpha;
     }
 #pragma unroll
