@@ -225,6 +225,31 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision);
  * tree of the per-cell sums, not the algorithm. */
 int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
 
+/* ---- one mesh over several devices (plain FP64) ----
+ * Replaces the reference's MPI halo updates for the flux pass
+ * (DelTess::update_Ws / update_gradients / update_dQs, src/DelTess_mpi.cpp:1614,
+ * 1781, 2024): each device holds its owned cells, numbered first, then the
+ * cells one face away (their gradients are computed here too) and the cells
+ * two faces away (state only), with every face of the first two groups, the
+ * faces touching an owned cell first.  sfx_mesh_set_ranges makes the pass
+ * compute gradients of cells [0, grad_cells), fluxes of faces
+ * [0, flux_faces) and update cells [0, update_cells) only; the owned cells
+ * then receive exactly the values a pass over the whole mesh gives them.
+ * Between steps the other cells' W and mass Q[0] come from their owners:
+ * sfx_mesh_pack_cells writes records [count][S + 1] (W, then Q[0]) of the
+ * listed local cells to a device buffer, sfx_mesh_unpack_cells stores such
+ * records into the listed cells.  idx, out and in are device pointers;
+ * stream NULL is the context's stream.  The lists are made once per
+ * partition and are not checked on every call: an index outside the mesh
+ * is skipped (never dereferenced).  SFX_ERR_UNSUPPORTED on a
+ * split-precision mesh. */
+int sfx_mesh_set_ranges(sfx_mesh* mesh, int32_t grad_cells, int32_t flux_faces,
+                        int32_t update_cells);
+int sfx_mesh_pack_cells(sfx_mesh* mesh, const int32_t* idx, int32_t count, double* out,
+                        void* stream);
+int sfx_mesh_unpack_cells(sfx_mesh* mesh, const int32_t* idx, int32_t count, const double* in,
+                          void* stream);
+
 /* ---- launch groups: many meshes per launch (SFX_PREC_SPLIT) ----
  * A group runs one step of every member mesh with one launch per phase
  * (gradients, faces, update): block b of a launch works on the mesh whose

@@ -129,6 +129,11 @@ PROTOTYPES = {
                                      _ip, _dp]),
     "sfx_voronoi_free": (None, [C.c_void_p]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sfx_mesh_set_ranges": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "sfx_mesh_pack_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                      C.c_void_p]),
+    "sfx_mesh_unpack_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                        C.c_void_p]),
     "sfx_mesh_clone": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "sfx_mesh_clone_bytes": (C.c_int64, [C.c_void_p, C.c_int32]),
     "sfx_group_set_steps": (C.c_int, [C.c_void_p, _ip]),

@@ -811,6 +811,37 @@ int sfx_mesh_set_lanes(sfx_mesh* m, int32_t lanes) {
     return SFX_OK;
 }
 
+int sfx_mesh_set_ranges(sfx_mesh* m, int32_t grad_cells, int32_t flux_faces,
+                        int32_t update_cells) {
+    if(!m) return SFX_ERR_INVALID;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    sfx_dmesh& d = m->d;
+    if(update_cells < 0 || update_cells > grad_cells || grad_cells > d.n_cells ||
+       flux_faces < 0 || flux_faces > d.n_faces)
+        return SFX_ERR_INVALID;
+    d.ranged = 1;
+    d.r_grad = grad_cells;
+    d.r_flux = flux_faces;
+    d.r_upd = update_cells;
+    return SFX_OK;
+}
+
+int sfx_mesh_pack_cells(sfx_mesh* m, const int32_t* idx, int32_t count, double* out,
+                        void* stream) {
+    if(!m || count < 0 || (count > 0 && (!idx || !out))) return SFX_ERR_INVALID;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    return sfx_fp64_pack_cells(&m->d, idx, count, out,
+                               stream ? stream : (void*)m->ctx->stream);
+}
+
+int sfx_mesh_unpack_cells(sfx_mesh* m, const int32_t* idx, int32_t count, const double* in,
+                          void* stream) {
+    if(!m || count < 0 || (count > 0 && (!idx || !in))) return SFX_ERR_INVALID;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    return sfx_fp64_unpack_cells(&m->d, idx, count, in,
+                                 stream ? stream : (void*)m->ctx->stream);
+}
+
 int sfx_mesh_totals(sfx_mesh* m, double* totals) {
     if(!m || !totals) return SFX_ERR_INVALID;
     return sfx_fp64_totals(&m->d, totals, m->ctx->stream);

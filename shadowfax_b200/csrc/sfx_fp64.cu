@@ -186,7 +186,7 @@ template <int D>
 __global__ void __launch_bounds__(128) k_gradients(sfx_dmesh m) {
     constexpr int S = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= m.n_cells || failed(m.err)) return;
+    if(i >= sfx_grad_cells(m) || failed(m.err)) return;
     const int n = m.n_cells, F = m.n_faces;
     double W[S], xi[D], Wmax[S], Wmin[S], delta[D][S];
 #pragma unroll
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
     constexpr int S = D + 2, TS = D == 3 ? 16 : 8;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (int)(t / S), k = (int)(t % S);
-    if(i >= m.n_cells || failed(m.err)) return;
+    if(i >= sfx_grad_cells(m) || failed(m.err)) return;
     const int n = m.n_cells, F = m.n_faces;
     const double W = m.W[(size_t)k * n + i];
     double delta[D];
@@ -1075,7 +1075,7 @@ __global__ void __launch_bounds__(128) k_faces(sfx_dmesh m, sfx_solver_params sp
                                                double dt, int write_branch) {
     constexpr int S = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if(f >= m.n_faces || failed(m.err)) return;
+    if(f >= sfx_flux_faces(m) || failed(m.err)) return;
     const int n = m.n_cells, F = m.n_faces;
     const double A = m.area[f];
     if(A == 0.) {
@@ -1248,7 +1248,7 @@ template <int D>
 __global__ void __launch_bounds__(128) k_apply(sfx_dmesh m, double gamma) {
     constexpr int S = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= m.n_cells || failed(m.err)) return;
+    if(i >= sfx_update_cells(m) || failed(m.err)) return;
     const int n = m.n_cells, F = m.n_faces;
     double dQ[S];
 #pragma unroll
@@ -1314,11 +1314,12 @@ __global__ void k_init_Q(sfx_dmesh m, double gamma, int kind) {
 constexpr int kTotBlocks = 1024;
 constexpr int kTotThreads = 256;
 
-__global__ void k_totals_partial(const double* Q, int n, int S, double* part) {
+/* sums of the fields over cells [0, count) of Q [S][n] */
+__global__ void k_totals_partial(const double* Q, int n, int count, int S, double* part) {
     __shared__ double sh[kTotThreads];
-    const int per = (n + kTotBlocks - 1) / kTotBlocks;
+    const int per = (count + kTotBlocks - 1) / kTotBlocks;
     const int b0 = blockIdx.x * per;
-    const int b1 = min(n, b0 + per);
+    const int b1 = min(count, b0 + per);
     for(int k = 0; k < S; ++k) {
         double acc = 0.;
         for(int i = b0 + threadIdx.x; i < b1; i += kTotThreads) acc = acc + Q[(size_t)k * n + i];
@@ -1391,6 +1392,32 @@ __global__ void k_riemann(sfx_solver_params sp, int n, const double* WLa,
     code[t] = st ? -st : c;
 }
 
+/* halo records of a split mesh: [count][S + 1], the cell's W then its mass
+ * Q[0] (the only Q field the face kernel reads of a cell it does not
+ * update); an index outside the mesh is skipped, never dereferenced */
+__global__ void k_pack_cells(sfx_dmesh m, const int32_t* idx, int count, double* out) {
+    const int S = m.S, R = S + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= (long long)count * R) return;
+    const int j = (int)(t / R), q = (int)(t % R);
+    const int c = idx[j];
+    if(c < 0 || c >= m.n_cells) return;
+    out[t] = q < S ? m.W[(size_t)q * m.n_cells + c] : m.Q[c];
+}
+
+__global__ void k_unpack_cells(sfx_dmesh m, const int32_t* idx, int count, const double* in) {
+    const int S = m.S, R = S + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= (long long)count * R) return;
+    const int j = (int)(t / R), q = (int)(t % R);
+    const int c = idx[j];
+    if(c < 0 || c >= m.n_cells) return;
+    if(q < S)
+        m.W[(size_t)q * m.n_cells + c] = in[t];
+    else
+        m.Q[c] = in[t];
+}
+
 inline int grid_for(long long n, int block) {
     return (int)((n + block - 1) / block);
 }
@@ -1419,11 +1446,12 @@ void sfx_solver_params_init(sfx_solver_params* p, int kind, double g, double tol
 }
 
 int sfx_fp64_gradients(const sfx_dmesh* m, void* stream) {
-    if(m->n_cells == 0) return SFX_OK;
+    const int nc = sfx_grad_cells(*m);
+    if(nc == 0) return SFX_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int B = 128;
     if(m->gterm && m->gshare) {
-        const long long cs = (long long)m->n_cells * m->S;
+        const long long cs = (long long)nc * m->S;
         if(m->dim == 3) {
             if(m->n_faces) k_grad_terms<3><<<grid_for(m->n_faces, B), B, 0, s>>>(*m);
             k_grad_sum<3><<<grid_for(cs, kGradBlock), kGradBlock, 0, s>>>(*m);
@@ -1435,19 +1463,20 @@ int sfx_fp64_gradients(const sfx_dmesh* m, void* stream) {
         return cuda_status(cudaGetLastError());
     }
     if(m->dim == 3)
-        k_gradients<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m);
+        k_gradients<3><<<grid_for(nc, B), B, 0, s>>>(*m);
     else
-        k_gradients<2><<<grid_for(m->n_cells, B), B, 0, s>>>(*m);
+        k_gradients<2><<<grid_for(nc, B), B, 0, s>>>(*m);
     sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
 
 int sfx_fp64_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
                    int write_branch, void* stream) {
-    if(m->n_faces == 0) return SFX_OK;
+    const int nf = sfx_flux_faces(*m);
+    if(nf == 0) return SFX_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int B = 128;
-    const int G = grid_for(m->n_faces, B);
+    const int G = grid_for(nf, B);
     if(m->dim == 3) {
         if(sp->kind == SFX_SOLVER_EXACT)
             k_faces<3, SFX_SOLVER_EXACT><<<G, B, 0, s>>>(*m, *sp, dt, write_branch);
@@ -1464,13 +1493,14 @@ int sfx_fp64_faces(const sfx_dmesh* m, const sfx_solver_params* sp, double dt,
 }
 
 int sfx_fp64_apply(const sfx_dmesh* m, const sfx_solver_params* sp, void* stream) {
-    if(m->n_cells == 0) return SFX_OK;
+    const int nc = sfx_update_cells(*m);
+    if(nc == 0) return SFX_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int B = 128;
     if(m->dim == 3)
-        k_apply<3><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma);
+        k_apply<3><<<grid_for(nc, B), B, 0, s>>>(*m, sp->gamma);
     else
-        k_apply<2><<<grid_for(m->n_cells, B), B, 0, s>>>(*m, sp->gamma);
+        k_apply<2><<<grid_for(nc, B), B, 0, s>>>(*m, sp->gamma);
     sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }
@@ -1489,8 +1519,8 @@ int sfx_fp64_init_Q(const sfx_dmesh* m, const sfx_solver_params* sp, void* strea
 
 int sfx_fp64_totals(const sfx_dmesh* m, double* host_out, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    k_totals_partial<<<kTotBlocks, kTotThreads, 0, s>>>(m->Q, m->n_cells, m->S,
-                                                         m->totals_scratch);
+    k_totals_partial<<<kTotBlocks, kTotThreads, 0, s>>>(m->Q, m->n_cells, sfx_update_cells(*m),
+                                                         m->S, m->totals_scratch);
     k_totals_final<<<1, 256, 0, s>>>(m->totals_scratch, m->S);
     sfx_count_launches(2);
     cudaError_t e = cudaMemcpyAsync(host_out, m->totals_scratch + (size_t)m->S * kTotBlocks,
@@ -1520,6 +1550,24 @@ int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n, const double* 
             k_riemann<2, SFX_SOLVER_HLLC><<<G, B, 0, s>>>(*sp, n, dWL, dWR, dn, reflective,
                                                          dhalf, dflux, dcode);
     }
+    sfx_count_launches(1);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_fp64_pack_cells(const sfx_dmesh* m, const int32_t* idx, int count, double* out,
+                        void* stream) {
+    if(count <= 0) return SFX_OK;
+    const long long t = (long long)count * (m->S + 1);
+    k_pack_cells<<<grid_for(t, 256), 256, 0, (cudaStream_t)stream>>>(*m, idx, count, out);
+    sfx_count_launches(1);
+    return cuda_status(cudaGetLastError());
+}
+
+int sfx_fp64_unpack_cells(const sfx_dmesh* m, const int32_t* idx, int count, const double* in,
+                          void* stream) {
+    if(count <= 0) return SFX_OK;
+    const long long t = (long long)count * (m->S + 1);
+    k_unpack_cells<<<grid_for(t, 256), 256, 0, (cudaStream_t)stream>>>(*m, idx, count, in);
     sfx_count_launches(1);
     return cuda_status(cudaGetLastError());
 }

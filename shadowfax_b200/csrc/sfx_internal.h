@@ -55,6 +55,10 @@ struct sfx_dmesh {
      * face kernels, so dQf lives inside it. */
     double* gterm;
     int32_t gshare; /* every local face's right position equals its right cell's */
+    /* one part of a mesh split over several devices (plain FP64): gradients
+     * of cells [0, r_grad), fluxes of faces [0, r_flux), update of cells
+     * [0, r_upd) (the owned cells, numbered first); ranged == 0: all */
+    int32_t ranged, r_grad, r_flux, r_upd;
     int32_t* branch; /* [F] scratch or NULL */
     sfx_dev_error* err;
     double* totals_scratch; /* [S * 1024] */
@@ -93,6 +97,15 @@ struct sfx_dmesh {
     int32_t* slowq_n;
     int32_t slowq_cap;
 };
+
+#if defined(__CUDACC__)
+#define SFX_RANGE_HD __host__ __device__ inline
+#else
+#define SFX_RANGE_HD inline
+#endif
+SFX_RANGE_HD int sfx_grad_cells(const sfx_dmesh& m) { return m.ranged ? m.r_grad : m.n_cells; }
+SFX_RANGE_HD int sfx_flux_faces(const sfx_dmesh& m) { return m.ranged ? m.r_flux : m.n_faces; }
+SFX_RANGE_HD int sfx_update_cells(const sfx_dmesh& m) { return m.ranged ? m.r_upd : m.n_cells; }
 
 /* one mesh of a launch group (device table entry); steps_left, when not
  * NULL, is the member's remaining step count: the kernels skip a member at 0
@@ -134,6 +147,11 @@ int sfx_fp64_apply(const sfx_dmesh* m, const sfx_solver_params* sp,
 int sfx_fp64_init_Q(const sfx_dmesh* m, const sfx_solver_params* sp,
                     void* stream);
 int sfx_fp64_totals(const sfx_dmesh* m, double* host_out, void* stream);
+/* halo records [count][S + 1] (W, then the mass Q[0]) of the listed cells */
+int sfx_fp64_pack_cells(const sfx_dmesh* m, const int32_t* idx, int count, double* out,
+                        void* stream);
+int sfx_fp64_unpack_cells(const sfx_dmesh* m, const int32_t* idx, int count, const double* in,
+                          void* stream);
 int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n,
                      const double* dWL, const double* dWR, const double* dn,
                      int reflective, double* dhalf, double* dflux,

@@ -94,6 +94,7 @@ class Context:
         self.dim = dim
         self.solver = solver
         self.precision = precision
+        self.device = device
         cfg = L.sfx_config(dim, solver.kind, solver.gamma, solver.tolerance, solver.cutoff,
                            precision, device)
         h = C.c_void_p()
@@ -202,6 +203,27 @@ class FluxPass:
 
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_mesh_set_lanes(self.h, lanes), "sfx_mesh_set_lanes")
+
+    def set_ranges(self, grad_cells: int, flux_faces: int, update_cells: int):
+        """one part of a mesh split over several devices (plain FP64):
+        gradients of cells [0, grad_cells), fluxes of faces [0, flux_faces),
+        update of cells [0, update_cells) (sfx_mesh_set_ranges)"""
+        L.check(L.lib().sfx_mesh_set_ranges(self.h, grad_cells, flux_faces, update_cells),
+                "sfx_mesh_set_ranges")
+
+    def pack_cells(self, idx, out) -> None:
+        """records [count, S + 1] (W, then the mass) of local cells idx into
+        the device buffer out; idx an int32 and out a float64 device tensor"""
+        L.check(L.lib().sfx_mesh_pack_cells(self.h, C.c_void_p(idx.data_ptr()), int(idx.numel()),
+                                            C.c_void_p(out.data_ptr()), None),
+                "sfx_mesh_pack_cells")
+
+    def unpack_cells(self, idx, inp) -> None:
+        """store records [count, S + 1] from the device buffer inp into the
+        local cells idx"""
+        L.check(L.lib().sfx_mesh_unpack_cells(self.h, C.c_void_p(idx.data_ptr()),
+                                              int(idx.numel()), C.c_void_p(inp.data_ptr()), None),
+                "sfx_mesh_unpack_cells")
 
     def tune(self, dt: float, reps: int = 3) -> int:
         """split pass: time the lanes-per-cell variants on this mesh's own

@@ -64,3 +64,93 @@ def test_two_cpu_ranks_reduce_work_and_time():
         assert n == 50
     # the ranks serve different streams (no request served twice)
     assert res[0][4] != res[1][4]
+
+
+def _split_mesh_rank(rank, world, port, name, nsteps, out):
+    """one rank of a mesh split over `world` ranks: the oracle's pass over
+    this rank's part (standing in for the device), the ring exchange through
+    the product's exchange_records over gloo"""
+    import datetime
+    import sys
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from golden_util import load_case
+        from oracle.oracle import Oracle, Params
+        from shadowfax_b200 import partition as P
+
+        oracle = Oracle()
+        mesh, meta, _ = load_case(name)
+        p = Params(solver=meta["solver"], gamma=meta["gamma"])
+        owner = P.partition(mesh, world)
+        pt = P.build_part(mesh, owner, rank)
+        plan = P.exchange_plan(mesh, owner, pt)
+        W = meta["W0"][pt.cells].copy()
+        Q = oracle.init_Q(pt.mesh, p, W)
+        R = mesh.dim + 3
+        recv = {q: torch.empty((len(rv), R), dtype=torch.float64) for q, (_, rv) in plan.items()}
+        for _ in range(nsteps):
+            _, dQ, _, rc, _ = oracle.flux_pass(pt.mesh, p, meta["dt"], W, Q)
+            assert rc == 0
+            Qt = Q.copy()
+            Qt[pt.n_own:, [0, -1]] = 1e300
+            Wn, Qn, rc, _ = oracle.apply(pt.mesh, p, dQ, W, Qt)
+            assert rc == 0
+            W[:pt.n_own], Q[:pt.n_own] = Wn[:pt.n_own], Qn[:pt.n_own]
+            send = {q: torch.from_numpy(np.concatenate([W[s], Q[s, :1]], axis=1))
+                    for q, (s, _) in plan.items()}
+            P.exchange_records(send, recv)
+            for q, (_, rv) in plan.items():
+                rec = recv[q].numpy()
+                W[rv] = rec[:, :-1]
+                Q[rv, 0] = rec[:, -1]
+        out[rank] = (pt.cells[:pt.n_own], W[:pt.n_own].copy(), Q[:pt.n_own].copy())
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name", ["random2d_periodic_exact", "sedov3d_hllc"])
+def test_split_mesh_over_two_cpu_ranks(name):
+    """the owned cells of both ranks, after steps with the ring exchange over
+    gloo, equal the oracle's steps over the whole mesh bit for bit"""
+    import sys
+
+    import numpy as np
+    sys.path.insert(0, os.path.dirname(__file__))
+    from golden_util import load_case
+    from oracle.oracle import Oracle, Params
+
+    world, nsteps = 2, 3
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        procs = [ctx.Process(target=_split_mesh_rank, args=(r, world, port, name, nsteps, out))
+                 for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(180)
+            assert p.exitcode == 0
+        res = dict(out)
+    oracle = Oracle()
+    mesh, meta, _ = load_case(name)
+    prm = Params(solver=meta["solver"], gamma=meta["gamma"])
+    r = oracle.run(mesh, prm, meta["dt"], nsteps, meta["W0"])
+    assert r["status"] == 0
+    seen = np.zeros(mesh.n_cells, int)
+    for rank in range(world):
+        cells, W, Q = res[rank]
+        seen[cells] += 1
+        assert np.array_equal(W, r["W"][cells])
+        assert np.array_equal(Q, r["Q"][cells])
+    assert np.all(seen == 1)
