@@ -88,6 +88,9 @@ def parse():
                     help="serve: take every arrival of this many seconds of the stream "
                          "instead of the first --steps requests (the whole stream is 60)")
     ap.add_argument("--chunk", type=int, default=4, help="serve: steps per scheduling round")
+    ap.add_argument("--pool-dir", default=None,
+                    help="serve: read the pool meshes from mesh files in this directory, "
+                         "writing the ones not there yet (sfx_meshfile_*)")
     ap.add_argument("--no-fp64-serve", action="store_true",
                     help="serve: skip serving the stream with the plain FP64 pass")
     a = ap.parse_args()
@@ -752,7 +755,7 @@ def bench_serve(args, rank, world, local, torch):
     reqs = serve_requests(args, rank)
     t_build = time.time()
     used = sorted({r.mesh for r in reqs})
-    pool = wl.serve_pool(only=set(used))
+    pool = wl.serve_pool(only=set(used), cache_dir=args.pool_dir)
     t_build = time.time() - t_build
     sample_every = max(1, len(reqs) // 24)
     torch.cuda.synchronize()
@@ -940,7 +943,7 @@ def run_reference_serve(args):
         return
     reqs = serve_requests(args, 0)
     P = min(os.cpu_count() or 1, SERVE_CPU_PROCS)
-    pool = wl.serve_pool(only={r.mesh for r in reqs[:P]})
+    pool = wl.serve_pool(only={r.mesh for r in reqs[:P]}, cache_dir=args.pool_dir)
     steps = max(1, min(args.steps, 2))
     cb = serve_cpu_sample(pool, reqs, steps)
     faces = sum(pool.meshes[r.mesh].n_active_faces for r in reqs[:P])

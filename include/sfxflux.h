@@ -49,6 +49,8 @@ extern "C" {
 #define SFX_ERR_NOMEM 10      /* device memory budget exceeded             */
 #define SFX_ERR_NOT_READY 11  /* server: result not available yet          */
 #define SFX_ERR_CLOSED 12     /* server: shut down                         */
+#define SFX_ERR_IO 14         /* mesh file missing, truncated, corrupt or of
+                                 another version                            */
 
 /* ---- solver kinds and precision modes ---- */
 #define SFX_SOLVER_EXACT 0 /* ExactRiemannSolver, tag "EXAC" */
@@ -297,6 +299,25 @@ int sfx_voronoi_export(const sfx_voronoi* v, double* cell_centroid,
                        int32_t* face_left, int32_t* face_right,
                        int32_t* face_kind, double* face_right_pos);
 void sfx_voronoi_free(sfx_voronoi* v);
+
+/* ---- versioned binary mesh file (no counterpart in the reference, which
+ * re-tessellates at every start; the pre-tessellated pool of the request
+ * service is built once and read back through these) ----
+ * sfx_meshfile_write stores a face list in the sfx_mesh_desc layout with its
+ * periodicity (face velocities when not NULL); sfx_meshfile_info returns its
+ * sizes (any output may be NULL); sfx_meshfile_read fills caller arrays of
+ * those sizes (face_velocity may be NULL; zeros when the file has none).
+ * Every read checks the magic, the version, the section table and a
+ * checksum of the payload: SFX_ERR_IO otherwise. */
+#define SFX_MESHFILE_VERSION 1
+int sfx_meshfile_write(const char* path, const sfx_mesh_desc* mesh, int32_t periodic);
+int sfx_meshfile_info(const char* path, int32_t* dim, int32_t* periodic, int64_t* n_cells,
+                      int64_t* n_faces, int64_t* n_cell_faces, int32_t* has_velocity);
+int sfx_meshfile_read(const char* path, double* cell_pos, double* cell_centroid,
+                      double* cell_volume, double* cell_total_area, int32_t* cell_face_offset,
+                      int32_t* cell_face_index, double* face_area, double* face_midpoint,
+                      int32_t* face_left, int32_t* face_right, int32_t* face_kind,
+                      double* face_right_pos, double* face_velocity);
 
 /* ---- request server: continuous batching of static-mesh integrations ----
  * No counterpart in the reference (Shadowfax runs one simulation per job).

@@ -20,12 +20,12 @@ STATUS_NAMES = {
     4: "SFX_ERR_NAN_FLUX", 5: "SFX_ERR_NEG_STATE", 6: "SFX_ERR_NOCONV",
     7: "SFX_ERR_BOUNDS", 8: "SFX_ERR_UNSUPPORTED", 9: "SFX_ERR_MESH",
     10: "SFX_ERR_NOMEM", 11: "SFX_ERR_NOT_READY", 12: "SFX_ERR_CLOSED",
-    13: "SFX_ERR_TOO_LARGE",
+    13: "SFX_ERR_TOO_LARGE", 14: "SFX_ERR_IO",
 }
 SFX_ERR_INVALID, SFX_ERR_CUDA, SFX_ERR_RIEMANN, SFX_ERR_NAN_FLUX = 1, 2, 3, 4
 SFX_ERR_NEG_STATE, SFX_ERR_NOCONV, SFX_ERR_BOUNDS, SFX_ERR_UNSUPPORTED = 5, 6, 7, 8
 SFX_ERR_MESH, SFX_ERR_NOMEM, SFX_ERR_NOT_READY, SFX_ERR_CLOSED = 9, 10, 11, 12
-SFX_ERR_TOO_LARGE = 13
+SFX_ERR_TOO_LARGE, SFX_ERR_IO = 13, 14
 
 SOLVER_EXACT, SOLVER_HLLC = 0, 1
 PREC_FP64, PREC_SPLIT = 0, 1
@@ -128,6 +128,11 @@ PROTOTYPES = {
     "sfx_voronoi_export": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip, _ip, _dp, _dp, _ip, _ip,
                                      _ip, _dp]),
     "sfx_voronoi_free": (None, [C.c_void_p]),
+    "sfx_meshfile_write": (C.c_int, [C.c_char_p, C.POINTER(sfx_mesh_desc), C.c_int32]),
+    "sfx_meshfile_info": (C.c_int, [C.c_char_p, _ip, _ip, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64), _ip]),
+    "sfx_meshfile_read": (C.c_int, [C.c_char_p, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _dp, _ip,
+                                    _ip, _ip, _dp, _dp]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_mesh_set_ranges": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sfx_mesh_pack_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,

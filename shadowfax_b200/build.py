@@ -7,6 +7,7 @@
   division and square root approximate)
 * ``csrc/sfx_api.cu``    C ABI (include/sfxflux.h)
 * ``csrc/sfx_voronoi.cpp`` host face-list builder
+* ``csrc/sfx_meshfile.cpp`` versioned binary mesh files
 
 with ``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo`` into
 ``shadowfax_b200/libsfxflux.so``.  nvcc cross-compiles, so this runs on a
@@ -42,6 +43,7 @@ UNITS = {
     "sfx_group.cu": [],
     "sfx_server.cu": [],
     "sfx_voronoi.cpp": [],
+    "sfx_meshfile.cpp": [],
 }
 
 

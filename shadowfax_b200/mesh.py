@@ -102,6 +102,38 @@ class Mesh:
         return cls(dim=dim, periodic=bool(periodic),
                    **{n: z[n] for n in cls._ARRAYS}).normalized()
 
+    def write_file(self, path: str | Path) -> None:
+        """the library's versioned binary mesh file (sfx_meshfile_write)"""
+        L.check(L.lib().sfx_meshfile_write(str(path).encode(), C.byref(self.desc()),
+                                           int(self.periodic)), "sfx_meshfile_write")
+
+    @classmethod
+    def read_file(cls, path: str | Path) -> "Mesh":
+        """a mesh from sfx_meshfile_write's file (sfx_meshfile_info/_read)"""
+        p = str(path).encode()
+        dim, per, vel = C.c_int32(), C.c_int32(), C.c_int32()
+        n, nf, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+        L.check(L.lib().sfx_meshfile_info(p, C.byref(dim), C.byref(per), C.byref(n),
+                                          C.byref(nf), C.byref(nnz), C.byref(vel)),
+                "sfx_meshfile_info")
+        d, n, nf, nnz = dim.value, n.value, nf.value, nnz.value
+        m = cls(dim=d, periodic=bool(per.value),
+                cell_pos=np.empty((n, d)), cell_centroid=np.empty((n, d)),
+                cell_volume=np.empty(n), cell_total_area=np.empty(n),
+                cell_face_offset=np.empty(n + 1, np.int32),
+                cell_face_index=np.empty(nnz, np.int32),
+                face_area=np.empty(nf), face_midpoint=np.empty((nf, d)),
+                face_left=np.empty(nf, np.int32), face_right=np.empty(nf, np.int32),
+                face_kind=np.empty(nf, np.int32), face_right_pos=np.empty((nf, d)),
+                face_velocity=np.empty((nf, d)) if vel.value else None)
+        L.check(L.lib().sfx_meshfile_read(
+            p, L.dptr(m.cell_pos), L.dptr(m.cell_centroid), L.dptr(m.cell_volume),
+            L.dptr(m.cell_total_area), L.iptr(m.cell_face_offset), L.iptr(m.cell_face_index),
+            L.dptr(m.face_area), L.dptr(m.face_midpoint), L.iptr(m.face_left),
+            L.iptr(m.face_right), L.iptr(m.face_kind), L.dptr(m.face_right_pos),
+            L.dptr(m.face_velocity) if vel.value else None), "sfx_meshfile_read")
+        return m
+
     def check_geometry(self, rtol: float = 1e-9) -> None:
         """Sanity checks of a tessellation of the unit box."""
         tot = float(self.cell_volume.sum())

@@ -2,7 +2,8 @@
 
 Inputs are seeded synthetic stand-ins (numpy PCG64 streams): generators
 uniform in the unit square/cube, tessellated by the host face-list builder,
-with each workload's initial states.  Nothing here reads files.
+with each workload's initial states.  Files are read only where a caller
+asks for a mesh cache (serve_pool's cache_dir).
 
   sod2d           2D Sod tube, reflective unit square, exact solver, dt = 1e-4, 100 steps
   sedov3d         3D Sedov-type blast, reflective unit cube, HLLC, global CFL 0.4, 50 steps
@@ -170,11 +171,16 @@ class ServeRequest:
 
 
 def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
-               workers: int = 0) -> ServePool:
+               workers: int = 0, cache_dir=None) -> ServePool:
     """the pool meshes (all 2k, or the indices in `only`), tessellated
-    concurrently, largest first"""
+    concurrently, largest first; with `cache_dir`, each mesh is read from
+    its mesh file there when present and written there after tessellation
+    otherwise (sfx_meshfile_*)"""
     import os
     from concurrent.futures import ThreadPoolExecutor
+    from pathlib import Path
+
+    from .mesh import Mesh
     sizes = serve_pool_sizes(k)
     jobs = [j for j in range(2 * k) if only is None or j in only]
     workers = workers or max(1, min(4, (os.cpu_count() or 4) // 4))
@@ -182,8 +188,16 @@ def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
     def one(j):
         dim, b = 2 + j // k, j % k
         n = int(sizes[b])
-        pos = random_generators(n, dim, seed * 1_000_003 + dim * 1000 + b)
-        mesh = build_voronoi(pos, periodic=True)
+        gen_seed = seed * 1_000_003 + dim * 1000 + b
+        path = None
+        if cache_dir:
+            path = Path(cache_dir) / f"pool_{dim}d_n{n}_seed{gen_seed}.sfxmesh"
+        if path is not None and path.exists():
+            mesh = Mesh.read_file(path)
+        else:
+            mesh = build_voronoi(random_generators(n, dim, gen_seed), periodic=True)
+            if path is not None:
+                mesh.write_file(path)
         Ws = [random_field_state(mesh, seed * 7919 + dim * 1000 + b * 10 + s)
               for s in range(states_per_mesh)]
         return mesh, Ws, [cfl_dt(mesh, W) for W in Ws]
