@@ -42,8 +42,7 @@ enum Section : uint32_t {
     kFaceRight,
     kFaceKind,
     kFaceRightPos,
-    kFaceVelocity,
-    kSectionEnd
+    kFaceVelocity
 };
 
 struct Header {
