@@ -217,10 +217,17 @@ class PartitionedPass:
     (plain FP64, one GPU per rank): the local mesh with its two rings on the
     device, the pass restricted to it, and the ring exchange after every
     step.  The owned cells' W and Q equal those of a pass over the whole
-    mesh, bit for bit."""
+    mesh, bit for bit.
+
+    Every rank of the group constructs its PartitionedPass (the constructor
+    ends with a barrier, so that the first point-to-point batch is not the
+    group's first collective) and calls step() with the same arguments.  The
+    context's stream becomes torch's current stream on ctx.device (set that
+    device current first), for the context's other meshes too."""
 
     def __init__(self, ctx, mesh: Mesh, owner: np.ndarray, rank: int, group=None):
         import torch
+        import torch.distributed as dist
 
         from .hydro import FluxPass
         self.part = build_part(mesh, owner, rank)
@@ -244,6 +251,8 @@ class PartitionedPass:
                          for p, (s, _) in self.plan.items()}
         self.recv_buf = {p: torch.empty((len(r), R), dtype=torch.float64, device=dev)
                          for p, (_, r) in self.plan.items()}
+        if dist.is_initialized():
+            dist.barrier(group)
 
     def set_primitive(self, W_global: np.ndarray) -> None:
         self.fp.set_primitive(np.asarray(W_global)[self.part.cells])

@@ -125,3 +125,18 @@ def test_decomposed_steps_equal_the_whole_mesh(oracle, name):
         assert np.array_equal(W[r], Wg[pt.cells])
         assert np.array_equal(Q[r][:pt.n_own], Qg[pt.cells[:pt.n_own]])
         assert np.array_equal(Q[r][:, 0], Qg[pt.cells, 0])
+
+
+def test_one_part_is_the_whole_mesh_and_bad_counts_are_refused():
+    mesh, _, _ = load_case("random2d_periodic_exact")
+    owner = P.partition(mesh, 1)
+    assert np.all(owner == 0)
+    pt = P.build_part(mesh, owner, 0)
+    assert pt.n_own == pt.n_grad == mesh.n_cells == len(pt.cells)
+    assert pt.n_flux == mesh.n_faces
+    assert np.array_equal(pt.cells, np.arange(mesh.n_cells))
+    assert np.array_equal(pt.mesh.cell_face_index, mesh.cell_face_index)
+    assert P.exchange_plan(mesh, owner, pt) == {}
+    for bad in (0, mesh.n_cells + 1):
+        with pytest.raises(ValueError):
+            P.partition(mesh, bad)
