@@ -266,9 +266,12 @@ class PartitionedPass:
             if idx.numel():
                 self.fp.unpack_cells(idx, self.recv_buf[p])
 
-    def step(self, dt: float, nsteps: int = 1) -> None:
+    def step(self, dt: float, nsteps: int = 1, check: bool = True) -> None:
+        """nsteps, each followed by the ring exchange; with `check`, each
+        step's status is read back (SfxError on the reference's errors, at
+        the cost of one synchronisation per step)"""
         for _ in range(nsteps):
-            self.fp.step(dt, 1, stats=False)
+            self.fp.step(dt, 1, stats=check)
             self.exchange()
 
     def owned_state(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
