@@ -241,6 +241,7 @@ class PartitionedPass:
         self.fp = FluxPass(ctx, self.part.mesh)
         self.fp.set_ranges(self.part.n_grad, self.part.n_flux, self.part.n_own)
         dev = torch.device("cuda", ctx.device)
+        self.send_buf_device = dev
         # the library's kernels on torch's current stream, so that the
         # records are packed before they are sent and stored after they arrive
         ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
@@ -267,11 +268,30 @@ class PartitionedPass:
                 self.fp.unpack_cells(idx, self.recv_buf[p])
 
     def step(self, dt: float, nsteps: int = 1, check: bool = True) -> None:
-        """nsteps, each followed by the ring exchange; with `check`, each
-        step's status is read back (SfxError on the reference's errors, at
-        the cost of one synchronisation per step)"""
+        """nsteps, each followed by the ring exchange.  With `check`, every
+        rank reads back its step's status and the ranks agree on the worst
+        one (a MAX all-reduce) before exchanging, so that a failing part
+        (the reference's exceptions) stops every rank with SfxError instead
+        of leaving the others waiting in the exchange."""
+        import torch
+        import torch.distributed as dist
+
+        from ._lib import SfxError
         for _ in range(nsteps):
-            self.fp.step(dt, 1, stats=check)
+            err = None
+            try:
+                self.fp.step(dt, 1, stats=check)
+            except SfxError as e:
+                err = e
+            if check and dist.is_initialized():
+                flag = torch.tensor([0 if err is None else err.status], dtype=torch.int32,
+                                    device=self.send_buf_device)
+                dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=self.group)
+                worst = int(flag.item())
+                if worst:
+                    raise err or SfxError(worst, "sfx_step on another rank")
+            elif err is not None:
+                raise err
             self.exchange()
 
     def owned_state(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
