@@ -241,7 +241,7 @@ class PartitionedPass:
         self.fp = FluxPass(ctx, self.part.mesh)
         self.fp.set_ranges(self.part.n_grad, self.part.n_flux, self.part.n_own)
         dev = torch.device("cuda", ctx.device)
-        self.send_buf_device = dev
+        self.device = dev
         # the library's kernels on torch's current stream, so that the
         # records are packed before they are sent and stored after they arrive
         ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
@@ -285,7 +285,7 @@ class PartitionedPass:
                 err = e
             if check and dist.is_initialized():
                 flag = torch.tensor([0 if err is None else err.status], dtype=torch.int32,
-                                    device=self.send_buf_device)
+                                    device=self.device)
                 dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=self.group)
                 worst = int(flag.item())
                 if worst:
