@@ -714,8 +714,9 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
             "peak_source": f"hbm_gbs {peak_kind} (of measured)",
             "algorithmic_bytes_per_launch": pc["algorithmic_bytes"][top],
             "kernel_ms": kms,
-            "note": "the exact-solver face kernel is bound by the FP64 pipe (p* iteration), "
-                    "not by HBM; its FP64 pipe utilisation is in profiles/",
+            "note": "the exact-solver face kernel is bound by instruction issue and FP64 "
+                    "latency (divergent solver paths), not by HBM; its pipe utilisation is "
+                    "in profiles/",
             "step_bytes_per_face": STEP_BYTES[("split", D)],
             "step_frac": pc["step_frac"],
             "classes": {f"{c[0]}D {c[1]}": v for c, v in per_class.items()}}
@@ -826,8 +827,8 @@ def bench_serve(args, rank, world, local, torch):
                                    f"dimension), random-field states, steps U{{10..200}}, "
                                    f"exact/HLLC 50/50, 150 GB budget",
                        "step": "one request of the stream",
-                       "precision": "split (FP32 reconstruction/HLLC, FP64 p* iteration, "
-                                    "FP64 accumulation)",
+                       "precision": "split (FP32 reconstruction/HLLC/p* Newton, FP64 final "
+                                    "p* step and accumulation)",
                        "chunk_steps": args.chunk, "resident_waves": nwaves,
                        "resident_failed_requests": nfail_res,
                        "l2": "working set > L2 (no flush)",

@@ -57,8 +57,9 @@ extern "C" {
 #define SFX_SOLVER_HLLC 1  /* HLLCRiemannSolver, tag "HLLC"  */
 
 #define SFX_PREC_FP64 0  /* plain FP64, bit-identical to the CPU oracle      */
-#define SFX_PREC_SPLIT 1 /* FP32 reconstruction/prediction/HLLC, FP64 p*
-                            iteration, FP64 accumulation of Q              */
+#define SFX_PREC_SPLIT 1 /* FP32 reconstruction/prediction/HLLC and p*
+                            Newton iteration, FP64 final p* step, sampling
+                            and accumulation of Q                          */
 
 /* ---- face kinds (the right generator of a VorFace) ---- */
 #define SFX_FACE_REAL 0     /* right is a local cell                        */
