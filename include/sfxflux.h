@@ -308,9 +308,14 @@ void sfx_voronoi_free(sfx_voronoi* v);
  * periodicity (face velocities when not NULL); sfx_meshfile_info returns its
  * sizes (any output may be NULL); sfx_meshfile_read fills caller arrays of
  * those sizes (face_velocity may be NULL; zeros when the file has none).
- * Every read checks the magic, the version, the section table and a
- * checksum of the payload: SFX_ERR_IO otherwise. */
+ * Every read checks the magic, the major version (a higher major is
+ * rejected; a later minor version only adds sections, which this reader
+ * skips), the section table against the file size, a checksum of the
+ * payload and the cell face offsets (0 first, never decreasing, n_cell_faces
+ * last): SFX_ERR_IO otherwise, SFX_ERR_NOMEM when the payload cannot be
+ * held in host memory. */
 #define SFX_MESHFILE_VERSION 1
+#define SFX_MESHFILE_MINOR_VERSION 0
 int sfx_meshfile_write(const char* path, const sfx_mesh_desc* mesh, int32_t periodic);
 int sfx_meshfile_info(const char* path, int32_t* dim, int32_t* periodic, int64_t* n_cells,
                       int64_t* n_faces, int64_t* n_cell_faces, int32_t* has_velocity);
@@ -399,6 +404,9 @@ int sfx_server_shutdown(sfx_server* srv);
  * on `cuda_stream` (NULL = legacy default stream), and waits for it before
  * returning the status.  The first call on a device looks up the scratch
  * array's device address; make that first call before any stream capture.
+ * The lookup is repeated when the device's context has changed (after a
+ * cudaDeviceReset), so make the first call after a reset before any capture
+ * too.
  * All calls share the scratch array: calls that overlap on the GPU (other
  * threads, other streams) race and must be serialised by the caller.
  * Mesh indices are not range-checked on the device: they must be valid. */

@@ -5,20 +5,24 @@
  * meshes is built once and read back by any caller of the C ABI.
  *
  * Layout, little-endian:
- *   header (128 bytes)   magic "SFXMESH\0", version, header size, dim,
+ *   header (128 bytes)   magic "SFXMESH\0", major version, header size, dim,
  *                        flags (bit 0 periodic, bit 1 face velocities),
  *                        n_cells, n_faces, n_cell_faces, section count,
- *                        payload offset and size, FNV-1a 64 checksum of the
- *                        payload
+ *                        minor version, payload offset and size, FNV-1a 64
+ *                        checksum of the payload
  *   section table        per array: id, element size, element count, offset
  *   payload              the arrays, each at a 64-byte aligned offset, in
  *                        the descriptor's layout ([n][dim] row-major)
- * A reader skips sections whose id it does not know, so later versions can
- * add arrays; a file with a higher major version is rejected.
+ * A reader skips sections whose id it does not know, so a later minor
+ * version can add arrays and stay readable; a file with a higher major
+ * version (a changed meaning of an existing array) is rejected.  Sizes in the
+ * header are never trusted: the payload must lie inside the file, and the
+ * cell face offsets must run from 0 to n_cell_faces without decreasing.
  */
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "sfxflux.h"
@@ -55,7 +59,7 @@ struct Header {
     int64_t n_faces;
     int64_t n_cell_faces;
     uint32_t n_sections;
-    uint32_t reserved;
+    uint32_t minor_version; /* readers ignore it: later minors only add sections */
     uint64_t payload_offset;
     uint64_t payload_bytes;
     uint64_t checksum;
@@ -143,6 +147,7 @@ int sfx_meshfile_write(const char* path, const sfx_mesh_desc* m, int32_t periodi
     std::memset(&h, 0, sizeof h);
     std::memcpy(h.magic, kMagic, 8);
     h.version = SFX_MESHFILE_VERSION;
+    h.minor_version = SFX_MESHFILE_MINOR_VERSION;
     h.header_bytes = kHeaderBytes;
     h.dim = (uint32_t)m->dim;
     h.flags = (periodic ? 1u : 0u) | (m->face_velocity ? 2u : 0u);
@@ -160,7 +165,12 @@ int sfx_meshfile_write(const char* path, const sfx_mesh_desc* m, int32_t periodi
     }
     h.payload_bytes = off - h.payload_offset;
     /* the payload with its zero padding, checksummed as written */
-    std::vector<uint8_t> payload(h.payload_bytes, 0);
+    std::vector<uint8_t> payload;
+    try {
+        payload.assign(h.payload_bytes, 0);
+    } catch(const std::bad_alloc&) {
+        return SFX_ERR_NOMEM;
+    }
     for(size_t i = 0; i < arrs.size(); ++i)
         if(tab[i].count)
             std::memcpy(payload.data() + (tab[i].offset - h.payload_offset), arrs[i].src,
@@ -194,12 +204,22 @@ int read_file(const char* path, Header& h, std::vector<Entry>& tab,
     File in;
     in.f = std::fopen(path, "rb");
     if(!in.f) return SFX_ERR_IO;
+    if(std::fseek(in.f, 0, SEEK_END) != 0) return SFX_ERR_IO;
+    const long long file_bytes = std::ftell(in.f);
+    if(file_bytes < 0 || std::fseek(in.f, 0, SEEK_SET) != 0) return SFX_ERR_IO;
     if(std::fread(&h, 1, sizeof h, in.f) != sizeof h) return SFX_ERR_IO;
-    if(std::memcmp(h.magic, kMagic, 8) != 0 || h.version != SFX_MESHFILE_VERSION ||
-       h.header_bytes != kHeaderBytes || (h.dim != 2 && h.dim != 3) || h.n_cells < 0 ||
-       h.n_faces < 0 || h.n_cell_faces < 0 || h.n_cells > INT32_MAX ||
-       h.n_faces > INT32_MAX || h.n_cell_faces > INT32_MAX || h.n_sections > 64)
+    /* major version 0 never existed; a higher major is a format this reader
+     * does not understand */
+    if(std::memcmp(h.magic, kMagic, 8) != 0 || h.version == 0 ||
+       h.version > SFX_MESHFILE_VERSION || h.header_bytes != kHeaderBytes ||
+       (h.dim != 2 && h.dim != 3) || h.n_cells < 0 || h.n_faces < 0 || h.n_cell_faces < 0 ||
+       h.n_cells > INT32_MAX - 1 || h.n_faces > INT32_MAX || h.n_cell_faces > INT32_MAX ||
+       h.n_sections > 64)
         return SFX_ERR_IO;
+    /* the payload lies inside the file (no allocation sized by a header
+     * field alone) */
+    const uint64_t fb = (uint64_t)file_bytes;
+    if(h.payload_offset > fb || h.payload_bytes > fb - h.payload_offset) return SFX_ERR_IO;
     tab.resize(h.n_sections);
     if(h.n_sections &&
        std::fread(tab.data(), sizeof(Entry), h.n_sections, in.f) != h.n_sections)
@@ -209,12 +229,17 @@ int read_file(const char* path, Header& h, std::vector<Entry>& tab,
     for(const Entry& e : tab) {
         if(e.elem_bytes != 4 && e.elem_bytes != 8) return SFX_ERR_IO;
         if(e.count > (uint64_t)1 << 40 || e.offset < h.payload_offset ||
-           e.offset + e.count * e.elem_bytes > h.payload_offset + h.payload_bytes)
+           e.offset - h.payload_offset > h.payload_bytes ||
+           e.count * e.elem_bytes > h.payload_bytes - (e.offset - h.payload_offset))
             return SFX_ERR_IO;
     }
     if(!payload) return SFX_OK;
     if(std::fseek(in.f, (long)h.payload_offset, SEEK_SET) != 0) return SFX_ERR_IO;
-    payload->assign(h.payload_bytes, 0);
+    try {
+        payload->assign(h.payload_bytes, 0);
+    } catch(const std::bad_alloc&) {
+        return SFX_ERR_NOMEM;
+    }
     if(h.payload_bytes &&
        std::fread(payload->data(), 1, h.payload_bytes, in.f) != h.payload_bytes)
         return SFX_ERR_IO;
@@ -228,7 +253,12 @@ int sfx_meshfile_info(const char* path, int32_t* dim, int32_t* periodic, int64_t
                       int64_t* n_faces, int64_t* n_cell_faces, int32_t* has_velocity) {
     Header h;
     std::vector<Entry> tab;
-    const int rc = read_file(path, h, tab, nullptr);
+    int rc;
+    try {
+        rc = read_file(path, h, tab, nullptr);
+    } catch(const std::bad_alloc&) {
+        return SFX_ERR_NOMEM;
+    }
     if(rc) return rc;
     if(dim) *dim = (int32_t)h.dim;
     if(periodic) *periodic = (h.flags & 1u) ? 1 : 0;
@@ -247,7 +277,12 @@ int sfx_meshfile_read(const char* path, double* cell_pos, double* cell_centroid,
     Header h;
     std::vector<Entry> tab;
     std::vector<uint8_t> payload;
-    const int rc = read_file(path, h, tab, &payload);
+    int rc;
+    try {
+        rc = read_file(path, h, tab, &payload);
+    } catch(const std::bad_alloc&) {
+        return SFX_ERR_NOMEM;
+    }
     if(rc) return rc;
     const bool vel = (h.flags & 2u) != 0;
     std::vector<Array> want = layout((int)h.dim, h.n_cells, h.n_faces, h.n_cell_faces, vel);
@@ -270,6 +305,13 @@ int sfx_meshfile_read(const char* path, double* cell_pos, double* cell_centroid,
             std::memcpy(dst[i], payload.data() + (e->offset - h.payload_offset),
                         e->count * e->elem_bytes);
     }
+    /* the cell face lists must cover exactly the n_cell_faces entries the
+     * caller sized cell_face_index for: sfx_mesh_upload reads up to
+     * offset[n_cells] of them */
+    const int32_t* off = cell_face_offset;
+    if(off[0] != 0 || off[h.n_cells] != h.n_cell_faces) return SFX_ERR_IO;
+    for(int64_t i = 0; i < h.n_cells; ++i)
+        if(off[i + 1] < off[i]) return SFX_ERR_IO;
     if(!vel && face_velocity && h.n_faces)
         std::memset(face_velocity, 0, sizeof(double) * (size_t)h.n_faces * h.dim);
     return SFX_OK;

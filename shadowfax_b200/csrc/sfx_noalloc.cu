@@ -11,13 +11,17 @@
  * The array is a file-scope __device__ variable, so every GPU that loads the
  * library holds it (SFX_NOALLOC_MAX_CELLS x 15 doubles = 7.5 MiB) until the
  * process exits.  In host code its name is only a host-side stand-in, not a
- * device address: the address is looked up once per device with
+ * device address: the address is looked up once per device context with
  * cudaGetSymbolAddress (on the first call made on that device, which should
- * therefore come before any stream capture) and passed to the kernels.
+ * therefore come before any stream capture) and passed to the kernels.  The
+ * lookup is repeated when the device's context changes (after a
+ * cudaDeviceReset the module is loaded again and the old address is gone);
+ * the first call after such a reset should again come before any capture.
  * Every call reuses the array and overwrites all the gradients it reads, so
  * nothing but the error record has to be cleared; calls that overlap on the
  * GPU race on the array.
  */
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -36,11 +40,45 @@ static __device__ __align__(256) sfx_dev_error g_noalloc_err;
 std::mutex g_setup_mutex;
 void* g_grad_addr[kMaxDevices];
 void* g_err_addr[kMaxDevices];
+unsigned long long g_ctx_id[kMaxDevices]; /* context the addresses belong to */
 
-/* per device, with that device current: device addresses of the arrays */
+typedef CUresult (*ctx_current_fn)(CUcontext*);
+typedef CUresult (*ctx_id_fn)(CUcontext, unsigned long long*);
+ctx_current_fn g_ctx_current = nullptr;
+ctx_id_fn g_ctx_get_id = nullptr;
+std::once_flag g_ctx_fn_once;
+
+/* the unique id of the calling thread's current context, 0 when there is
+ * none or the driver cannot report it (then every call looks the addresses
+ * up again) */
+unsigned long long current_context_id() {
+    std::call_once(g_ctx_fn_once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) ==
+                   cudaSuccess &&
+           q == cudaDriverEntryPointSuccess)
+            g_ctx_current = (ctx_current_fn)f;
+        f = nullptr;
+        if(cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+           q == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = (ctx_id_fn)f;
+        cudaGetLastError();
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if(!g_ctx_current || !g_ctx_get_id || g_ctx_current(&c) != CUDA_SUCCESS || !c ||
+       g_ctx_get_id(c, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+/* per device, with that device current: device addresses of the arrays in
+ * the current context */
 int scratch_addresses(int dev, double** grad, sfx_dev_error** err) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if(!g_grad_addr[dev]) {
+    const unsigned long long id = current_context_id();
+    if(!g_grad_addr[dev] || id == 0 || id != g_ctx_id[dev]) {
         void* g = nullptr;
         void* e = nullptr;
         if(cudaGetSymbolAddress(&g, g_noalloc_grad) != cudaSuccess ||
@@ -50,6 +88,8 @@ int scratch_addresses(int dev, double** grad, sfx_dev_error** err) {
         }
         g_err_addr[dev] = e;
         g_grad_addr[dev] = g;
+        /* the lookup made the device's context current if it was not */
+        g_ctx_id[dev] = current_context_id();
     }
     *grad = (double*)g_grad_addr[dev];
     *err = (sfx_dev_error*)g_err_addr[dev];

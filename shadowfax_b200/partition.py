@@ -223,9 +223,16 @@ class PartitionedPass:
     ends with a barrier, so that the first point-to-point batch is not the
     group's first collective) and calls step() with the same arguments.  The
     context's stream becomes torch's current stream on ctx.device (set that
-    device current first), for the context's other meshes too."""
+    device current first), for the context's other meshes too.
 
-    def __init__(self, ctx, mesh: Mesh, owner: np.ndarray, rank: int, group=None):
+    Over a gloo group the records are staged through host memory and the
+    status flag is a CPU tensor.  `flux_pass` replaces the device pass over
+    the part (any object with FluxPass's set_ranges / set_primitive / step /
+    pack_cells / unpack_cells / state working on CPU tensors); tests use it to
+    run this class on CPU ranks."""
+
+    def __init__(self, ctx, mesh: Mesh, owner: np.ndarray, rank: int, group=None,
+                 flux_pass=None):
         import torch
         import torch.distributed as dist
 
@@ -238,13 +245,22 @@ class PartitionedPass:
                     (len(r) and (r.min() < self.part.n_own or r.max() >= n_local)):
                 raise ValueError("exchange list outside the part")
         self.group = group
-        self.fp = FluxPass(ctx, self.part.mesh)
+        gloo = dist.is_initialized() and dist.get_backend(group) == "gloo"
+        if flux_pass is None:
+            self.fp = FluxPass(ctx, self.part.mesh)
+            dev = torch.device("cuda", ctx.device)
+            # the library's kernels on torch's current stream, so that the
+            # records are packed before they are sent and stored after they
+            # arrive
+            ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        else:
+            self.fp = flux_pass
+            dev = torch.device("cpu")
         self.fp.set_ranges(self.part.n_grad, self.part.n_flux, self.part.n_own)
-        dev = torch.device("cuda", ctx.device)
+        # records are packed and stored on `device`; they travel from
+        # `comm_device` (host memory for gloo)
         self.device = dev
-        # the library's kernels on torch's current stream, so that the
-        # records are packed before they are sent and stored after they arrive
-        ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        self.comm_device = torch.device("cpu") if gloo else dev
         R = mesh.dim + 3
         self.send_idx = {p: torch.as_tensor(s, device=dev) for p, (s, _) in self.plan.items()}
         self.recv_idx = {p: torch.as_tensor(r, device=dev) for p, (_, r) in self.plan.items()}
@@ -262,7 +278,14 @@ class PartitionedPass:
         for p, idx in self.send_idx.items():
             if idx.numel():
                 self.fp.pack_cells(idx, self.send_buf[p])
-        exchange_records(self.send_buf, self.recv_buf, self.group)
+        if self.comm_device == self.device:
+            exchange_records(self.send_buf, self.recv_buf, self.group)
+        else:
+            recv = {p: b.to(self.comm_device) for p, b in self.recv_buf.items()}
+            exchange_records({p: b.to(self.comm_device) for p, b in self.send_buf.items()},
+                             recv, self.group)
+            for p, b in recv.items():
+                self.recv_buf[p].copy_(b)
         for p, idx in self.recv_idx.items():
             if idx.numel():
                 self.fp.unpack_cells(idx, self.recv_buf[p])
@@ -285,7 +308,7 @@ class PartitionedPass:
                 err = e
             if check and dist.is_initialized():
                 flag = torch.tensor([0 if err is None else err.status], dtype=torch.int32,
-                                    device=self.device)
+                                    device=self.comm_device)
                 dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=self.group)
                 worst = int(flag.item())
                 if worst:

@@ -1,7 +1,9 @@
 """The versioned binary mesh file (sfx_meshfile_*): round trips, the layout
 read back by an independent parser written from the format's description,
-forward compatibility (unknown sections are skipped) and rejection of
-corrupt, truncated and other-version files."""
+forward compatibility (unknown sections and later minor versions are read)
+and rejection of corrupt, truncated and other-major-version files, of header
+sizes that do not fit the file and of cell face offsets that do not cover
+the face list."""
 import struct
 
 import numpy as np
@@ -76,7 +78,7 @@ def test_layout_matches_its_description(tmp_path):
         assert np.array_equal(secs[sid], getattr(m, name).ravel()), name
 
 
-def _write_py(path, m: Mesh, extra=None, version=1):
+def _write_py(path, m: Mesh, extra=None, version=1, minor=0):
     """an independent writer, with optional extra sections {id: bytes}"""
     arrs = [(sid, eb, getattr(m, name)) for name, sid, eb in ARRAYS
             if getattr(m, name) is not None]
@@ -94,7 +96,7 @@ def _write_py(path, m: Mesh, extra=None, version=1):
         off += len(b)
     flags = int(m.periodic) | (2 if m.face_velocity is not None else 0)
     head = HEADER.pack(b"SFXMESH\0", version, 128, m.dim, flags, m.n_cells, m.n_faces, m.nnz,
-                       nsec, 0, poff, len(body), _fnv1a(bytes(body)))
+                       nsec, minor, poff, len(body), _fnv1a(bytes(body)))
     raw = head + b"".join(table)
     raw += bytes(poff - len(raw))
     path.write_bytes(raw + bytes(body))
@@ -145,3 +147,52 @@ def test_serve_pool_reads_back_its_cached_meshes(tmp_path):
         _same(a.meshes[j], b.meshes[j])
         for x, y in zip(a.states[j], b.states[j]):
             assert np.array_equal(x, y)
+
+
+def test_later_minor_version_with_new_sections_is_read(tmp_path):
+    m = _mesh(3, True)
+    f = tmp_path / "m.sfxmesh"
+    _write_py(f, m, extra={90: np.arange(6, dtype=np.int32).tobytes()}, minor=3)
+    _same(m, Mesh.read_file(f))
+    _write_py(f, m, version=0)
+    with pytest.raises(L.SfxError, match="SFX_ERR_IO"):
+        Mesh.read_file(f)
+
+
+def test_header_sizes_beyond_the_file_are_rejected(tmp_path):
+    """the header is not covered by the checksum: a payload size far beyond
+    the file must be refused before anything is allocated for it"""
+    m = _mesh(2, False)
+    f = tmp_path / "m.sfxmesh"
+    m.write_file(f)
+    raw = bytearray(f.read_bytes())
+    fields = list(HEADER.unpack_from(raw, 0))
+    for k, v in ((11, 1 << 62), (11, len(raw)), (10, len(raw) + 64)):
+        bad = list(fields)
+        bad[k] = v
+        g = tmp_path / f"bad{k}_{v}.sfxmesh"
+        g.write_bytes(HEADER.pack(*bad) + bytes(raw[HEADER.size:]))
+        with pytest.raises(L.SfxError, match="SFX_ERR_IO"):
+            Mesh.read_file(g)
+
+
+@pytest.mark.parametrize("how", ["past_end", "short", "decreasing", "nonzero_first"])
+def test_cell_face_offsets_must_cover_the_face_list(tmp_path, how):
+    """a well-formed file (valid checksum) whose cell face offsets do not run
+    from 0 to n_cell_faces without decreasing is rejected (the upload would
+    read past the face index array)"""
+    m = _mesh(2, True, n=400)
+    off = m.cell_face_offset.copy()
+    if how == "past_end":
+        off[-1] += 7
+    elif how == "short":
+        off[-1] -= 1
+    elif how == "decreasing":
+        off[5], off[6] = off[6], off[5]
+    else:
+        off[0] = 1
+    m.cell_face_offset = off
+    f = tmp_path / f"{how}.sfxmesh"
+    _write_py(f, m)
+    with pytest.raises(L.SfxError, match="SFX_ERR_IO"):
+        Mesh.read_file(f)

@@ -1,10 +1,15 @@
-"""The N>1 host logic of bench.py on CPU ranks (gloo, world size 2): each rank
-serves its own request stream, and the whole-job figure is the work of all
-ranks over the slowest rank's time."""
+"""The N>1 host logic on CPU ranks (gloo, world size 2): the whole-job figure
+of bench.py is the work of all ranks over the slowest rank's time; one mesh
+split over two ranks (the exchange, and PartitionedPass itself with the CPU
+oracle standing in for the device pass) equals the whole-mesh pass bit for
+bit, and a failing step on one rank stops both ranks with SfxError instead
+of leaving one waiting in the exchange."""
 import os
 import socket
 
+import numpy as np
 import pytest
+import torch
 import torch.multiprocessing as mp
 
 
@@ -154,3 +159,142 @@ def test_split_mesh_over_two_cpu_ranks(name):
         assert np.array_equal(W, r["W"][cells])
         assert np.array_equal(Q, r["Q"][cells])
     assert np.all(seen == 1)
+
+
+class _OraclePass:
+    """FluxPass's interface over the CPU oracle, on CPU tensors: the device
+    pass's stand-in inside PartitionedPass on gloo ranks.  fail_at=k makes
+    the k-th step raise the library's SfxError (a failure made on the host)."""
+
+    def __init__(self, oracle, mesh, p, fail_at=None):
+        self.oracle, self.mesh, self.p, self.fail_at, self.k = oracle, mesh, p, fail_at, 0
+
+    def set_ranges(self, grad_cells, flux_faces, update_cells):
+        self.n_own = update_cells
+
+    def set_primitive(self, W):
+        self.W = np.array(W, np.float64)
+        self.Q = self.oracle.init_Q(self.mesh, self.p, self.W)
+
+    def step(self, dt, nsteps=1, stats=True):
+        from shadowfax_b200._lib import SFX_ERR_NEG_STATE, SfxError
+        for _ in range(nsteps):
+            self.k += 1
+            if self.k == self.fail_at:
+                raise SfxError(SFX_ERR_NEG_STATE, "sfx_step", 0)
+            _, dQ, _, rc, _ = self.oracle.flux_pass(self.mesh, self.p, dt, self.W, self.Q)
+            assert rc == 0
+            Qt = self.Q.copy()
+            Qt[self.n_own:, [0, -1]] = 1e300      # ring cells are not updated
+            Wn, Qn, rc, _ = self.oracle.apply(self.mesh, self.p, dQ, self.W, Qt)
+            assert rc == 0
+            n = self.n_own
+            self.W[:n], self.Q[:n] = Wn[:n], Qn[:n]
+
+    def pack_cells(self, idx, out):
+        i = idx.numpy()
+        out.copy_(torch.from_numpy(np.concatenate([self.W[i], self.Q[i, :1]], axis=1)))
+
+    def unpack_cells(self, idx, inp):
+        i = idx.numpy()
+        rec = inp.numpy()
+        self.W[i] = rec[:, :-1]
+        self.Q[i, 0] = rec[:, -1]
+
+    def state(self):
+        return self.W.copy(), self.Q.copy()
+
+
+def _partitioned_rank(rank, world, port, name, nsteps, fail_rank, out):
+    import datetime
+    import sys
+    import time
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    # a short timeout: a rank left waiting in the exchange ends with a
+    # timeout error, not with the SfxError the test expects
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=20))
+    try:
+        from golden_util import load_case
+        from oracle.oracle import Oracle, Params
+        from shadowfax_b200 import partition as P
+        from shadowfax_b200._lib import SfxError
+
+        mesh, meta, _ = load_case(name)
+        p = Params(solver=meta["solver"], gamma=meta["gamma"])
+        owner = P.partition(mesh, world)
+        part = P.build_part(mesh, owner, rank)
+        stub = _OraclePass(Oracle(), part.mesh, p, fail_at=2 if rank == fail_rank else None)
+        pp = P.PartitionedPass(None, mesh, owner, rank, flux_pass=stub)
+        pp.set_primitive(meta["W0"])
+        t0 = time.perf_counter()
+        try:
+            pp.step(meta["dt"], nsteps)
+            cells, W, Q = pp.owned_state()
+            out[rank] = ("ok", cells, W, Q, pp.comm_device.type)
+        except SfxError as e:
+            out[rank] = ("SfxError", e.status, time.perf_counter() - t0, stub.k)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_partitioned(name, nsteps, fail_rank):
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        procs = [ctx.Process(target=_partitioned_rank,
+                             args=(r, world, port, name, nsteps, fail_rank, out))
+                 for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(180)
+            assert p.exitcode == 0
+        return dict(out)
+
+
+@pytest.mark.parametrize("name", ["random2d_periodic_exact", "sedov3d_hllc"])
+def test_partitioned_pass_over_two_cpu_ranks(name):
+    """PartitionedPass itself (exchange lists, packing, the exchange, the
+    per-step status agreement) on two gloo ranks: the owned cells equal the
+    oracle's whole-mesh steps bit for bit"""
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from golden_util import load_case
+    from oracle.oracle import Oracle, Params
+
+    nsteps = 3
+    res = _run_partitioned(name, nsteps, fail_rank=-1)
+    mesh, meta, _ = load_case(name)
+    r = Oracle().run(mesh, Params(solver=meta["solver"], gamma=meta["gamma"]), meta["dt"],
+                     nsteps, meta["W0"])
+    seen = np.zeros(mesh.n_cells, int)
+    for rank in range(2):
+        kind, cells, W, Q, comm = res[rank]
+        assert kind == "ok" and comm == "cpu"
+        seen[cells] += 1
+        assert np.array_equal(W, r["W"][cells])
+        assert np.array_equal(Q, r["Q"][cells])
+    assert np.all(seen == 1)
+
+
+@pytest.mark.parametrize("fail_rank", [0, 1])
+def test_failing_step_on_one_rank_stops_both(fail_rank):
+    """the second step fails on one rank (SfxError from its pass): both ranks
+    raise SfxError with that status after the same step, well inside the
+    process group's timeout, and neither exchanges after the failure"""
+    from shadowfax_b200._lib import SFX_ERR_NEG_STATE
+    res = _run_partitioned("random2d_periodic_exact", 4, fail_rank)
+    for rank in range(2):
+        kind, status, secs, k = res[rank]
+        assert kind == "SfxError" and status == SFX_ERR_NEG_STATE
+        assert k == 2            # no rank ran a step after the failing one
+        assert secs < 15.0
