@@ -1,22 +1,27 @@
 """Benchmark of the B200 flux pass (one JSON line on rank 0).
 
-Default workload (--workload serve): the serving request stream -- Poisson
-arrivals at 200 requests/s (seed 5), 70% 2D / 30% 3D static Voronoi meshes
-(periodic unit box) with generator counts log-uniform in [1e3, 1e6] served
-from a pre-tessellated pool (10 log-size bins per dimension), random-field
-states, U{10..200} steps, exact or HLLC 50/50.  A "step" is one request; the
-default run takes the stream's first 400 arrivals (about 2 s of the 60 s
-stream; --duration 60 runs it whole).  The unit of work is the face-step
-(one nonzero-area face processed in one time step, with its share of the
-gradient and update work).
+Default workload (--workload serve): the serving request stream, whole --
+Poisson arrivals at 200 requests/s for 60 s (seed 5, 12,058 requests), 70%
+2D / 30% 3D static Voronoi meshes (periodic unit box) with generator counts
+log-uniform in [1e3, 1e6] served from a pre-tessellated pool (10 log-size
+bins per dimension), random-field states, U{10..200} steps, exact or HLLC
+50/50.  The unit of work is the face-step (one nonzero-area face processed
+in one time step, with its share of the gradient and update work).
 
-  value  the stream's requests with all states resident in HBM, co-batched
-         per (dimension, solver) class in launch groups, rounds of --chunk
-         steps, CUDA events on the device (FP32/FP64 split pass);
-  e2e    the same stream served by the request server (sfx_server_*) from
-         host memory at the arrival times: faces/s over the makespan, p50/p99
-         request latency; beside it the same stream served with the plain
-         FP64 pass one request at a time, and the split-vs-FP64 error.
+  value  the whole stream's requests with their states resident in HBM,
+         co-batched per (dimension, solver) class in launch groups, rounds
+         of --chunk steps, CUDA events on the device (FP32/FP64 split pass).
+         The requests form --steps consecutive segments of arrivals, one
+         bench step each (states loaded before each segment's timed region).
+  e2e    the whole stream served by the request server (sfx_server_*) from
+         host memory at the arrival times: face-steps of completed requests
+         over the makespan, p50/p99 request latency.
+  served_speedup_vs_fp64
+         e2e over the plain FP64 pass's served throughput on every
+         --fp64-every-th request (submitted at once, a saturated server;
+         the FP64 pass over the whole stream would take about 50 minutes),
+         with the per-field relative L1 and max error of the split results
+         against FP64 on those requests.
 
 Other workloads: --workload sedov3d (Sedov 3D blast, 262,144 generators,
 HLLC, one mesh; --precision fp64|split), --workload random3d (3D supersonic
@@ -31,12 +36,16 @@ Timing: CUDA events on the library's streams, barrier + synchronize on both
 sides, max over ranks; untimed warm-up before the timed region.  Working
 sets are larger than the 126 MB L2, so no separate L2 flush is done.
 
-N>1: every rank runs its own requests or meshes (independent units, no
-data-path collective): weak scaling.
+N>1 (serve): the GPUs share the one stream, whole requests each, assigned in
+arrival order to the GPU with the least face work so far (no data-path
+collective); value and e2e are all GPUs' face-steps over the slowest GPU's
+time.  Other workloads: every rank runs its own meshes (weak scaling).
 
 --impl reference times the reference's own CPU flux pass (the unmodified
 Shadowfax sources built into oracle/_ref) on the host cores: for the stream,
-one process per request on the first requests.
+one process per request on its first requests, each stepping its request
+--steps times; that process loads no GPU library (its meshes come from the
+standalone sfx_meshgen builder and a numpy reader).
 """
 from __future__ import annotations
 
@@ -68,8 +77,9 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (sedov3d 50, batch2d 20); serve: requests of the "
-                         "stream (default 400)")
+                    help="timed steps (sedov3d 50, batch2d 20); serve: the whole stream is "
+                         "timed, its resident replay in this many consecutive segments of "
+                         "arrivals (default 20), one step each")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
@@ -84,18 +94,20 @@ def parse():
                          "on one mesh; random3d: periodic 3D random field, exact solver; "
                          "batch2d: 1,024 2D meshes")
     ap.add_argument("--meshes", type=int, default=1024, help="batch2d: number of meshes")
-    ap.add_argument("--duration", type=float, default=None,
-                    help="serve: take every arrival of this many seconds of the stream "
-                         "instead of the first --steps requests (the whole stream is 60)")
+    ap.add_argument("--duration", type=float, default=60.0,
+                    help="serve: seconds of the stream (default: the whole 60 s)")
+    ap.add_argument("--requests", type=int, default=None,
+                    help="serve: only the stream's first N arrivals (quick runs)")
+    ap.add_argument("--fp64-every", type=int, default=48,
+                    help="serve: every N-th request is also served by the plain FP64 pass "
+                         "(0: none)")
     ap.add_argument("--chunk", type=int, default=4, help="serve: steps per scheduling round")
     ap.add_argument("--pool-dir", default=None,
                     help="serve: read the pool meshes from mesh files in this directory, "
                          "writing the ones not there yet (sfx_meshfile_*)")
-    ap.add_argument("--no-fp64-serve", action="store_true",
-                    help="serve: skip serving the stream with the plain FP64 pass")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = {"serve": 400, "sedov3d": 50, "random3d": 10, "batch2d": 20}[a.workload]
+        a.steps = {"serve": 20, "sedov3d": 50, "random3d": 10, "batch2d": 20}[a.workload]
     if a.n is None:
         a.n = {"random3d": 2_097_152}.get(a.workload, N_GEN)
     if a.solver is None:
@@ -279,7 +291,7 @@ def cpu_baseline(pr, steps: int = 3):
                       f"mesh, reference VorCell/VorFace/HLLC loops, 1 MPI rank (single thread)"}
 
 
-def cpu_baseline_many(probs, steps: int = 2):
+def cpu_baseline_many(probs, steps: int = 2, warmup: int = 1):
     """reference CPU pass on a sample of the batch: one mesh per process, as
     many processes as host cores, run concurrently (the reference has no
     threads; independent meshes are its best case)"""
@@ -292,19 +304,24 @@ def cpu_baseline_many(probs, steps: int = 2):
 
     def one(pr):
         p = Params(solver=pr.solver, gamma=pr.gamma, use_libm_pow=True)
-        r = run_reference(pr.mesh, p, pr.dt, steps + 1, pr.W0, pow_kind="libm")
-        return pr.mesh.n_active_faces * steps, float(np.sum(r["step_seconds"][1:]))
+        r = run_reference(pr.mesh, p, pr.dt, steps + warmup, pr.W0, pow_kind="libm")
+        # a request that fails inside the sample (the reference's exceptions)
+        # counts the steps it completed
+        done = min(int(r["steps"]), steps + warmup) - warmup
+        if done <= 0:
+            return 0, 0.0
+        return pr.mesh.n_active_faces * done, float(np.sum(r["step_seconds"][warmup:warmup + done]))
 
     with ThreadPoolExecutor(max_workers=P) as ex:
         res = list(ex.map(one, sample))
     # sum of the per-process rates: every core kept busy (the makespan of
     # unequal meshes would leave cores idle and understate the CPU)
-    value = sum(w / s for w, s in res)
+    value = sum(w / s for w, s in res if s > 0)
     return {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
             "sample": f"{len(sample)} meshes of the batch ({sum(p.mesh.n_cells for p in sample)} "
-                      f"cells), {steps} timed steps each, one reference process per mesh on "
-                      f"{P} host cores concurrently (P processes, not an MPI run; value = "
-                      f"sum of the per-process rates)"}
+                      f"cells), {warmup} warm-up + {steps} timed steps each, one reference "
+                      f"process per mesh on {P} host cores concurrently (P processes, not an "
+                      f"MPI run; value = sum of the per-process rates)"}
 
 
 def bench_batch(args, rank, world, local, torch):
@@ -437,13 +454,32 @@ SERVE_BUDGET = 150 << 30
 SERVE_CPU_PROCS = 48
 
 
-def serve_requests(args, rank):
-    """the request stream: first --steps arrivals, or --duration seconds"""
+def serve_requests(args):
+    """the request stream: every arrival of --duration seconds (default the
+    whole 60 s), or the first --requests arrivals (quick runs)"""
     from shadowfax_b200 import workloads as wl
-    seed = 5 + 1000 * rank
-    if args.duration:
-        return wl.serve_stream(duration=args.duration, seed=seed)
-    return wl.serve_stream(count=args.steps, seed=seed)
+    if args.requests:
+        return wl.serve_stream(count=args.requests, seed=5)
+    return wl.serve_stream(duration=args.duration, seed=5)
+
+
+def shard_requests(reqs, world: int, k: int = 10) -> np.ndarray:
+    """The rank serving each request of one stream shared by `world` GPUs:
+    whole requests, no data-path collective.  In arrival order each request
+    goes to the rank with the least face work assigned so far (the lowest
+    rank on ties), the face work of a request being its pool mesh's cells x
+    faces per cell (3 in 2D, 7.8 in 3D, Poisson-Voronoi averages) x its steps.
+    Every rank computes the same assignment from the stream alone."""
+    from shadowfax_b200 import workloads as wl
+    sizes = wl.serve_pool_sizes(k)
+    load = np.zeros(world)
+    owner = np.empty(len(reqs), np.int64)
+    for j, r in enumerate(reqs):
+        dim, n = 2 + r.mesh // k, float(sizes[r.mesh % k])
+        q = int(np.argmin(load))
+        owner[j] = q
+        load[q] += n * (3.0 if dim == 2 else 7.8) * r.nsteps
+    return owner
 
 
 def l1_rel_fields(a, b):
@@ -456,22 +492,35 @@ def l1_rel_fields(a, b):
     return np.array([e[0], e[1:D + 1].max(), e[D + 1]])
 
 
-def run_served(pool, reqs, precision, chunk, sample_every, device=0):
-    """serve the stream through the request server (C ABI, host states in
-    and out): submit each request at its arrival time from a feeder thread,
-    collect completions concurrently; returns per-request results (states
-    kept for every sample_every-th request), launches and server stats"""
+def max_rel_fields(a, b):
+    """largest per-cell error per conserved field relative to the field's
+    largest magnitude (momentum: the largest momentum magnitude)"""
+    D = b.shape[1] - 2
+    den = np.abs(b).max(0)
+    den[1:D + 1] = np.sqrt((b[:, 1:D + 1] ** 2).sum(1)).max()
+    e = np.abs(a - b).max(0) / np.maximum(den, 1e-300)
+    return np.array([e[0], e[1:D + 1].max(), e[D + 1]])
+
+
+def run_served(pool, reqs, precision, chunk, keep_states=False, device=0, at_once=False):
+    """serve requests through the request server (C ABI, host states in and
+    out): submitted at their arrival times from a feeder thread (at_once:
+    all at time 0, a saturated server), completions collected concurrently;
+    returns per-request results (with states when keep_states), launches and
+    server stats"""
     from shadowfax_b200 import _lib as L
     from shadowfax_b200.serve import Server
     srv = Server(precision=precision, memory_budget=SERVE_BUDGET, chunk_steps=chunk,
                  device=device)
     try:
         ids = {j: srv.add_mesh(m) for j, m in enumerate(pool.meshes) if m is not None}
-        # warm-up: a short request per class on the smallest meshes
+        # warm-up: a short request per class on the smallest meshes present
         warm = []
-        for j0 in (0, pool.k):
+        for d in (2, 3):
+            js = [j for j in ids if (j >= pool.k) == (d == 3)]
             for solver in ("Exact", "HLLC"):
-                if j0 in ids:
+                if js:
+                    j0 = min(js)
                     warm.append(srv.submit(ids[j0], pool.states[j0][0], solver,
                                            pool.dts[j0][0], 3))
         srv.drain(600.0)
@@ -486,7 +535,7 @@ def run_served(pool, reqs, precision, chunk, sample_every, device=0):
         def feeder():
             for j, r in enumerate(reqs):
                 delay = t_base + r.t - time.perf_counter()
-                if delay > 0:
+                if delay > 0 and not at_once:
                     time.sleep(delay)
                 rid = srv.submit(ids[r.mesh], pool.states[r.mesh][r.state], r.solver,
                                  pool.dts[r.mesh][r.state], r.nsteps)
@@ -511,7 +560,7 @@ def run_served(pool, reqs, precision, chunk, sample_every, device=0):
                 with lock:
                     items = list(pending.items())
                 for rid, j in items:
-                    res = srv.poll(rid, want_state=(j % sample_every == 0))
+                    res = srv.poll(rid, want_state=keep_states)
                     if res is not None:
                         results[j] = res
                         with lock:
@@ -525,7 +574,7 @@ def run_served(pool, reqs, precision, chunk, sample_every, device=0):
     return [results[j] for j in range(len(reqs))], launches, st
 
 
-def served_summary(res, reqs, st=None):
+def served_summary(res, st=None):
     ok = [r for r in res if r.status == 0]
     lat = np.array([r.t_done - r.t_submit for r in ok]) if ok else np.zeros(1)
     t0 = min(r.t_submit for r in res)
@@ -542,13 +591,32 @@ def served_summary(res, reqs, st=None):
             if st is not None else None}
 
 
-def run_resident(pool, reqs, chunk, torch, local):
-    """the stream's requests with every state resident in HBM before the
-    timed region: requests co-batched per (dimension, solver) class, one
-    launch group per class on its own stream, rounds of `chunk` steps with
-    device step counters and the finished requests dropped between rounds
-    (the server's schedule without arrivals and host transfers).  Waves of
-    requests fit the 150 GB budget.  Returns (face_steps, ms, roofline)."""
+def _budget_waves(idx, nbytes):
+    """consecutive runs of requests whose instances fit the device budget"""
+    waves, cur, used = [], [], 0
+    for j in idx:
+        b = nbytes(j)
+        if cur and used + b > SERVE_BUDGET:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += b
+    if cur:
+        waves.append(cur)
+    return waves
+
+
+def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
+    """The requests with every state resident in HBM before each timed
+    region, co-batched per (dimension, solver) class: one launch group per
+    class on its own stream, rounds of `chunk` steps with device step
+    counters, finished requests dropped between rounds (the server's
+    schedule without arrivals and host transfers).  The requests, in arrival
+    order, form `nseg` consecutive segments, one bench step each; a segment
+    larger than the 150 GB budget runs in waves.  Before the first timed
+    segment: the per-kernel roofline on the first wave and `warmup` untimed
+    rounds of every class, then the states are loaded again.  Returns a dict
+    (face_steps, ms, segment_ms, launches, roofline, waves, failed)."""
     from shadowfax_b200 import _lib as L
     from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
     pool_ctx = {d: Context(d, RiemannSolverFactory.generate("HLLC"), L.PREC_SPLIT, device=local)
@@ -561,98 +629,106 @@ def run_resident(pool, reqs, chunk, torch, local):
         cstream[c] = torch.cuda.Stream(device=local)
         cctx[c].set_stream(cstream[c].cuda_stream)
     main = torch.cuda.current_stream(local)
-    # waves under the budget, in arrival order
-    waves, cur, used = [], [], 0
-    for j, r in enumerate(reqs):
-        b = bases[r.mesh].clone_bytes(L.PREC_SPLIT)
-        if cur and used + b > SERVE_BUDGET:
-            waves.append(cur)
-            cur, used = [], 0
-        cur.append(j)
-        used += b
-    if cur:
-        waves.append(cur)
-    total_ms, face_steps, launches, roof = 0.0, 0, 0, None
+    segments = [s for s in np.array_split(np.arange(len(reqs)), nseg) if len(s)]
+    nbytes = lambda j: bases[reqs[j].mesh].clone_bytes(L.PREC_SPLIT)  # noqa: E731
+    seg_ms, face_steps, launches, roof, nwaves = [], 0, 0, None, 0
     failed = set()
-    for w, wave in enumerate(waves):
-        inst = {}
-        for j in wave:
-            r = reqs[j]
-            c = (pool.meshes[r.mesh].dim, r.solver)
-            fp = bases[r.mesh].clone(cctx[c])
-            fp.set_primitive(pool.states[r.mesh][r.state])
-            inst[j] = (c, fp)
-        if w == 0:
-            roof = resident_roofline(pool, reqs, inst, classes, cctx)
-            for j, (c, fp) in inst.items():      # back to the initial states
-                fp.set_primitive(pool.states[reqs[j].mesh][reqs[j].state])
-        torch.cuda.synchronize()
-        live = {c: [j for j in wave if inst[j][0] == c] for c in classes}
-        left = {j: reqs[j].nsteps for j in wave}
-        groups = {c: None for c in classes}
-        reused = {c: 0 for c in classes}
-        n0 = L.lib().sfx_launch_count()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.nvtx.range_push("resident")  # the timed region, for profilers
-        e0.record(main)
-        for c in classes:
-            cstream[c].wait_event(e0)
-        while any(live.values()):
+    first = True
+    for seg in segments:
+        ms_seg = 0.0
+        for wave in _budget_waves(seg, nbytes):
+            nwaves += 1
+            inst = {}
+            for j in wave:
+                r = reqs[j]
+                c = (pool.meshes[r.mesh].dim, r.solver)
+                fp = bases[r.mesh].clone(cctx[c])
+                fp.set_primitive(pool.states[r.mesh][r.state])
+                inst[j] = (c, fp)
+            if first:
+                roof = resident_roofline(pool, reqs, inst, classes, cctx)
+                for c in classes:
+                    js = [j for j in wave if inst[j][0] == c]
+                    if js and warmup:
+                        g = Group(cctx[c], [inst[j][1] for j in js],
+                                  [pool.dts[reqs[j].mesh][reqs[j].state] for j in js])
+                        for _ in range(warmup):
+                            g.step(chunk, graph=False, status=False)
+                        g.close()
+                torch.cuda.synchronize()
+                for j, (c, fp) in inst.items():      # back to the initial states
+                    fp.set_primitive(pool.states[reqs[j].mesh][reqs[j].state])
+                first = False
+            torch.cuda.synchronize()
+            live = {c: [j for j in wave if inst[j][0] == c] for c in classes}
+            left = {j: reqs[j].nsteps for j in wave}
+            groups = {c: None for c in classes}
+            reused = {c: 0 for c in classes}
+            n0 = L.lib().sfx_launch_count()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("resident")  # the timed region, for profilers
+            e0.record(main)
             for c in classes:
-                if groups[c] is None and live[c]:
-                    groups[c] = Group(cctx[c], [inst[j][1] for j in live[c]],
-                                      [pool.dts[reqs[j].mesh][reqs[j].state] for j in live[c]])
-                    groups[c].set_steps([left[j] for j in live[c]])
-                    reused[c] = 0
+                cstream[c].wait_event(e0)
+            while any(live.values()):
+                for c in classes:
+                    if groups[c] is None and live[c]:
+                        groups[c] = Group(cctx[c], [inst[j][1] for j in live[c]],
+                                          [pool.dts[reqs[j].mesh][reqs[j].state]
+                                           for j in live[c]])
+                        groups[c].set_steps([left[j] for j in live[c]])
+                        reused[c] = 0
+                for c in classes:
+                    if groups[c] is not None:
+                        groups[c].step(chunk, graph=reused[c] > 0, status=False)
+                for c in classes:
+                    g = groups[c]
+                    if g is None:
+                        continue
+                    steps_left = g.get_steps()
+                    st = g.status()
+                    for j, k, e in zip(live[c], steps_left, st):
+                        left[j] = 0 if e else int(k)
+                        if e:
+                            failed.add(j)
+                    keep = [j for j in live[c] if left[j] > 0]
+                    if len(keep) != len(live[c]):
+                        g.close()
+                        groups[c] = None
+                        live[c] = keep
+                    else:
+                        reused[c] += 1
+            for c in classes:
+                ev = torch.cuda.Event()
+                ev.record(cstream[c])
+                main.wait_event(ev)
+            e1.record(main)
+            torch.cuda.nvtx.range_pop()
+            torch.cuda.synchronize()
+            ms_seg += e0.elapsed_time(e1)
+            launches += L.lib().sfx_launch_count() - n0
+            face_steps += sum(pool.meshes[reqs[j].mesh].n_active_faces * reqs[j].nsteps
+                              for j in wave if j not in failed)
             for c in classes:
                 if groups[c] is not None:
-                    groups[c].step(chunk, graph=reused[c] > 0, status=False)
-            for c in classes:
-                g = groups[c]
-                if g is None:
-                    continue
-                steps_left = g.get_steps()
-                st = g.status()
-                for j, k, e in zip(live[c], steps_left, st):
-                    left[j] = 0 if e else int(k)
-                    if e:
-                        failed.add(j)
-                keep = [j for j in live[c] if left[j] > 0]
-                if len(keep) != len(live[c]):
-                    g.close()
-                    groups[c] = None
-                    live[c] = keep
-                else:
-                    reused[c] += 1
-        for c in classes:
-            ev = torch.cuda.Event()
-            ev.record(cstream[c])
-            main.wait_event(ev)
-        e1.record(main)
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        launches += L.lib().sfx_launch_count() - n0
-        face_steps += sum(pool.meshes[reqs[j].mesh].n_active_faces * reqs[j].nsteps
-                          for j in wave if j not in failed)
-        for c in classes:
-            if groups[c] is not None:
-                groups[c].close()
-        for c, fp in inst.values():
-            fp.close()
+                    groups[c].close()
+            for c, fp in inst.values():
+                fp.close()
+        seg_ms.append(ms_seg)
     for fp in bases.values():
         fp.close()
     for c in classes:
         cctx[c].close()
     for c in pool_ctx.values():
         c.close()
-    return face_steps, total_ms, launches, roof, len(waves), len(failed)
+    return {"face_steps": face_steps, "ms": float(sum(seg_ms)), "segment_ms": seg_ms,
+            "launches": launches, "roofline": roof, "waves": nwaves, "failed": len(failed)}
 
 
-# DRAM bytes (read + write) per face of one launch, from the ncu capture of a
-# 300,000-cell periodic random-field mesh (2,396,113 faces) in
-# profiles/split_kernels_random3d.md; the gathers and the per-face records
+# DRAM bytes (read + write) per face of one launch, from one-kernel ncu
+# captures of a 300,000-cell periodic random-field mesh (3D, 2,396,113 faces)
+# and of a 300,000-cell periodic 2D mesh; the gathers and the per-face records
 # scale with the faces, so a launch over F faces moves about F times these
 TRAFFIC_B_PER_FACE = {("k_group_sfaces", 3, "Exact"): 106.1, ("k_group_sfaces", 3, "HLLC"): 104.3,
                       ("k_group_sgrad", 3): 59.4, ("k_group_sapply", 3): 53.0}
@@ -709,14 +785,14 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
             "class": f"{D}D {top_c[1]}, {pc['requests']} requests, {pc['faces']} faces",
             "achieved": pc["achieved_gbs"][top], "peak": peak, "unit": "GB/s",
             "frac": pc["achieved_gbs"][top] / peak, "traffic": traffic,
-            "traffic_note": "bytes per face from the ncu capture of a 300k-cell mesh "
-                            "(profiles/split_kernels_random3d.md) x faces of this launch",
+            "traffic_note": "DRAM bytes per face from a one-kernel ncu capture of a "
+                            "300,000-cell mesh of the same dimension and solver, times the "
+                            "faces of this launch",
             "peak_source": f"hbm_gbs {peak_kind} (of measured)",
             "algorithmic_bytes_per_launch": pc["algorithmic_bytes"][top],
             "kernel_ms": kms,
             "note": "the exact-solver face kernel is bound by instruction issue and FP64 "
-                    "latency (divergent solver paths), not by HBM; its pipe utilisation is "
-                    "in profiles/",
+                    "latency (divergent solver paths), not by HBM",
             "step_bytes_per_face": STEP_BYTES[("split", D)],
             "step_frac": pc["step_frac"],
             "classes": {f"{c[0]}D {c[1]}": v for c, v in per_class.items()}}
@@ -728,9 +804,9 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
     return roof
 
 
-def serve_cpu_sample(pool, reqs, steps: int = 2):
+def serve_cpu_sample(pool, reqs, steps: int = 2, warmup: int = 1):
     """the reference CPU pass on the stream's first P requests (P = host
-    cores), one process per request, concurrently"""
+    cores, at most 48), one process per request, concurrently"""
     from shadowfax_b200.workloads import Problem
     P = min(os.cpu_count() or 1, SERVE_CPU_PROCS)
     probs = []
@@ -738,125 +814,173 @@ def serve_cpu_sample(pool, reqs, steps: int = 2):
         m = pool.meshes[r.mesh]
         probs.append(Problem(f"req{len(probs)}", m, pool.states[r.mesh][r.state], r.solver,
                              pool.dts[r.mesh][r.state], steps))
-    cb = cpu_baseline_many(probs, steps)
+    cb = cpu_baseline_many(probs, steps, warmup)
     if cb is not None:
         cb["sample"] = (f"the stream's first {len(probs)} requests ({sum(p.mesh.n_cells for p in probs)}"
-                        f" cells, both solvers, 2D and 3D), {steps} timed steps each, one "
-                        f"reference process per request on {P} host cores concurrently "
-                        f"(P processes, not an MPI run; value = sum of the per-process rates)")
+                        f" cells, both solvers, 2D and 3D), {warmup} warm-up + {steps} timed "
+                        f"steps each, one reference process per request on {len(probs)} host cores "
+                        f"concurrently (P processes, not an MPI run; value = sum of the "
+                        f"per-process rates)")
     return cb
 
 
+def serve_config(args, reqs, world):
+    """the workload description both arms print (no GPU or pool needed)"""
+    from shadowfax_b200 import workloads as wl
+    n2 = sum(1 for r in reqs if r.mesh < 10)
+    whole = not args.requests and args.duration >= 60.0
+    span = "the whole 60 s stream" if whole else f"{reqs[-1].t:.1f} s of the 60 s stream"
+    return {"workload": f"serve: request stream of {len(reqs)} Poisson arrivals at 200/s "
+                        f"({span}, seed 5), {n2} 2D / {len(reqs) - n2} 3D periodic static "
+                        f"meshes, N log-uniform in [1e3, 1e6] from a pool of 20 pre-tessellated "
+                        f"meshes (10 log bins per dimension), random-field states, steps "
+                        f"U{{10..200}}, exact/HLLC 50/50, gamma 5/3, 150 GB device budget",
+            "step": f"one of {args.steps} consecutive segments of the stream's arrivals",
+            "l2": "working set > L2 (no flush)",
+            "parallelism": (f"{world} GPUs, whole requests per GPU by least face work"
+                            if world > 1 else "1 GPU"),
+            "pool_sizes": [int(x) for x in wl.serve_pool_sizes()]}
+
+
 def bench_serve(args, rank, world, local, torch):
-    """the request stream served by the continuous-batching server
-    (FP32/FP64 split, co-batched) against the same stream served with the
-    plain FP64 pass one request at a time"""
+    """The request stream on this rank's GPU: the resident replay (value),
+    the stream served from host memory at its arrival times (e2e, p50/p99),
+    and a sample of it served by the plain FP64 pass and by the split pass
+    with every request submitted at once (the split-vs-FP64 throughput ratio
+    of a saturated server, and the accuracy of the split results)."""
     from shadowfax_b200 import _lib as L
     from shadowfax_b200 import workloads as wl
-    reqs = serve_requests(args, rank)
+    all_reqs = serve_requests(args)
+    owner = shard_requests(all_reqs, world)
+    reqs = [r for r, o in zip(all_reqs, owner) if o == rank]
     t_build = time.time()
-    used = sorted({r.mesh for r in reqs})
+    used = sorted({r.mesh for r in all_reqs})
     pool = wl.serve_pool(only=set(used), cache_dir=args.pool_dir)
     t_build = time.time() - t_build
-    sample_every = max(1, len(reqs) // 24)
+    offered = sum(pool.meshes[r.mesh].n_active_faces * r.nsteps for r in all_reqs)
+    log = (lambda *a: print(*a, file=sys.stderr, flush=True)) if rank == 0 else (lambda *a: None)
+    log(f"[bench] {len(all_reqs)} requests, {offered:.3e} face-steps offered; pool "
+        f"{t_build:.0f} s")
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     with ClockSampler(local) as clk:
         clk.wait_first_sample()
         clk.mark("t0")
-        # resident (device-timed) throughput and the roofline
-        fs, ms, launches_res, roof, nwaves, nfail_res = run_resident(pool, reqs, args.chunk,
-                                                                     torch, local)
-        # the same stream served from host memory
-        res32, launches, st32 = run_served(pool, reqs, L.PREC_SPLIT, args.chunk,
-                                           sample_every, local)
+        t0 = time.time()
+        res = run_resident(pool, reqs, args.steps, args.warmup, args.chunk, torch, local)
+        log(f"[bench] resident {res['face_steps'] / res['ms'] * 1e3:.3e} face-steps/s "
+            f"({time.time() - t0:.0f} s)")
+        t0 = time.time()
+        res32, launches, st32 = run_served(pool, reqs, L.PREC_SPLIT, args.chunk, False, local)
         clk.mark("t1")
+        log(f"[bench] served ({time.time() - t0:.0f} s)")
         time.sleep(0.3)
-    # the same stream served with the plain FP64 pass, the comparison of the
-    # headline (one GPU only: it takes ~15x the split run's time, and the
-    # multi-GPU runs report the whole-job figures alone)
-    fp64_serve = world == 1 and not args.no_fp64_serve
-    res64, st64 = None, None
-    if fp64_serve:
-        res64, _, st64 = run_served(pool, reqs, L.PREC_FP64, args.chunk, sample_every, local)
-    split = served_summary(res32, reqs, st32)
-    fp64 = served_summary(res64, reqs, st64) if fp64_serve else None
-    # the whole job's served figure: all ranks' face-steps over the longest makespan
+    split = served_summary(res32, st32)
     e2e_value, _, _ = reduce_over_ranks(1e3 * split["makespan_s"], split["face_steps"],
                                         f"cuda:{local}", world)
-    # accuracy and conservation on the sampled requests
-    errs, drift = [], []
-    for j in (range(0, len(reqs), sample_every) if fp64_serve else ()):
-        a, b = res32[j], res64[j]
-        if a.status or b.status:
-            continue
-        errs.append(l1_rel_fields(a.Q, b.Q))
-        m = pool.meshes[reqs[j].mesh]
-        W0 = pool.states[reqs[j].mesh][reqs[j].state]
-        D = m.dim
-        V = m.cell_volume
-        mass0 = float((W0[:, 0] * V).sum())
-        e0 = float(((W0[:, D + 1] / (wl.GAMMA - 1) + 0.5 * W0[:, 0] *
-                     (W0[:, 1:D + 1] ** 2).sum(1)) * V).sum())
-        drift.append([abs(a.Q[:, 0].sum() - mass0) / mass0,
-                      abs(a.Q[:, D + 1].sum() - e0) / e0,
-                      abs(b.Q[:, 0].sum() - mass0) / mass0,
-                      abs(b.Q[:, D + 1].sum() - e0) / e0])
-    errs = [float(v) for v in np.max(errs, 0)] if errs else [None] * 3
-    drift = [float(v) for v in np.max(drift, 0)] if drift else [None] * 4
-    value, ms_max, _ = reduce_over_ranks(ms, fs, f"cuda:{local}", world)
+    # a sample served by both passes, every request submitted at once
+    sub = reqs[::args.fp64_every] if args.fp64_every > 0 else []
+    fp64s = splits = None
+    errs, maxe, drift = [], [], []
+    if sub:
+        t0 = time.time()
+        res64, _, st64 = run_served(pool, sub, L.PREC_FP64, args.chunk, True, local, at_once=True)
+        sub32, _, sts = run_served(pool, sub, L.PREC_SPLIT, args.chunk, True, local, at_once=True)
+        log(f"[bench] fp64 sample {len(sub)} requests ({time.time() - t0:.0f} s)")
+        fp64s, splits = served_summary(res64, st64), served_summary(sub32, sts)
+        for j, (a, b) in enumerate(zip(sub32, res64)):
+            if a.status or b.status:
+                continue
+            errs.append(l1_rel_fields(a.Q, b.Q))
+            maxe.append(max_rel_fields(a.Q, b.Q))
+            m = pool.meshes[sub[j].mesh]
+            W0 = pool.states[sub[j].mesh][sub[j].state]
+            D = m.dim
+            V = m.cell_volume
+            mass0 = float((W0[:, 0] * V).sum())
+            en0 = float(((W0[:, D + 1] / (wl.GAMMA - 1) + 0.5 * W0[:, 0] *
+                          (W0[:, 1:D + 1] ** 2).sum(1)) * V).sum())
+            drift.append([abs(a.Q[:, 0].sum() - mass0) / mass0,
+                          abs(a.Q[:, D + 1].sum() - en0) / en0,
+                          abs(b.Q[:, 0].sum() - mass0) / mass0,
+                          abs(b.Q[:, D + 1].sum() - en0) / en0])
+    fp64_val, _, _ = reduce_over_ranks(1e3 * (fp64s["makespan_s"] if fp64s else 1.0),
+                                       fp64s["face_steps"] if fp64s else 0, f"cuda:{local}", world)
+    split_sub_val, _, _ = reduce_over_ranks(1e3 * (splits["makespan_s"] if splits else 1.0),
+                                            splits["face_steps"] if splits else 0,
+                                            f"cuda:{local}", world)
+    # every rank's worst error (MAX over ranks of the per-field maxima)
+    ev = torch.tensor([*(np.max(errs, 0) if errs else [-1.0] * 3),
+                       *(np.max(maxe, 0) if maxe else [-1.0] * 3),
+                       *(np.max(drift, 0) if drift else [-1.0] * 4)],
+                      dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        torch.distributed.all_reduce(ev, op=torch.distributed.ReduceOp.MAX)
+    ev = [float(x) if x >= 0 else None for x in ev.tolist()]
+    value, ms_max, fs_total = reduce_over_ranks(res["ms"], res["face_steps"], f"cuda:{local}",
+                                                world)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = serve_cpu_sample(pool, reqs)
+        cb = serve_cpu_sample(pool, all_reqs)
     h2d = sum(pool.states[r.mesh][r.state].nbytes for r in reqs)
     d2h = 2 * h2d
-    n2 = sum(1 for r in reqs if r.mesh < pool.k)
-    line = None
-    if rank == 0:
-        line = {
-            "metric": METRIC_SERVE, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": len(reqs), "warmup": args.warmup,
-            "ms_per_step": ms_max / len(reqs),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": f"serve: request stream, {len(reqs)} Poisson arrivals "
-                                   f"at 200/s (seed 5; {'%.1f s' % reqs[-1].t} of the 60 s stream), "
-                                   f"{n2} 2D / {len(reqs) - n2} 3D, N log-uniform in [1e3, 1e6] "
-                                   f"from a pool of {len(used)} periodic meshes (10 log bins per "
-                                   f"dimension), random-field states, steps U{{10..200}}, "
-                                   f"exact/HLLC 50/50, 150 GB budget",
-                       "step": "one request of the stream",
-                       "precision": "split (FP32 reconstruction/HLLC/p* Newton, FP64 final "
-                                    "p* step and accumulation)",
-                       "chunk_steps": args.chunk, "resident_waves": nwaves,
-                       "resident_failed_requests": nfail_res,
-                       "l2": "working set > L2 (no flush)",
-                       "parallelism": f"replicas x{world}",
-                       "pool_build_s": round(t_build, 1)},
-            "clocks": clk.summary(),
-            "served": split,
-            "served_fp64_per_request": fp64,
-            "served_speedup_vs_fp64": split["value"] / fp64["value"] if fp64 else None,
-            "split_vs_fp64_max_rel_l1": {"mass": errs[0], "momentum": errs[1],
-                                         "energy": errs[2],
-                                         "sample": f"every {sample_every}th request"},
-            "conservation_max_rel_drift": {
-                "split": {"mass": drift[0], "energy": drift[1]},
-                "fp64": {"mass": drift[2], "energy": drift[3]},
-                "note": "energy changes where get_W floors the pressure at 1e-30 and "
-                        "rewrites the energy (the reference algorithm does the same)"},
-            "roofline": roof,
-            "cpu_baseline": cb,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / len(reqs),
-                    "d2h_bytes_per_step": d2h / len(reqs),
-                    "note": "served stream: request states from host memory, results to host "
-                            "memory, makespan from first arrival to last completion"},
-            "p50_latency_s": split["p50_latency_s"], "p99_latency_s": split["p99_latency_s"],
-            "gpu_launches": int(launches_res),
-            "gpu_launches_served": int(launches),
-        }
-    return line
+    if rank != 0:
+        return None
+    cfg = serve_config(args, all_reqs, world)
+    fields = ("mass", "momentum", "energy")
+    speedup = e2e_value / fp64_val if fp64s and fp64_val > 0 else None
+    return {
+        "metric": METRIC_SERVE, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+        "config": cfg,
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps,
+                "note": "the whole stream served by the request server at its arrival "
+                        "times: request states from host memory, results (W and Q) to host "
+                        "memory, completed face-steps over the makespan (first arrival to "
+                        "last completion)"},
+        "served_speedup_vs_fp64": speedup,
+        "served_speedup_vs_fp64_same_sample": (split_sub_val / fp64_val
+                                               if fp64s and fp64_val > 0 else None),
+        "p50_latency_s": split["p50_latency_s"], "p99_latency_s": split["p99_latency_s"],
+        "split_vs_fp64_error": {
+            "rel_l1": dict(zip(fields, ev[0:3])), "max_rel": dict(zip(fields, ev[3:6])),
+            "requests": len(errs),
+            "sample": f"every {args.fp64_every}th request of the stream, run to completion "
+                      f"by both passes; max over requests; max_rel = largest cell error / "
+                      f"largest magnitude of the field"},
+        "fp64_served": {"value": fp64_val, "unit": UNIT,
+                        "sample": f"every {args.fp64_every}th request ({len(sub)} on rank 0), "
+                                  f"all submitted at once to a plain-FP64 server (each request "
+                                  f"stepped with its own launches)",
+                        "detail": fp64s},
+        "split_served_same_sample": {"value": split_sub_val, "unit": UNIT, "detail": splits},
+        "conservation_max_rel_drift": {
+            "split": {"mass": ev[6], "energy": ev[7]},
+            "fp64": {"mass": ev[8], "energy": ev[9]},
+            "note": "energy changes where get_W floors the pressure at 1e-30 and "
+                    "rewrites the energy (the reference algorithm does the same)"},
+        "served": split,
+        "resident": {"face_steps": int(fs_total), "ms": ms_max, "waves": res["waves"],
+                     "failed_requests": res["failed"],
+                     "segment_ms": [round(x, 3) for x in res["segment_ms"]],
+                     "chunk_steps": args.chunk,
+                     "note": "value: states resident in HBM, co-batched per (dimension, "
+                             "solver) class in launch groups, CUDA events per segment"},
+        "roofline": res["roofline"],
+        "cpu_baseline": cb,
+        "gpu_launches": int(res["launches"]),
+        "gpu_launches_served": int(launches),
+        "pool_build_s": round(t_build, 1),
+        "face_steps_offered": int(offered),
+        "precision": "split: FP32 gradients/reconstruction/HLLC/p* Newton, FP64 final p* "
+                     "step, exact-solver sampling, accumulation and get_W",
+    }
 
 
 def flux_error_by_branch(pr, device):
@@ -933,30 +1057,38 @@ def run_reference_arm(args, rank, world):
 
 
 def run_reference_serve(args):
-    """--impl reference on the request stream: the reference CPU pass, one
-    process per request on all host cores, for the stream's first requests
-    (a bounded sample per step; the reference has no request loop)"""
+    """--impl reference on the request stream: the reference CPU pass
+    (oracle/_ref, the unmodified Shadowfax sources) on the host cores, one
+    process per request for the stream's first P requests, each process
+    --warmup untimed and --steps timed steps (a bounded sample: the reference
+    has no request loop).  The meshes are made by the standalone sfx_meshgen
+    program and read with numpy, so this process never loads the GPU library."""
     from oracle.oracle import ref_binary
     from shadowfax_b200 import workloads as wl
     if not (ref_binary(2, "libm").exists() and ref_binary(3, "libm").exists()):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref reference harness not built (needs the reference tree)"}))
         return
-    reqs = serve_requests(args, 0)
+    reqs = serve_requests(args)
     P = min(os.cpu_count() or 1, SERVE_CPU_PROCS)
-    pool = wl.serve_pool(only={r.mesh for r in reqs[:P]}, cache_dir=args.pool_dir)
-    steps = max(1, min(args.steps, 2))
-    cb = serve_cpu_sample(pool, reqs, steps)
+    with tempfile.TemporaryDirectory() as td:
+        pool = wl.serve_pool(only={r.mesh for r in reqs[:P]}, cache_dir=args.pool_dir or td,
+                             library=False)
+        cb = serve_cpu_sample(pool, reqs, args.steps, args.warmup)
     faces = sum(pool.meshes[r.mesh].n_active_faces for r in reqs[:P])
     line = {"metric": METRIC_SERVE, "value": cb["value"], "unit": UNIT, "n_gpus": 1,
-            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * faces / cb["value"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * faces / cb["value"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "serve: request stream (first requests, one "
-                                   "reference process each)", "precision": "fp64"},
+            "config": serve_config(args, reqs, 1),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU flux pass on a bounded sample of the stream (its first "
+                    "requests, one process each, every process stepping its request --steps "
+                    "times); the meshes come from the standalone face-list builder "
+                    "(sfx_meshgen), the same face lists the GPU pass gets"}
     print(json.dumps(line))
 
 

@@ -10,8 +10,10 @@
 * ``csrc/sfx_meshfile.cpp`` versioned binary mesh files
 
 with ``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo`` into
-``shadowfax_b200/libsfxflux.so``.  nvcc cross-compiles, so this runs on a
-machine without a GPU.  A source newer than the library triggers a rebuild.
+``shadowfax_b200/libsfxflux.so``, and the host-only mesh-file generator
+``shadowfax_b200/sfx_meshgen`` (``csrc/sfx_meshgen.cpp`` with the builder and
+mesh-file sources, g++ only).  nvcc cross-compiles, so this runs on a
+machine without a GPU.  A source newer than a target triggers its rebuild.
 """
 from __future__ import annotations
 
@@ -24,6 +26,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libsfxflux.so"
+MESHGEN = PKG / "sfx_meshgen"
+MESHGEN_SRC = ["sfx_meshgen.cpp", "sfx_voronoi.cpp", "sfx_meshfile.cpp"]
 OBJ = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,7 +77,21 @@ def _compile(src: Path) -> Path:
     return obj
 
 
+def build_meshgen(force: bool = False) -> Path:
+    srcs = [CSRC / s for s in MESHGEN_SRC]
+    deps = srcs + [PKG.parent / "include" / "sfxflux.h", Path(__file__)]
+    if not force and MESHGEN.exists() and all(MESHGEN.stat().st_mtime >= d.stat().st_mtime
+                                              for d in deps):
+        return MESHGEN
+    tmp = MESHGEN.with_suffix(".tmp")
+    subprocess.run(["g++", "-std=c++17", "-O3", "-ffp-contract=off", "-pthread", "-I",
+                    str(PKG.parent / "include"), *map(str, srcs), "-o", str(tmp)], check=True)
+    os.replace(tmp, MESHGEN)
+    return MESHGEN
+
+
 def build_library(force: bool = False, verbose: bool = True) -> Path:
+    build_meshgen(force)
     if not force and not needs_build():
         return LIB
     srcs = _sources()

@@ -13,12 +13,21 @@ reflective mirror) and the right generator's position.
 from __future__ import annotations
 
 import ctypes as C
+import os
+import struct
+import subprocess
+import tempfile
 from dataclasses import dataclass, field
 from pathlib import Path
 
 import numpy as np
 
 from . import _lib as L
+
+# mesh file header and section entry (sfx_meshfile.cpp)
+_MESHFILE_HEADER = struct.Struct("<8sIIIIqqqIIQQQ48x")
+_MESHFILE_ENTRY = struct.Struct("<IIQQ")
+MESHGEN = Path(__file__).resolve().parent / "sfx_meshgen"
 
 
 @dataclass
@@ -134,6 +143,52 @@ class Mesh:
             L.dptr(m.face_velocity) if vel.value else None), "sfx_meshfile_read")
         return m
 
+    @classmethod
+    def read_file_numpy(cls, path: str | Path, verify_checksum: bool = False) -> "Mesh":
+        """a mesh file read with numpy alone (no GPU library loaded), for
+        CPU-only jobs: the same structural checks as sfx_meshfile_read
+        (magic, major version, section table inside the file, cell face
+        offsets covering the face list); the FNV-1a payload checksum only
+        with verify_checksum (a byte-serial hash, slow in Python)"""
+        raw = np.memmap(path, dtype=np.uint8, mode="r")
+        head = _MESHFILE_HEADER.unpack_from(raw, 0)
+        (magic, major, hbytes, dim, flags, n, nf, nnz, nsec, _minor, poff, pbytes,
+         csum) = head
+        if (magic != b"SFXMESH\0" or major == 0 or major > 1 or hbytes != 128
+                or dim not in (2, 3) or min(n, nf, nnz) < 0 or nsec > 64
+                or poff > raw.size or pbytes > raw.size - poff):
+            raise ValueError(f"{path}: not a readable mesh file")
+        if verify_checksum:
+            h = 1469598103934665603
+            for x in bytes(raw[poff:poff + pbytes]):
+                h = ((h ^ x) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+            if h != csum:
+                raise ValueError(f"{path}: checksum mismatch")
+        secs = {}
+        for i in range(nsec):
+            sid, eb, cnt, off = _MESHFILE_ENTRY.unpack_from(raw, 128 + i * _MESHFILE_ENTRY.size)
+            if eb not in (4, 8) or off < poff or off + cnt * eb > poff + pbytes:
+                raise ValueError(f"{path}: section {sid} outside the payload")
+            secs[sid] = np.array(np.frombuffer(raw, "<f8" if eb == 8 else "<i4", cnt, off))
+        want = {1: n * dim, 2: n * dim, 3: n, 4: n, 5: n + 1, 6: nnz, 7: nf, 8: nf * dim,
+                9: nf, 10: nf, 11: nf, 12: nf * dim}
+        if flags & 2:
+            want[13] = nf * dim
+        for sid, cnt in want.items():
+            if sid not in secs or secs[sid].size != cnt:
+                raise ValueError(f"{path}: section {sid} missing or of the wrong size")
+        off = secs[5]
+        if off[0] != 0 or off[-1] != nnz or np.any(np.diff(off) < 0):
+            raise ValueError(f"{path}: cell face offsets do not cover the face list")
+        return cls(dim=dim, periodic=bool(flags & 1),
+                   cell_pos=secs[1].reshape(n, dim), cell_centroid=secs[2].reshape(n, dim),
+                   cell_volume=secs[3], cell_total_area=secs[4], cell_face_offset=off,
+                   cell_face_index=secs[6], face_area=secs[7],
+                   face_midpoint=secs[8].reshape(nf, dim), face_left=secs[9],
+                   face_right=secs[10], face_kind=secs[11],
+                   face_right_pos=secs[12].reshape(nf, dim),
+                   face_velocity=secs[13].reshape(nf, dim) if flags & 2 else None)
+
     def check_geometry(self, rtol: float = 1e-9) -> None:
         """Sanity checks of a tessellation of the unit box."""
         tot = float(self.cell_volume.sum())
@@ -194,3 +249,21 @@ def build_voronoi(pos: np.ndarray, periodic: bool = False, nthreads: int = 0) ->
     finally:
         lib.sfx_voronoi_free(h)
     return m
+
+
+def build_voronoi_file(pos: np.ndarray, periodic: bool, path: str | Path,
+                       nthreads: int = 0) -> None:
+    """Tessellate generators with the standalone sfx_meshgen program (the same
+    builder as build_voronoi, run in a child process without the GPU
+    library) and write the face list as a mesh file at `path`."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n, dim = pos.shape
+    if not MESHGEN.exists():
+        raise FileNotFoundError(f"{MESHGEN} not built (shadowfax_b200.build)")
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "pos.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<iq", dim, n))
+            pos.tofile(f)
+        subprocess.run([str(MESHGEN), fin, str(int(periodic)), str(path), str(nthreads)],
+                       check=True)

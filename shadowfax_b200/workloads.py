@@ -171,16 +171,21 @@ class ServeRequest:
 
 
 def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
-               workers: int = 0, cache_dir=None) -> ServePool:
+               workers: int = 0, cache_dir=None, library: bool = True) -> ServePool:
     """the pool meshes (all 2k, or the indices in `only`), tessellated
     concurrently, largest first; with `cache_dir`, each mesh is read from
     its mesh file there when present and written there after tessellation
-    otherwise (sfx_meshfile_*)"""
+    otherwise (sfx_meshfile_*).  library=False builds and reads the meshes
+    without loading the GPU library (the standalone sfx_meshgen program and
+    the numpy mesh-file reader; needs cache_dir): the same face lists, for
+    CPU-only jobs."""
     import os
     from concurrent.futures import ThreadPoolExecutor
     from pathlib import Path
 
-    from .mesh import Mesh
+    from .mesh import Mesh, build_voronoi_file
+    if not library and not cache_dir:
+        raise ValueError("serve_pool(library=False) needs a cache_dir for its mesh files")
     sizes = serve_pool_sizes(k)
     jobs = [j for j in range(2 * k) if only is None or j in only]
     workers = workers or max(1, min(4, (os.cpu_count() or 4) // 4))
@@ -192,7 +197,11 @@ def serve_pool(k: int = 10, seed: int = 5, states_per_mesh: int = 2, only=None,
         path = None
         if cache_dir:
             path = Path(cache_dir) / f"pool_{dim}d_n{n}_seed{gen_seed}.sfxmesh"
-        if path is not None and path.exists():
+        if not library:
+            if not path.exists():
+                build_voronoi_file(random_generators(n, dim, gen_seed), True, path)
+            mesh = Mesh.read_file_numpy(path)
+        elif path is not None and path.exists():
             mesh = Mesh.read_file(path)
         else:
             mesh = build_voronoi(random_generators(n, dim, gen_seed), periodic=True)

@@ -196,3 +196,32 @@ def test_cell_face_offsets_must_cover_the_face_list(tmp_path, how):
     _write_py(f, m)
     with pytest.raises(L.SfxError, match="SFX_ERR_IO"):
         Mesh.read_file(f)
+
+
+@pytest.mark.parametrize("dim,periodic", [(2, True), (3, False)])
+def test_standalone_builder_and_numpy_reader(tmp_path, dim, periodic):
+    """sfx_meshgen (the builder as a program of its own, no GPU library)
+    writes the same face list as build_voronoi, and the numpy reader reads
+    back what sfx_meshfile_read reads, checksum included"""
+    from shadowfax_b200.mesh import build_voronoi_file
+    pos = random_generators(1200, dim, 11)
+    f = tmp_path / "g.sfxmesh"
+    build_voronoi_file(pos, periodic, f)
+    ref = build_voronoi(pos, periodic=periodic)
+    _same(ref, Mesh.read_file(f))
+    _same(ref, Mesh.read_file_numpy(f, verify_checksum=True))
+
+
+def test_numpy_reader_rejects_what_the_library_rejects(tmp_path):
+    m = _mesh(2, True, n=300)
+    off = m.cell_face_offset.copy()
+    off[-1] += 3
+    m.cell_face_offset = off
+    f = tmp_path / "bad.sfxmesh"
+    _write_py(f, m)
+    with pytest.raises(ValueError):
+        Mesh.read_file_numpy(f)
+    m = _mesh(2, True, n=300)
+    _write_py(f, m, version=2)
+    with pytest.raises(ValueError):
+        Mesh.read_file_numpy(f)

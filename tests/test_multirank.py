@@ -1,5 +1,6 @@
-"""The N>1 host logic on CPU ranks (gloo, world size 2): the whole-job figure
-of bench.py is the work of all ranks over the slowest rank's time; one mesh
+"""The N>1 host logic on CPU ranks (gloo, world size 2): the ranks share one
+request stream (whole requests, least face work first) and the whole-job
+figure of bench.py is the work of all ranks over the slowest rank's time; one mesh
 split over two ranks (the exchange, and PartitionedPass itself with the CPU
 oracle standing in for the device pass) equals the whole-mesh pass bit for
 bit, and a failing step on one rank stops both ranks with SfxError instead
@@ -30,24 +31,24 @@ def _rank_main(rank, world, port, out):
                             timeout=datetime.timedelta(seconds=60))
     try:
         import bench
-        from shadowfax_b200 import workloads as wl
 
         class A:
-            steps = 50
-            duration = None
+            requests = 300
+            duration = 60.0
 
-        reqs = bench.serve_requests(A, rank)
-        work = sum(r.nsteps for r in reqs)
+        reqs = bench.serve_requests(A)
+        owner = bench.shard_requests(reqs, world)
+        mine = [j for j, o in enumerate(owner) if o == rank]
+        work = sum(reqs[j].nsteps for j in mine)
         ms = 100.0 * (rank + 1)
         value, ms_max, total = bench.reduce_over_ranks(ms, work, "cpu", world)
-        out[rank] = (value, ms_max, total, work, [(r.mesh, r.nsteps) for r in reqs[:5]],
-                     len(wl.serve_stream(count=50, seed=5 + 1000 * rank)))
+        out[rank] = (value, ms_max, total, work, mine, owner.tolist())
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
-def test_two_cpu_ranks_reduce_work_and_time():
+def test_two_cpu_ranks_share_one_stream_and_reduce_work_and_time():
     world = 2
     port = _free_port()
     ctx = mp.get_context("spawn")
@@ -62,13 +63,35 @@ def test_two_cpu_ranks_reduce_work_and_time():
         res = dict(out)
     w0, w1 = res[0][3], res[1][3]
     for r in range(world):
-        value, ms_max, total, _, _, n = res[r]
+        value, ms_max, total, _, _, _ = res[r]
         assert ms_max == pytest.approx(200.0)          # the slowest rank's time
         assert total == pytest.approx(w0 + w1)          # all ranks' work
         assert value == pytest.approx((w0 + w1) / 0.2)
-        assert n == 50
-    # the ranks serve different streams (no request served twice)
-    assert res[0][4] != res[1][4]
+    # both ranks computed the same assignment; every request is served once
+    assert res[0][5] == res[1][5]
+    mine0, mine1 = set(res[0][4]), set(res[1][4])
+    assert not (mine0 & mine1) and len(mine0 | mine1) == 300
+
+
+def test_stream_sharding_balances_face_work():
+    """whole requests to the least-loaded GPU in arrival order: the estimated
+    face work per GPU differs by less than the largest single request"""
+    import bench
+    from shadowfax_b200 import workloads as wl
+    reqs = wl.serve_stream(count=2000, seed=5)
+    sizes = wl.serve_pool_sizes()
+    work = np.array([sizes[r.mesh % 10] * (3.0 if r.mesh < 10 else 7.8) * r.nsteps
+                     for r in reqs])
+    for world in (1, 2, 3, 8):
+        owner = bench.shard_requests(reqs, world)
+        assert owner.min() >= 0 and owner.max() < world
+        load = np.bincount(owner, weights=work, minlength=world)
+        assert load.max() - load.min() <= work.max()
+        # arrival order is kept within each GPU's share
+        for q in range(world):
+            ts = [reqs[j].t for j in np.flatnonzero(owner == q)]
+            assert ts == sorted(ts)
+    assert np.all(bench.shard_requests(reqs, 1) == 0)
 
 
 def _split_mesh_rank(rank, world, port, name, nsteps, out):
