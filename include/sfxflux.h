@@ -227,6 +227,11 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision);
  * kernels (1, 2, 4, 8 or 16; default 1 in 2D, 4 in 3D).  Changes the summation
  * tree of the per-cell sums, not the algorithm. */
 int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
+/* split pass: register cap of the face kernel, 0 (64 registers, four
+ * 256-thread blocks per SM; the default) or 1 (80 registers, three blocks).
+ * Changes the schedule only, not the results. */
+#define SFX_FACE_VARIANTS 2
+int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
 
 /* ---- one mesh over several devices (plain FP64) ----
  * Replaces the reference's MPI halo updates for the flux pass
@@ -273,6 +278,11 @@ int sfx_group_step(sfx_group* group, int32_t nsteps, int32_t use_graph,
  * gradient and update kernels; *lanes receives it */
 int sfx_group_tune(sfx_group* group, int32_t reps, int32_t* lanes);
 int sfx_group_set_lanes(sfx_group* group, int32_t lanes);
+/* time each face-kernel variant (SFX_FACE_VARIANTS) on this group, every
+ * timed face launch after a gradient launch (the states are read, none
+ * changes), and keep the fastest; *variant receives it */
+int sfx_group_tune_faces(sfx_group* group, int32_t reps, int32_t* variant);
+int sfx_group_set_face_variant(sfx_group* group, int32_t variant);
 /* per-member remaining step counts, kept on the device: a member at 0 is
  * skipped by the launches and each step counts the others down, so members
  * with different step counts share launches without host round trips */

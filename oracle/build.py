@@ -4,11 +4,15 @@
   (sfx_oracle.c), compiled with gcc from this directory.
 * ``oracle/_ref/refharness_{2,3}d_{libm,sfxpow}`` - the reference Shadowfax
   flux-pass sources compiled UNMODIFIED from the reference tree
-  (``$SFX_REFERENCE_SRC``, default /root/reference/src) together with
+  (``$SFX_REFERENCE_SRC``; by default ``reference/src`` beside this
+  repository's directory) together with
   oracle/refharness (single-rank MPI stand-in, version header, TimeLine
   constructor, driver).  Built only where the reference tree exists; the
   binaries then travel with the repository.  "libm" keeps glibc's pow,
-  "sfxpow" routes pow() to sfx_pow (refharness/pow_interpose.c).
+  "sfxpow" routes pow() and cbrt() to sfx_pow and sfx_cbrt
+  (refharness/pow_interpose.c).
+* ``oracle/_ref/refharness_{2,3}d_moving_{libm,sfxpow}`` - the same sources
+  built without -DSTATIC (moving generators: VorFace::set_v and the drift).
 
 Nothing here is linked into or called by the product library.
 """
@@ -21,7 +25,8 @@ from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path(os.environ.get("SFX_REFERENCE_SRC", "/root/reference/src"))
+REF_SRC = Path(os.environ.get("SFX_REFERENCE_SRC",
+                              str(HERE.parent.parent / "reference" / "src")))
 OUT = HERE / "_ref"
 ORACLE_SO = HERE / "libsfxoracle.so"
 
@@ -35,8 +40,11 @@ REF_UNITS = [
 # the reference's release flags plus: no FMA contraction (matches x86-64 default
 # code generation on every host), no builtin pow folding (so the sfxpow build
 # can interpose pow), <array> pre-included (src/RestartFile.hpp uses std::array)
-REF_FLAGS = ["-O2", "-ffp-contract=off", "-fno-builtin-pow", "-std=c++11",
-             "-include", "array", "-DSTATIC", "-w"]
+REF_FLAGS = ["-O2", "-ffp-contract=off", "-fno-builtin-pow", "-fno-builtin-cbrt", "-std=c++11",
+             "-include", "array", "-w"]
+# the two variants: static generators (the reference's -DSTATIC build) and
+# moving ones
+VARIANTS = {"": ["-DSTATIC"], "_moving": []}
 
 
 def _newer(out: Path, deps: list[Path]) -> bool:
@@ -54,8 +62,8 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_SO
 
 
-def ref_binary(dim: int, pow_kind: str) -> Path:
-    return OUT / f"refharness_{dim}d_{pow_kind}"
+def ref_binary(dim: int, pow_kind: str, moving: bool = False) -> Path:
+    return OUT / f"refharness_{dim}d{'_moving' if moving else ''}_{pow_kind}"
 
 
 def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
@@ -70,18 +78,21 @@ def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
            "-I", str(REF_SRC), "-I", str(REF_SRC / "utilities")]
     harness = HERE / "refharness" / "harness.cpp"
     interpose = HERE / "refharness" / "pow_interpose.c"
-    outs = [ref_binary(d, k) for d in (2, 3) for k in ("libm", "sfxpow")]
-    deps = [harness, interpose, HERE / "refharness" / "shim" / "mpi.h", Path(__file__)]
+    outs = [ref_binary(d, k, mv) for d in (2, 3) for k in ("libm", "sfxpow")
+            for mv in (False, True)]
+    deps = [harness, interpose, HERE / "refharness" / "shim" / "mpi.h", Path(__file__),
+            HERE.parent / "shadowfax_b200" / "csrc" / "sfx_pow.h"]
     if not force and all(_newer(o, deps) for o in outs):
         return outs
     tasks = []
     for d in (2, 3):
-        for u in REF_UNITS:
-            o = obj / (u.replace("/", "_") + f".{d}d.o")
-            tasks.append(["g++", *REF_FLAGS, f"-Dndim_={d}", *inc, "-c", str(REF_SRC / u),
-                          "-o", str(o)])
-        tasks.append(["g++", *REF_FLAGS, f"-Dndim_={d}", *inc, "-c", str(harness), "-o",
-                      str(obj / f"harness.{d}d.o")])
+        for var, vflags in VARIANTS.items():
+            for u in REF_UNITS:
+                o = obj / (u.replace("/", "_") + f".{d}d{var}.o")
+                tasks.append(["g++", *REF_FLAGS, *vflags, f"-Dndim_={d}", *inc, "-c",
+                              str(REF_SRC / u), "-o", str(o)])
+            tasks.append(["g++", *REF_FLAGS, *vflags, f"-Dndim_={d}", *inc, "-c", str(harness),
+                          "-o", str(obj / f"harness.{d}d{var}.o")])
     tasks.append(["gcc", "-O2", "-ffp-contract=off", "-std=c99", "-c", str(interpose), "-o",
                   str(obj / "pow_interpose.o")])
     with ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -89,12 +100,13 @@ def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
             if r.returncode:
                 raise RuntimeError(f"reference build failed: {' '.join(r.args)}\n{r.stderr}")
     for d in (2, 3):
-        objs = [str(obj / (u.replace("/", "_") + f".{d}d.o")) for u in REF_UNITS]
-        objs.append(str(obj / f"harness.{d}d.o"))
-        for k in ("libm", "sfxpow"):
-            extra = [str(obj / "pow_interpose.o")] if k == "sfxpow" else []
-            subprocess.run(["g++", "-o", str(ref_binary(d, k)), *objs, *extra, "-lm"],
-                           check=True)
+        for var in VARIANTS:
+            objs = [str(obj / (u.replace("/", "_") + f".{d}d{var}.o")) for u in REF_UNITS]
+            objs.append(str(obj / f"harness.{d}d{var}.o"))
+            for k in ("libm", "sfxpow"):
+                extra = [str(obj / "pow_interpose.o")] if k == "sfxpow" else []
+                subprocess.run(["g++", "-o", str(ref_binary(d, k, var == "_moving")), *objs,
+                                *extra, "-lm"], check=True)
     return outs
 
 

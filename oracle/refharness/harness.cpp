@@ -4,7 +4,7 @@
  * This translation unit is linked against the UNMODIFIED reference Shadowfax
  * sources of the hot path (VorFace, VorCell, VorGen, GasParticle, Particle and
  * the Exact/HLLC Riemann solvers), compiled from the reference tree by
- * oracle/build_ref.sh.  It reads a face-list mesh in the sfxflux binary
+ * oracle/build.py.  It reads a face-list mesh in the sfxflux binary
  * exchange format, builds the reference's own VorGen / VorCell / VorFace /
  * GasParticle objects from it and runs the reference's per-step loop for a
  * static mesh with one global time step:
@@ -108,6 +108,24 @@ int run_steps(Reader& in, const char* outpath) {
     in.read(hdr, 8);
     const int dim = hdr[0], ncell = hdr[1], nface = hdr[2], nnz = hdr[3];
     const int solverkind = hdr[4], nsteps = hdr[5];
+    /* moving generators (builds without -DSTATIC only): per step the
+     * generator velocities of VorCell::get_velocity with the reflective-box
+     * check of src/Simulation.cpp:366-398, the face velocities of
+     * VorFace::set_v, and the drift after the update (src/Simulation.cpp:
+     * 473-481).  One step per tessellation, as in the reference, where the
+     * mesh is rebuilt after every drift. */
+    const int moving = hdr[6], periodic = hdr[7];
+#ifdef STATIC
+    if(moving) {
+        fprintf(stderr, "harness: moving generators need a build without -DSTATIC\n");
+        return 5;
+    }
+#else
+    if(moving && nsteps != 1) {
+        fprintf(stderr, "harness: moving generators take one step per tessellation\n");
+        return 5;
+    }
+#endif
     double prm[4];
     in.read(prm, 4);
     const double gamma = prm[0], tol = prm[1], cutoff = prm[2], dt = prm[3];
@@ -240,6 +258,30 @@ int run_steps(Reader& in, const char* outpath) {
     try {
         for(int step = 0; step < nsteps; ++step) {
             auto t0 = std::chrono::steady_clock::now();
+#ifndef STATIC
+            if(moving) {
+                for(int i = 0; i < ncell; ++i) {
+                    StateVector Wgas = parts[i]->get_Wvec();
+                    Vec v = cells[i]->get_velocity();
+                    if(!periodic) {
+                        /* the unit box: centre 0.5, half side 0.5
+                         * (RectangularBox::inside, src/RectangularBox.cpp:91-99) */
+                        Vec newx = parts[i]->get_position() + dt * v;
+                        bool inside = true;
+                        for(unsigned int l = 0; l < ndim_; l++)
+                            if(fabs(0.5 - newx[l]) > 1. / 2) inside = false;
+                        if(!inside) {
+                            v[0] -= Wgas[1];
+                            v[1] -= Wgas[2];
+#if ndim_ == 3
+                            v[2] -= Wgas[3];
+#endif
+                        }
+                    }
+                    parts[i]->set_velocity(v);
+                }
+            }
+#endif
             for(int i = 0; i < ncell; ++i) {
                 StateVector gradients[3];
                 cells[i]->estimate_gradient(gradients);
@@ -261,6 +303,9 @@ int run_steps(Reader& in, const char* outpath) {
                 }
             }
             for(int i = 0; i < ncell; ++i) {
+#ifndef STATIC
+                if(moving) parts[i]->drift(dt);
+#endif
                 parts[i]->update_Q();
             }
             for(int i = 0; i < ncell; ++i) {
@@ -298,6 +343,13 @@ int run_steps(Reader& in, const char* outpath) {
     fwrite(buf.data(), sizeof(double), buf.size(), out);
     fwrite(grad_last.data(), sizeof(double), grad_last.size(), out);
     fwrite(dQ_last.data(), sizeof(double), dQ_last.size(), out);
+    if(moving) {
+        /* generator positions after the drift */
+        std::vector<double> pb((size_t)ncell * dim);
+        for(int i = 0; i < ncell; ++i)
+            for(int l = 0; l < dim; ++l) pb[(size_t)i * dim + l] = parts[i]->get_position()[l];
+        fwrite(pb.data(), sizeof(double), pb.size(), out);
+    }
     fclose(out);
     return 0;
 }

@@ -134,6 +134,7 @@ PROTOTYPES = {
     "sfx_meshfile_read": (C.c_int, [C.c_char_p, _dp, _dp, _dp, _dp, _ip, _ip, _dp, _dp, _ip,
                                     _ip, _ip, _dp, _dp]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sfx_mesh_set_face_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_mesh_set_ranges": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sfx_mesh_pack_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                       C.c_void_p]),
@@ -161,6 +162,8 @@ PROTOTYPES = {
     "sfx_group_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _ip]),
     "sfx_group_tune": (C.c_int, [C.c_void_p, C.c_int32, _ip]),
     "sfx_group_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sfx_group_tune_faces": (C.c_int, [C.c_void_p, C.c_int32, _ip]),
+    "sfx_group_set_face_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_group_free": (C.c_int, [C.c_void_p]),
     "sfx_flux_pass_noalloc": (C.c_int, [C.POINTER(sfx_device_mesh), C.POINTER(sfx_config),
                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,

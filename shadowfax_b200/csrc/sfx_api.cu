@@ -139,6 +139,7 @@ int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t 
         g.n_meshes = 1;
         g.dim = m->d.dim;
         g.lanes = m->d.lanes;
+        g.face_variant = m->d.face_variant;
         sfx_split_blocks(m->d.dim, m->d.lanes, m->d.n_cells, m->d.n_faces, g.blocks);
         return sfx_split_group_phase(&g, phase, &c->sp, s);
     }
@@ -189,7 +190,8 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     d.cw = d.cg = nullptr;
     d.dqm = nullptr;
     d.dqv = nullptr;
-    d.slowq = d.slowq_n = nullptr;
+    d.slowq = nullptr;
+    d.slowq_n = nullptr;
     d.slowq_cap = 0;
     struct Slot {
         void** p;
@@ -203,7 +205,7 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     A(&d.totals_scratch, (size_t)(S + 1) * 1024);
     if(split) {
         A(&d.cw, 2 * n);
-        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
+        A(&d.cg, (size_t)sfx_split_grad_vec4(dim) * n);
         A(&d.dqm, F);
         A(&d.dqv, (size_t)dim * F);
         d.slowq_cap = slowq_capacity(F);
@@ -360,7 +362,7 @@ int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
     if(precision == SFX_PREC_SPLIT) {
         /* fg, fi, fsh, an, dqm, dqv, queue; cw, cg, cx, self table; nbe */
         bytes += F * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + 4 * slowq_capacity(F) + 4;
-        bytes += n * (32 + 16 * ((dim * S + 3) / 4) + 16) + 256;
+        bytes += n * (32 + 16 * sfx_split_grad_vec4((int)dim) + 16) + 256;
         bytes += nnz * 4;
     }
     return bytes;
@@ -533,7 +535,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         A(&d.fi, F);
         A(&d.fsh, F);
         A(&d.cw, 2 * n);
-        A(&d.cg, (size_t)((dim * S + 3) / 4) * n);
+        A(&d.cg, (size_t)sfx_split_grad_vec4(dim) * n);
         A(&d.cx, n);
         A(&d.nbe, nnz);
         A(&d.an, (size_t)dim * F);
@@ -721,7 +723,7 @@ int sfx_flux_pass(sfx_mesh* m, double dt, double* grad, double* dQ_face,
     std::vector<double> tg(grad ? n * D * S : 0), tq(dQ_face ? F * S : 0);
     if(grad && split) {
         /* FP32 gradient records [n][G float4] -> [D*S][n] */
-        const int G = (D * S + 3) / 4;
+        const int G = sfx_split_grad_vec4(D);
         std::vector<float> tf((size_t)n * G * 4);
         SFX_TRY(cuda_ok(cudaMemcpyAsync(tf.data(), m->d.cg, sizeof(float) * tf.size(),
                                         cudaMemcpyDeviceToHost, s)));
@@ -796,7 +798,7 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
     const int64_t n = b.n_cells, F = b.n_faces, S = b.S, D = b.dim;
     int64_t bytes = n * S * 16 + (S + 1) * 1024 * 8 + 64;
     if(precision == SFX_PREC_SPLIT)
-        bytes += n * 32 + n * 16 * ((D * S + 3) / 4) + F * 8 + F * D * 8 +
+        bytes += n * 32 + n * 16 * sfx_split_grad_vec4((int)D) + F * 8 + F * D * 8 +
                  4 * (int64_t)slowq_capacity(F) + 4 + (int64_t)sizeof(sfx_group_entry) + 24;
     else
         bytes += n * D * S * 8 + F * 4 +
@@ -808,6 +810,12 @@ int sfx_mesh_set_lanes(sfx_mesh* m, int32_t lanes) {
     if(!m || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16))
         return SFX_ERR_INVALID;
     m->d.lanes = lanes;
+    return SFX_OK;
+}
+
+int sfx_mesh_set_face_variant(sfx_mesh* m, int32_t variant) {
+    if(!m || variant < 0 || variant >= SFX_FACE_VARIANTS) return SFX_ERR_INVALID;
+    m->d.face_variant = variant;
     return SFX_OK;
 }
 

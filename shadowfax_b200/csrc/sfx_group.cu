@@ -155,6 +155,13 @@ extern "C" int sfx_group_set_dt(sfx_group* g, const double* dt) {
     return upload_layout(g);
 }
 
+extern "C" int sfx_group_set_face_variant(sfx_group* g, int32_t variant) {
+    if(!g || variant < 0 || variant >= SFX_FACE_VARIANTS) return SFX_ERR_INVALID;
+    g->dev.face_variant = variant;
+    drop_graph(g); /* a captured step holds the old kernel */
+    return SFX_OK;
+}
+
 extern "C" int sfx_group_set_lanes(sfx_group* g, int32_t lanes) {
     if(!g || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16))
         return SFX_ERR_INVALID;
@@ -322,6 +329,47 @@ extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
     int r2 = sfx_group_set_lanes(g, best);
     if(lanes_out) *lanes_out = best;
     return rc ? rc : r2;
+}
+
+extern "C" int sfx_group_tune_faces(sfx_group* g, int32_t reps, int32_t* variant_out) {
+    if(!g || reps <= 0) return SFX_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)sfx_ctx_stream(g->ctx);
+    const sfx_solver_params* sp = sfx_ctx_params(g->ctx);
+    cudaEvent_t e0, e1;
+    if(cudaEventCreate(&e0) != cudaSuccess) return SFX_ERR_CUDA;
+    if(cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return SFX_ERR_CUDA;
+    }
+    int best = g->dev.face_variant;
+    float best_ms = 1e30f;
+    int rc = SFX_OK;
+    for(int v = 0; v < SFX_FACE_VARIANTS && !rc; ++v) {
+        g->dev.face_variant = v;
+        float total = 0.f;
+        /* every face launch follows a gradient launch, which also empties
+         * the queued-face lists; one untimed pair, then reps timed */
+        for(int r = 0; r <= reps && !rc; ++r) {
+            rc = sfx_split_group_phase(&g->dev, 0, sp, s);
+            if(!rc) rc = cuda_ok(cudaEventRecord(e0, s));
+            if(!rc) rc = sfx_split_group_phase(&g->dev, 1, sp, s);
+            if(!rc) rc = cuda_ok(cudaEventRecord(e1, s));
+            if(!rc) rc = cuda_ok(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            if(!rc) rc = cuda_ok(cudaEventElapsedTime(&ms, e0, e1));
+            if(r > 0) total += ms;
+        }
+        if(!rc && total < best_ms) {
+            best_ms = total;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->dev.face_variant = best;
+    drop_graph(g);
+    if(variant_out) *variant_out = best;
+    return rc;
 }
 
 extern "C" int sfx_group_set_steps(sfx_group* g, const int32_t* steps) {

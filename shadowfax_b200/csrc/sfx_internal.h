@@ -29,6 +29,7 @@ struct sfx_dmesh {
     int64_t nnz;
     int32_t has_velocity;
     int32_t lanes; /* split pass: lanes per cell of the gradient/update kernels */
+    int32_t face_variant; /* split pass: register cap of the face kernel (sfx_split.cu) */
     /* cells */
     double* pos;    /* [dim][n]  */
     double* cen;    /* [dim][n]  */
@@ -70,7 +71,10 @@ struct sfx_dmesh {
      * fi [F] int2: {L, R}; R = -1 mirror, R | 1<<30 periodic image;
      * fsh [F]: periodic image shift, 2 bits per axis (0, +1, -1 box);
      * cw [2n] float4 cell record {rho, v.., p | Q.m, total area ..};
-     * cg [G*n] float4 gradients (G = 4 in 3D, 2 in 2D);
+     * cg [G*n] float4 per-cell record: the limited gradients [dim][S], then
+     *     dW/dt [S] (the Euler Jacobian at the cell state times those
+     *     gradients, the MUSCL-Hancock prediction every face of the cell
+     *     shares), zero padded (G = sfx_split_grad_vec4(dim): 5 in 3D, 3 in 2D);
      * cx [n] float4 {x - centroid, volume};
      * an [dim][F] FP64 area vector A n (n from x_L to x_R), for the pressure
      *     force, so that the forces on a cell cancel to FP64 round-off in a
@@ -125,6 +129,7 @@ struct sfx_group_dev {
     int32_t n_meshes;
     int32_t dim;
     int32_t lanes; /* lanes per cell of the gradient and update kernels */
+    int32_t face_variant; /* 0: 64 registers (4 blocks per SM), 1: 80 (3 blocks) */
     int32_t blocks[3];
 };
 
@@ -199,6 +204,12 @@ int sfx_mesh_clone_async(sfx_ctx* ctx, sfx_mesh* base, void* stream, sfx_mesh** 
  * tuning, the same for a mesh alone and in a group: one in 2D (about six
  * faces per cell), four in 3D (about sixteen); measured fastest on 300,000-cell
  * meshes */
+/* float4s of the split pass's per-cell gradient record (cg) */
+inline int sfx_split_grad_vec4(int dim) {
+    const int S = dim + 2;
+    return (dim * S + S + 3) / 4;
+}
+
 inline int sfx_default_lanes(int dim) {
     return dim == 2 ? 1 : 4;
 }

@@ -364,4 +364,51 @@ SFX_HD double sfx_pow_fast(double x, double y) {
     return q * sfx_u2d((uint64_t)(ni + 1023) << 52);
 }
 
+
+/*
+ * sfx_cbrt: a deterministic cube root for host and device code (the moving
+ * mesh's generator velocity, VorCell::get_velocity, src/VorCell.cpp:966-1008,
+ * takes the cube root of the cell volume; glibc's and CUDA's cbrt can differ
+ * in the last bit).  Only IEEE basic operations and FMA:
+ *   |x| = 2^(3k) t, t in [1, 8) (subnormals scaled by 2^162 first);
+ *   Newton's iteration y <- (2 y + t / y^2) / 3 from y = (t + 2) / 3, which is
+ *   never below t^(1/3) (arithmetic-geometric mean inequality), so the
+ *   iterates fall monotonically to the root: six steps reach double
+ *   precision on [1, 8);
+ *   one more step with the residual y^3 - t formed exactly to first order
+ *   (products split by FMA), then 2^k and the sign.
+ * Special values: +-0, +-inf and NaN are returned as they are.
+ */
+SFX_HD double sfx_cbrt(double x) {
+    if(x == 0.0 || x != x || x - x != 0.0) return x; /* 0, NaN, inf */
+    const double ax = x < 0.0 ? -x : x;
+    uint64_t u = sfx_d2u(ax);
+    int adj = 0;
+    double a = ax;
+    if((u >> 52) == 0) { /* subnormal */
+        a = ax * 0x1p162;
+        u = sfx_d2u(a);
+        adj = -54;
+    }
+    const int e = (int)(u >> 52) - 1023;
+    /* e = 3k + r, r in {0, 1, 2} */
+    int k = e >= 0 ? e / 3 : -((-e + 2) / 3);
+    const int r = e - 3 * k;
+    const double t = sfx_u2d((u & 0x000fffffffffffffull) | ((uint64_t)(1023 + r) << 52));
+    double y = (t + 2.0) / 3.0;
+    for(int i = 0; i < 6; ++i) y = (2.0 * y + t / (y * y)) / 3.0;
+    /* y^3 - t with the rounding errors of y*y and (y*y)*y kept */
+    const double p = y * y;
+    const double pe = sfx_fma(y, y, -p);
+    const double q = p * y;
+    const double qe = sfx_fma(p, y, -q) + pe * y;
+    const double res = (q - t) + qe;
+    y = y - res / (3.0 * p);
+    k += adj;
+    /* y * 2^k, k within the normal exponent range for every double x */
+    const double sc = sfx_u2d((uint64_t)(1023 + k) << 52);
+    const double out = y * sc;
+    return x < 0.0 ? -out : out;
+}
+
 #endif /* SFX_POW_H */

@@ -101,14 +101,28 @@ __device__ __forceinline__ void store_cell(float4* cw, int i, const float* W, fl
     }
 }
 
-/* gradient record: g[l][k] at flat l*S+k, padded to float4s */
+/* per-cell gradient record: g[l][k] at flat l*S+k, then dW/dt[k] at
+ * D*S+k, padded to float4s (GradVec4<D>::value of them) */
 template <int D>
-__device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i,
-                                          float (*g)[D + 2]) {
-    constexpr int S = D + 2, G = (D * S + 3) / 4;
+struct GradVec4 {
+    static constexpr int value = (D * (D + 2) + (D + 2) + 3) / 4;
+};
+
+template <int D>
+__device__ __forceinline__ void sdwdt(float gamma, const float* W, const float (*g)[D + 2],
+                                      float* dW);
+
+/* a cell's gradients and dW/dt: with STORED the record's dW/dt, otherwise
+ * only the gradient float4s are read and dW/dt is formed here (the HLLC face
+ * kernel, which is closer to the memory bound than to the issue bound) */
+template <int D, bool STORED>
+__device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i, float gamma,
+                                          const float* W, float (*g)[D + 2], float* dWdt) {
+    constexpr int S = D + 2, G = GradVec4<D>::value;
+    constexpr int GL = STORED ? G : (D * S + 3) / 4;
     float t[4 * G];
 #pragma unroll
-    for(int q = 0; q < G; ++q) {
+    for(int q = 0; q < GL; ++q) {
         const float4 v = __ldg(cg + (size_t)G * i + q);
         t[4 * q] = v.x;
         t[4 * q + 1] = v.y;
@@ -119,13 +133,19 @@ __device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i,
     for(int l = 0; l < D; ++l)
 #pragma unroll
         for(int k = 0; k < S; ++k) g[l][k] = t[l * S + k];
+    if(STORED) {
+#pragma unroll
+        for(int k = 0; k < S; ++k) dWdt[k] = t[D * S + k];
+    } else {
+        sdwdt<D>(gamma, W, g, dWdt);
+    }
 }
 
 template <int D>
 __device__ __forceinline__ void geom(const float4* __restrict__ fg, int f, float& A, float* c,
                                      float* r, float& rn) {
-    const float4 g0 = __ldg(fg + 2 * f);
-    const float4 g1 = __ldg(fg + 2 * f + 1);
+    const float4 g0 = __ldg(fg + 2 * (size_t)f);
+    const float4 g1 = __ldg(fg + 2 * (size_t)f + 1);
     A = g0.x;
     c[0] = g0.y;
     c[1] = g0.z;
@@ -276,10 +296,10 @@ __device__ __forceinline__ double seg_sum(double v) {
 }
 
 template <int D, int LPC>
-__device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
-    constexpr int S = D + 2, G = (D * S + 3) / 4;
+__device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma, const int t) {
+    constexpr int S = D + 2, G = GradVec4<D>::value;
     const int i = t / LPC, lane = t % LPC;
-    if(t == 0) *m.slowq_n = 0; /* a new step: empty the slow-face queue */
+    if(t == 0) *m.slowq_n = 0; /* a new step: empty the queued-face list */
     /* whole warps stay alive for the shuffles; lanes past the end idle */
     const bool live = i < m.n_cells && !failed(m.err);
     const int ic = live ? i : 0;
@@ -395,14 +415,21 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const int t) {
 #pragma unroll
     for(int k = 0; k < S; ++k) alpha[k] = seg_min<LPC>(alpha[k]);
     if(!live) return;
-    /* lane q < G writes float4 q of the gradient record */
+    /* lane q % LPC writes float4 q of the gradient record: the limited
+     * gradients, then dW/dt at the cell state (every face of the cell
+     * predicts its half step with it) */
     float out[4 * G];
+    float lg[D][S];
 #pragma unroll
     for(int l = 0; l < D; ++l)
 #pragma unroll
-        for(int k = 0; k < S; ++k) out[l * S + k] = delta[l][k] * alpha[k];
+        for(int k = 0; k < S; ++k) {
+            lg[l][k] = delta[l][k] * alpha[k];
+            out[l * S + k] = lg[l][k];
+        }
+    sdwdt<D>(gamma, W, lg, out + D * S);
 #pragma unroll
-    for(int q = D * S; q < 4 * G; ++q) out[q] = 0.f;
+    for(int q = D * S + S; q < 4 * G; ++q) out[q] = 0.f;
 #pragma unroll
     for(int q = 0; q < G; ++q)
         if(lane == q % LPC)
@@ -451,12 +478,14 @@ __device__ __forceinline__ float slimit(float phimid0, float phiL, float phiR, f
 }
 
 template <int D>
-__device__ __forceinline__ void spredict(float gamma, float hdt, float* Wt, const float* Wself,
+__device__ __forceinline__ void spredict(float hdt, float* Wt, const float* Wself,
                                          const float* Wother, const float (*g)[D + 2],
-                                         const float* d, bool do_limit, float r) {
+                                         const float* dWdt, const float* d, bool do_limit,
+                                         float r) {
     constexpr int S = D + 2;
     float dW[S];
-    sdwdt<D>(gamma, Wt, g, dW);
+#pragma unroll
+    for(int k = 0; k < S; ++k) dW[k] = dWdt[k];
 #pragma unroll
     for(int k = 0; k < S; ++k) {
         float s = 0.f;
@@ -783,18 +812,47 @@ struct XS {
  * takes a Newton step to (nearly) zero pressure (where the reference's
  * iteration can stop at p = 0), when the FP64 step is not small, or when it
  * moves a side between shock and rarefaction. */
-template <int D>
-__device__ __forceinline__ bool fast_root(const sfx_solver_params& s, const double* WL,
-                                          const double* WR, double aL, double aR, double vL,
+/* f_K, f_K' and z_K = (p/p_K)^((g-1)/(2g)) (rarefaction side) of one side in
+ * FP64 (XS::side without the shared power) */
+__device__ __forceinline__ void side64(const sfx_solver_params& s, double p, double rho,
+                                       double pK, double a, double& f, double& fp, double& z) {
+    if(p > pK) {
+        const double A = s.tdgp1 / rho, B = s.gm1dgp1 * pK;
+        const double q = sqrt(A / (p + B));
+        f = (p - pK) * q;
+        fp = (1. - 0.5 * (p - pK) / (B + p)) * q;
+        z = 0.;
+    } else {
+        const double r = p / pK;
+        z = xpow(r, s.gm1d2g);
+        f = s.tdgm1 * a * (z - 1.);
+        fp = r > 0. ? z / (r * (rho * a)) : 1. / (rho * a) * xpow(r, -s.gp1d2g);
+    }
+}
+
+/* p* for the face kernel: Newton's method in FP32 from the reference's
+ * initial guess, then one FP64 Newton step from the FP32 root.  The face's
+ * states are FP32 values; the FP32 root is within about 1e-6 of p*, and the
+ * FP64 step (quadratic convergence) takes it to about 1e-12, inside the
+ * iteration's 1e-8 tolerance.  f_K and the rarefaction powers z_K at the
+ * final pressure are the FP64 values at the FP32 root carried along the
+ * step to first order (error of the order of the step squared).  Two FP64
+ * powers at most instead of one per FP64 iteration plus two per face.
+ * Returns false, and the FP64 iteration runs from the start, outside the
+ * range where FP32 is safe, when the FP32 iteration does not converge or
+ * takes a Newton step to (nearly) zero pressure (where the reference's
+ * iteration can stop at p = 0), when the FP64 step is not small, or when it
+ * moves a side between shock and rarefaction. */
+__device__ __forceinline__ bool fast_root(const sfx_solver_params& s, double rL, double pL,
+                                          double rR, double pR, double aL, double aR, double vL,
                                           double vR, double& p, double& fL, double& fR,
                                           double& zL, double& zR) {
-    const double pL = WL[D + 1], pR = WR[D + 1];
     constexpr double lo = 1e-12, hi = 1e12;
-    if(!(pL > lo && pL < hi && pR > lo && pR < hi && WL[0] > lo && WL[0] < hi && WR[0] > lo &&
-         WR[0] < hi && fabs(vR - vL) < hi))
+    if(!(pL > lo && pL < hi && pR > lo && pR < hi && rL > lo && rL < hi && rR > lo &&
+         rR < hi && fabs(vR - vL) < hi))
         return false;
     const float e = (float)s.gm1d2g, tdgm1 = (float)s.tdgm1;
-    const float fpL = (float)pL, fpR = (float)pR, frL = (float)WL[0], frR = (float)WR[0];
+    const float fpL = (float)pL, fpR = (float)pR, frL = (float)rL, frR = (float)rR;
     const float faL = (float)aL, faR = (float)aR, dv = (float)(vR - vL);
     const float AL = (float)s.tdgp1 / frL, BL = (float)s.gm1dgp1 * fpL;
     const float AR = (float)s.tdgp1 / frR, BR = (float)s.gm1dgp1 * fpR;
@@ -838,11 +896,10 @@ __device__ __forceinline__ bool fast_root(const sfx_solver_params& s, const doub
         pg = pn;
         if(conv) break;
     }
-    XS<D> x{s};
     const double p0 = (double)pg;
     double fpl, fpr;
-    x.side(p0, WL, aL, 0., 0., fL, fpl, zL);
-    x.side(p0, WR, aR, 0., 0., fR, fpr, zR);
+    side64(s, p0, rL, pL, aL, fL, fpl, zL);
+    side64(s, p0, rR, pR, aR, fR, fpr, zR);
     const double dp = -(fL + fR + (vR - vL)) / (fpl + fpr);
     const double p1 = p0 + dp;
     if(!(fabs(dp) <= 1e-5 * p0) || (p0 > pL) != (p1 > pL) || (p0 > pR) != (p1 > pR))
@@ -910,7 +967,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         XS<D> x{s};
         const double pL = WL[D + 1], pR = WR[D + 1];
         double p = 0., fL = 0., zL = 0., fR = 0., zR = 0.;
-        if(MODE != kSolveDefer || !fast_root<D>(s, WL, WR, aL, aR, vL, vR, p, fL, fR, zL, zR)) {
+        if(MODE != kSolveDefer ||
+           !fast_root(s, WL[0], pL, WR[0], pR, aL, aR, vL, vR, p, fL, fR, zL, zR)) {
         /* p_K^-e (e = (g-1)/(2g)): (p/p_K)^e = p^e p_K^-e, one pow per
          * evaluation for both sides (0: not finite, pow of the ratio) */
         double iL = xpow(pL, -s.gm1d2g), iR = xpow(pR, -s.gm1d2g);
@@ -1077,48 +1135,58 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
     return bad ? SFX_ERR_RIEMANN : SFX_OK;
 }
 
-template <int D, int SOLVER, int MODE>
-__device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
-                                            const float dt, const int f) {
+/* Phase one of every face kernel: a face's two predicted states (MUSCL-
+ * Hancock half step with the pairwise limiter, VorFace.cpp:670-838), its unit
+ * normal and what its dQ needs.  The over-flux limits lim_K = A / total_area_K
+ * * Q.m_K (VorFace.cpp:837-866) are formed here once. */
+template <int D>
+struct FaceWork {
+    float WL[D + 2], WR[D + 2], n[D];
+    float A, limL, limR;
+    bool mirror;
+};
+
+/* false: nothing to solve (a face past the end, or of zero area, whose dQ is
+ * written as zero here) */
+template <int D, bool STORED>
+__device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma, const float hdt,
+                                          const int f, FaceWork<D>& w) {
     constexpr int S = D + 2;
-    if(f >= m.n_faces || failed(m.err)) return;
-    float A, c[D], r[D], rn;
-    geom<D>(m.fg, f, A, c, r, rn);
-    if(A == 0.f) {
+    float c[D], r[D], rn;
+    geom<D>(m.fg, f, w.A, c, r, rn);
+    if(w.A == 0.f) {
         m.dqm[f] = make_float2(0.f, 0.f);
 #pragma unroll
         for(int l = 0; l < D; ++l) m.dqv[(size_t)l * m.n_faces + f] = 0.;
-        return;
+        return false;
     }
     const int2 fi = __ldg(m.fi + f);
     const int iL = fi.x;
-    const bool mirror = fi.y < 0;
-    const int iR = mirror ? 0 : (fi.y & kIndexMask);
-    const float g = (float)sp.gamma;
-    const float hdt = 0.5f * dt;
-    float nrm[D];
+    w.mirror = fi.y < 0;
+    const int iR = w.mirror ? 0 : (fi.y & kIndexMask);
     const float irn = 1.f / rn;
 #pragma unroll
-    for(int l = 0; l < D; ++l) nrm[l] = -r[l] * irn;
+    for(int l = 0; l < D; ++l) w.n[l] = -r[l] * irn;
     const Cell<D> cL = load_cell<D>(m.cw, iL);
     const float4 xL = __ldg(m.cx + iL);
     const float xmcL[3] = {xL.x, xL.y, xL.z};
-    float WL[S], WR[S], WLr[S], WRr[S];
+    float WLr[S], WRr[S];
 #pragma unroll
     for(int k = 0; k < S; ++k) {
-        WL[k] = cL.W[k];
-        WR[k] = 0.f;
+        w.WL[k] = cL.W[k];
+        w.WR[k] = 0.f;
         WRr[k] = 0.f;
     }
-    float QmR = 0.f, taR = 1.f, rr = 1.f;
-    if(!mirror) {
+    w.limL = w.A / cL.tarea * cL.Qm;
+    w.limR = 0.f;
+    float rr = 1.f;
+    if(!w.mirror) {
         const Cell<D> cR = load_cell<D>(m.cw, iR);
         const float4 xR = __ldg(m.cx + iR);
         const float xmcR[3] = {xR.x, xR.y, xR.z};
 #pragma unroll
-        for(int k = 0; k < S; ++k) WR[k] = cR.W[k];
-        QmR = cR.Qm;
-        taR = cR.tarea;
+        for(int k = 0; k < S; ++k) w.WR[k] = cR.W[k];
+        w.limR = w.A / cR.tarea * cR.Qm;
         /* centroid difference (unshifted centroids, as the reference) */
         float sh[D];
 #pragma unroll
@@ -1139,72 +1207,65 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
             dR[l] = c[l] + xmcR[l] + 0.5f * r[l];
         }
         rr = sqrtf(cd2);
-        float gR[D][S];
-        load_grad<D>(m.cg, iR, gR);
+        float gR[D][S], dWR[S];
+        load_grad<D, STORED>(m.cg, iR, gamma, w.WR, gR, dWR);
 #pragma unroll
-        for(int k = 0; k < S; ++k) WRr[k] = WR[k];
-        spredict<D>(g, hdt, WRr, WR, WL, gR, dR, true, rr);
+        for(int k = 0; k < S; ++k) WRr[k] = w.WR[k];
+        spredict<D>(hdt, WRr, w.WR, w.WL, gR, dWR, dR, true, rr);
     }
     {
-        float dL[D], gL[D][S];
+        float dL[D], gL[D][S], dWL[S];
 #pragma unroll
         for(int l = 0; l < D; ++l) dL[l] = c[l] + xmcL[l] - 0.5f * r[l];
-        load_grad<D>(m.cg, iL, gL);
+        load_grad<D, STORED>(m.cg, iL, gamma, w.WL, gL, dWL);
 #pragma unroll
-        for(int k = 0; k < S; ++k) WLr[k] = WL[k];
-        spredict<D>(g, hdt, WLr, WL, WR, gL, dL, !mirror, rr);
+        for(int k = 0; k < S; ++k) WLr[k] = w.WL[k];
+        spredict<D>(hdt, WLr, w.WL, w.WR, gL, dWL, dL, !w.mirror, rr);
     }
-    if(WL[0] != 0.f) {
+    if(w.WL[0] != 0.f) {
 #pragma unroll
-        for(int k = 0; k < S; ++k) WL[k] = WLr[k];
+        for(int k = 0; k < S; ++k) w.WL[k] = WLr[k];
     }
-    if(WR[0] != 0.f) {
+    if(w.WR[0] != 0.f) {
 #pragma unroll
-        for(int k = 0; k < S; ++k) WR[k] = WRr[k];
+        for(int k = 0; k < S; ++k) w.WR[k] = WRr[k];
     }
-    SFlux<D> F;
-    int status = SFX_OK;
-    if(SOLVER == SFX_SOLVER_HLLC) {
-        shllc<D>(g, WL, WR, nrm, mirror, F);
-    } else {
-        double dWL[S], dWR[S], dn[D], h[S];
+    return true;
+}
+
+/* the exact solver's flux contracted with n (ExactRiemannSolver::get_flux,
+ * :815-880) from its half state */
+template <int D>
+__device__ __forceinline__ void exact_flux(double gamma, const double* h, const double* dn,
+                                           SFlux<D>& F) {
+    F.m = 0.f;
+    F.P = 0.f;
+    F.E = 0.f;
 #pragma unroll
-        for(int l = 0; l < D; ++l) dn[l] = nrm[l];
+    for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
+    if(h[0] != 0.) {
+        double un = 0., v2 = 0.;
 #pragma unroll
-        for(int k = 0; k < S; ++k) {
-            dWL[k] = WL[k];
-            dWR[k] = WR[k];
+        for(int l = 0; l < D; ++l) {
+            un += h[1 + l] * dn[l];
+            v2 += h[1 + l] * h[1 + l];
         }
-        status = sexact<D, MODE>(sp, dWL, dWR, dn, mirror, h);
-        if(MODE == kSolveDefer && status == kDefer) {
-            /* Brent's method: the face goes to the queue (room for every face)
-             * and the follow-up launch writes its dQ */
-            m.slowq[atomicAdd(m.slowq_n, 1)] = f;
-            return;
-        }
-        F.m = 0.f;
-        F.P = 0.f;
-        F.E = 0.f;
+        const double e = 0.5 * h[0] * v2 + h[D + 1] / (gamma - 1.);
+        const double mf = h[0] * un;
+        F.m = (float)mf;
 #pragma unroll
-        for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
-        if(h[0] != 0.) {
-            /* ExactRiemannSolver::get_flux contracted with n (:815-880) */
-            double un = 0., v2 = 0.;
-#pragma unroll
-            for(int l = 0; l < D; ++l) {
-                un += h[1 + l] * dn[l];
-                v2 += h[1 + l] * h[1 + l];
-            }
-            const double e = 0.5 * h[0] * v2 + h[D + 1] / (sp.gamma - 1.);
-            const double mf = h[0] * un;
-            F.m = (float)mf;
-#pragma unroll
-            for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * h[1 + l]);
-            F.P = (float)h[D + 1];
-            F.E = (float)((e + h[D + 1]) * un);
-        }
+        for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * h[1 + l]);
+        F.P = (float)h[D + 1];
+        F.E = (float)((e + h[D + 1]) * un);
     }
-    if(mirror) {
+}
+
+/* Last phase of every face kernel: dt A flux with the over-flux limiter, the
+ * face's dQ records and its status. */
+template <int D>
+__device__ __forceinline__ void face_dq(const sfx_dmesh& m, const float dt, const int f,
+                                        const FaceWork<D>& w, SFlux<D> F, int status) {
+    if(w.mirror) {
         /* the reflective Riemann problem has zero normal velocity at the wall:
          * no mass, energy or advected momentum crosses it, only the pressure
          * force (the FP32 solver would leave a round-off-sized leak) */
@@ -1213,7 +1274,7 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
 #pragma unroll
         for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
     }
-    const float dtA = dt * A;
+    const float dtA = dt * w.A;
     float dm = dtA * F.m, dE = dtA * F.E;
     /* momentum: advective part in FP32, pressure force dt P (A n) in FP64 */
     double dv[D];
@@ -1223,18 +1284,16 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
     for(int l = 0; l < D; ++l)
         dv[l] = (double)(dtA * F.mv[l]) + dtP * __ldg(m.an + (size_t)l * FF + f);
     /* over-flux limiter (VorFace.cpp:837-866) */
-    const float afL = A / cL.tarea;
-    if(dm > afL * cL.Qm) {
-        const float cf = fabsf(afL * cL.Qm / dm);
+    if(dm > w.limL) {
+        const float cf = fabsf(w.limL / dm);
         dm *= cf;
         dE *= cf;
 #pragma unroll
         for(int l = 0; l < D; ++l) dv[l] *= (double)cf;
     }
-    if(!mirror) {
-        const float afR = A / taR;
-        if(-dm > afR * QmR) {
-            const float cf = fabsf(afR * QmR / dm);
+    if(!w.mirror) {
+        if(-dm > w.limR) {
+            const float cf = fabsf(w.limR / dm);
             dm *= cf;
             dE *= cf;
 #pragma unroll
@@ -1246,6 +1305,210 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
     for(int l = 0; l < D; ++l) m.dqv[(size_t)l * FF + f] = dv[l];
     if(status == SFX_OK && F.m != F.m) status = SFX_ERR_NAN_FLUX;
     if(status != SFX_OK) report_face(m.err, f, status);
+}
+
+template <int D, int SOLVER, int MODE>
+__device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
+                                            const float dt, const int f) {
+    constexpr int S = D + 2;
+    if(f >= m.n_faces || failed(m.err)) return;
+    FaceWork<D> w;
+    /* HLLC forms dW/dt itself; the exact solver's kernels read it */
+    if(!face_work<D, SOLVER != SFX_SOLVER_HLLC>(m, (float)sp.gamma, 0.5f * dt, f, w)) return;
+    SFlux<D> F;
+    int status = SFX_OK;
+    if(SOLVER == SFX_SOLVER_HLLC) {
+        shllc<D>((float)sp.gamma, w.WL, w.WR, w.n, w.mirror, F);
+    } else {
+        double dWL[S], dWR[S], dn[D], h[S];
+#pragma unroll
+        for(int l = 0; l < D; ++l) dn[l] = w.n[l];
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            dWL[k] = w.WL[k];
+            dWR[k] = w.WR[k];
+        }
+        static_assert(MODE == kSolveInline, "queued faces come from k_group_sfaces_exact");
+        status = sexact<D, MODE>(sp, dWL, dWR, dn, w.mirror, h);
+        exact_flux<D>(sp.gamma, h, dn, F);
+    }
+    face_dq<D>(m, dt, f, w, F, status);
+}
+
+/* -------------------- exact solver: faces sorted by wave pattern --------------------
+ * The exact face kernel works in three phases per block of 256 faces:
+ *   1. every thread forms its face's predicted states (face_work) and
+ *      classifies the face's wave pattern in FP32 from the signs of
+ *      f(p_min) and f(p_max) (f increasing in p*): two rarefactions, two
+ *      shocks, or a shock on the lower-pressure side and a rarefaction on the
+ *      other (two classes, by which side that is).  Faces outside the range
+ *      where the FP32 iteration is safe, and vacuum faces, go to the queue
+ *      solved by k_group_sfaces_slow;
+ *   2. a counting sort of the block's faces by class (warp ballots, one scan
+ *      of the 4 x 8 per-warp counts) through shared memory;
+ *   3. thread t solves the block's t-th face in class order: p* by Newton in
+ *      FP32 from the reference's guess plus one FP64 Newton step (fast_root),
+ *      then the sampled half state in FP64.  A warp now takes one branch of
+ *      the per-side shock/rarefaction code in every iteration.  A face whose
+ *      FP32 iteration is refused, or whose state turns out to be a vacuum
+ *      case in FP64, goes to the queue (warp-aggregated push).
+ * Which thread solves a face changes nothing in its arithmetic, so reruns are
+ * bitwise identical. */
+constexpr int kClassRR = 0, kClassSS = 1, kClassSR = 2, kClassRS = 3, kNClass = 4;
+constexpr int kClassQueue = 4, kClassNone = 5;
+constexpr int kExactBlock = 256;
+
+template <int D>
+__device__ __forceinline__ int wave_class(const sfx_solver_params& s, const FaceWork<D>& w) {
+    const float rL = w.WL[0], pL = w.WL[D + 1];
+    const float rR = w.mirror ? rL : w.WR[0], pR = w.mirror ? pL : w.WR[D + 1];
+    constexpr float lo = 1e-12f, hi = 1e12f;
+    if(!(rL > lo && rL < hi && rR > lo && rR < hi && pL > lo && pL < hi && pR > lo && pR < hi))
+        return kClassQueue;
+    float vL = 0.f, vR = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        vL += w.WL[1 + l] * w.n[l];
+        vR += w.WR[1 + l] * w.n[l];
+    }
+    if(w.mirror) vR = -vL;
+    const float g = (float)s.gamma, tdgm1 = (float)s.tdgm1, e = (float)s.gm1d2g;
+    const float aL = sqrtf(g * pL / rL), aR = sqrtf(g * pR / rR);
+    const float dv = vR - vL;
+    /* vacuum generation (and states near it, FP32 being coarse): the queue */
+    if(!(tdgm1 * (aL + aR) > 1.0001f * dv)) return kClassQueue;
+    const bool lowL = pL <= pR;
+    const float pmin = lowL ? pL : pR, pmax = lowL ? pR : pL;
+    /* f(p_min): the lower side contributes 0, the other one rarefies */
+    const float ahi = lowL ? aR : aL;
+    const float fmin = tdgm1 * ahi * (exp2f(e * __log2f(pmin / pmax)) - 1.f) + dv;
+    if(fmin >= 0.f) return kClassRR;
+    /* f(p_max): the lower side is a shock, the other one contributes 0 */
+    const float rlo = lowL ? rL : rR;
+    const float A = (float)s.tdgp1 / rlo, B = (float)s.gm1dgp1 * pmin;
+    const float fmax = (pmax - pmin) * sqrtf(A / (pmax + B)) + dv;
+    if(fmax <= 0.f) return kClassSS;
+    return lowL ? kClassSR : kClassRS;
+}
+
+/* phase 3: p* by fast_root and the sampled half state; kDefer when the face
+ * needs the FP64 iteration or is a vacuum case, SFX_ERR_RIEMANN for an
+ * unphysical half state, SFX_OK otherwise */
+template <int D>
+__device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const FaceWork<D>& w,
+                                          SFlux<D>& F) {
+    /* a reflective right state is the left state with the normal velocity
+     * reversed: only its normal velocity enters, and of its flux only the
+     * pressure survives (face_dq) */
+    const float* WRf = w.mirror ? w.WL : w.WR;
+    double vL = 0., vR = 0.;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        vL += (double)w.WL[1 + l] * (double)w.n[l];
+        vR += (double)WRf[1 + l] * (double)w.n[l];
+    }
+    if(w.mirror) vR = -vL;
+    const double rL = w.WL[0], pL = w.WL[D + 1], rR = WRf[0], pR = WRf[D + 1];
+    const double g = s.gamma;
+    const double aL = sqrt(g * pL / rL);
+    const double aR = sqrt(g * pR / rR);
+    if(s.tdgm1 * (aL + aR) <= vR - vL) return kDefer;
+    double p, fL, fR, zL, zR;
+    if(!fast_root(s, rL, pL, rR, pR, aL, aR, vL, vR, p, fL, fR, zL, zR)) return kDefer;
+    /* sampling at x/t = 0 (ExactRiemannSolver.cpp:178-265): the side, the
+     * half state's density and pressure, and its velocity shift along n */
+    const double u = 0.5 * (vL + vR) + 0.5 * (fR - fL);
+    const bool right = u < 0.;
+    double srho = right ? rR : rL, spr = right ? pR : pL, vhalf = 0.;
+    if(right) {
+        const double r = p / pR;
+        if(p > pR) {
+            if(vR + aR * sqrt(s.gp1d2g * r + s.gm1d2g) > 0.) {
+                srho = rR * (r + s.gm1dgp1) / (s.gm1dgp1 * r + 1.);
+                spr = p;
+                vhalf = u - vR;
+            }
+        } else if(vR + aR > 0.) {
+            if(u + aR * zR <= 0.) {
+                const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
+                srho = rR * xpow(base, s.tdgm1);
+                vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
+                spr = pR * xpow(base, s.tgdgm1);
+            } else {
+                srho = rR * xpow(r, s.ginv);
+                spr = p;
+                vhalf = u - vR;
+            }
+        }
+    } else {
+        const double r = p / pL;
+        if(p > pL) {
+            if(vL - aL * sqrt(s.gp1d2g * r + s.gm1d2g) < 0.) {
+                srho = rL * (r + s.gm1dgp1) / (s.gm1dgp1 * r + 1.);
+                spr = p;
+                vhalf = u - vL;
+            }
+        } else if(vL - aL < 0.) {
+            if(u - aL * zL > 0.) {
+                const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
+                srho = rL * xpow(base, s.tdgm1);
+                vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
+                spr = pL * xpow(base, s.tgdgm1);
+            } else {
+                srho = rL * xpow(r, s.ginv);
+                spr = p;
+                vhalf = u - vL;
+            }
+        }
+    }
+    /* the half state's velocity and its flux (ExactRiemannSolver::get_flux
+     * contracted with n, :815-880) */
+    const float* Wk = right ? WRf : w.WL;
+    double hv[D], un = 0., v2 = 0.;
+    bool bad = !(srho >= 0.) || !(spr >= 0.);
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        hv[l] = (double)Wk[1 + l] + vhalf * (double)w.n[l];
+        bad |= hv[l] != hv[l];
+        un += hv[l] * (double)w.n[l];
+        v2 += hv[l] * hv[l];
+    }
+    F.m = 0.f;
+    F.P = 0.f;
+    F.E = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
+    if(srho != 0.) {
+        const double e = 0.5 * srho * v2 + spr / (g - 1.);
+        const double mf = srho * un;
+        F.m = (float)mf;
+#pragma unroll
+        for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * hv[l]);
+        F.P = (float)spr;
+        F.E = (float)((e + spr) * un);
+    }
+    return bad ? SFX_ERR_RIEMANN : SFX_OK;
+}
+
+/* queue face f of the block's mesh for the lanes with `push` set: one
+ * atomic per warp (all 32 lanes call this) */
+__device__ __forceinline__ void queue_faces(const sfx_dmesh& m, bool push, int f) {
+    const unsigned q = __ballot_sync(0xffffffffu, push);
+    if(!q) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(q) - 1;
+    int base = 0;
+    if(lane == leader) base = atomicAdd(m.slowq_n, __popc(q));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const int at = base + __popc(q & ((1u << lane) - 1u));
+    /* the queue has room for every face and each face is queued at most once
+     * per step (the gradient launch empties it); a full queue is reported */
+    if(push) {
+        if(at < m.slowq_cap)
+            m.slowq[at] = f;
+        else
+            report_face(m.err, f, SFX_ERR_INVALID);
+    }
 }
 
 /* ------------------------------- update ------------------------------- */
@@ -1350,35 +1613,189 @@ __device__ __forceinline__ bool member_done(const sfx_group_entry* tab, int mi) 
     return sl && *(volatile const int32_t*)sl <= 0;
 }
 
-template <int D, int LPC>
-__global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
-                                                     int nm) {
+template <int D, int MINB>
+__global__ void __launch_bounds__(kExactBlock, MINB)
+        k_group_sfaces_exact(const sfx_group_entry* tab, const int* pre, int nm,
+                             sfx_solver_params sp) {
+    constexpr int S = D + 2;
+    constexpr int NW = kExactBlock / 32;
+    /* the block's faces in class order: states, normals, area, limits, face id
+     * (bit 31: mirror) */
+    __shared__ float sW[2 * S][kExactBlock];
+    __shared__ float sn[D][kExactBlock];
+    __shared__ float sA[kExactBlock], sLL[kExactBlock], sLR[kExactBlock];
+    __shared__ int sf[kExactBlock];
+    __shared__ int sbase[kNClass][NW];
+    __shared__ int stotal;
     const int mi = group_mesh_of_block(pre, nm);
-    if(member_done(tab, mi)) return;
-    sgrad_body<D, LPC>(tab[mi].m, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+    if(member_done(tab, mi)) return; /* the same for every thread of the block */
+    const sfx_dmesh& m = tab[mi].m;
+    const float dt = tab[mi].dt;
+    const int f = (blockIdx.x - __ldg(pre + mi)) * kExactBlock + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    /* phase 1 (no thread leaves before the block's barriers) */
+    FaceWork<D> w;
+    int cls = kClassNone;
+    if(f < m.n_faces && !failed(m.err) &&
+       face_work<D, true>(m, (float)sp.gamma, 0.5f * dt, f, w))
+        cls = wave_class<D>(sp, w);
+    queue_faces(m, cls == kClassQueue, f);
+    /* phase 2: counting sort by class */
+    unsigned mine = 0; /* the ballot of this thread's class */
+#pragma unroll
+    for(int c = 0; c < kNClass; ++c) {
+        const unsigned b = __ballot_sync(0xffffffffu, cls == c);
+        if(lane == c) sbase[c][warp] = __popc(b);
+        if(cls == c) mine = b;
+    }
+    __syncthreads();
+    if(warp == 0) {
+        /* exclusive scan of the counts in (class, warp) order: lane l holds
+         * entry l of the 4 x 8 table */
+        const int c0 = lane / NW, w0 = lane % NW;
+        const int v = sbase[c0][w0];
+        int x = v;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if(lane >= o) x += y;
+        }
+        __syncwarp();
+        sbase[c0][w0] = x - v;
+        if(lane == 31) stotal = x;
+    }
+    __syncthreads();
+    if(cls < kNClass) {
+        const int slot = sbase[cls][warp] + __popc(mine & ((1u << lane) - 1u));
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            sW[k][slot] = w.WL[k];
+            sW[S + k][slot] = w.WR[k];
+        }
+#pragma unroll
+        for(int l = 0; l < D; ++l) sn[l][slot] = w.n[l];
+        sA[slot] = w.A;
+        sLL[slot] = w.limL;
+        sLR[slot] = w.limR;
+        sf[slot] = f | (w.mirror ? (int)kRightBit : 0);
+    }
+    __syncthreads();
+    /* phase 3 */
+    const int t = threadIdx.x;
+    bool push = false;
+    int fq = 0;
+    if(t < stotal) {
+        FaceWork<D> v;
+#pragma unroll
+        for(int k = 0; k < S; ++k) {
+            v.WL[k] = sW[k][t];
+            v.WR[k] = sW[S + k][t];
+        }
+#pragma unroll
+        for(int l = 0; l < D; ++l) v.n[l] = sn[l][t];
+        v.A = sA[t];
+        v.limL = sLL[t];
+        v.limR = sLR[t];
+        const int e = sf[t];
+        v.mirror = e < 0;
+        fq = e & 0x7fffffff;
+        SFlux<D> F;
+        const int st = exact_fast<D>(sp, v, F);
+        if(st == kDefer)
+            push = true;
+        else
+            face_dq<D>(m, dt, fq, v, F, st);
+    }
+    queue_faces(m, push, fq);
 }
 
-template <int D, int SOLVER>
-__global__ void __launch_bounds__(256, 4)
+template <int D, int LPC>
+__global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
+                                                     int nm, float gamma) {
+    const int mi = group_mesh_of_block(pre, nm);
+    if(member_done(tab, mi)) return;
+    sgrad_body<D, LPC>(tab[mi].m, gamma,
+                       (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+}
+
+template <int D, int SOLVER, int MINB>
+__global__ void __launch_bounds__(256, MINB)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
-    sfaces_body<D, SOLVER, SOLVER == SFX_SOLVER_EXACT ? kSolveDefer : kSolveInline>(
+    sfaces_body<D, SOLVER, kSolveInline>(
             tab[mi].m, sp, tab[mi].dt, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
-/* the queued exact-solver faces of every member, one per thread */
+/* The queued exact-solver faces of every member, one per thread: the FP64
+ * iteration from the reference's guess (the monotone Newton search where
+ * the reference runs Brent's method) and the vacuum cases.  Each block reads
+ * the members' queue lengths (kSlowChunk members at a time, in parallel),
+ * forms their prefix sums in shared memory and strides over the flattened
+ * list, finding a slot's member by binary search: no thread walks the
+ * member list. */
+constexpr int kSlowBlock = 128, kSlowChunk = 2048, kSlowPer = kSlowChunk / kSlowBlock;
+
 template <int D>
-__global__ void __launch_bounds__(128) k_group_sfaces_slow(const sfx_group_entry* tab, int nm,
-                                                          sfx_solver_params sp) {
-    for(int mi = 0; mi < nm; ++mi) {
-        if(member_done(tab, mi)) continue;
-        const sfx_dmesh& m = tab[mi].m;
-        const int n = min(*m.slowq_n, m.slowq_cap);
-        for(int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-            sfaces_body<D, SFX_SOLVER_EXACT, kSolveInline>(m, sp, tab[mi].dt,
-                                                            __ldg(m.slowq + j));
+__global__ void __launch_bounds__(kSlowBlock) k_group_sfaces_slow(const sfx_group_entry* tab,
+                                                                 int nm, sfx_solver_params sp) {
+    __shared__ int spre[kSlowChunk + 1];
+    __shared__ int swarp[kSlowBlock / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for(int base = 0; base < nm; base += kSlowChunk) {
+        const int cnt = min(nm - base, kSlowChunk);
+        /* thread t sums the queue lengths of members [t kSlowPer, (t+1) kSlowPer) */
+        int loc[kSlowPer];
+        int sum = 0;
+#pragma unroll
+        for(int k = 0; k < kSlowPer; ++k) {
+            const int mi = t * kSlowPer + k;
+            int c = 0;
+            if(mi < cnt && !member_done(tab, base + mi)) {
+                const sfx_dmesh& m = tab[base + mi].m;
+                c = min(*(volatile const int32_t*)m.slowq_n, m.slowq_cap);
+            }
+            loc[k] = c;
+            sum += c;
+        }
+        /* exclusive block scan of the per-thread sums */
+        int x = sum;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if(lane >= o) x += y;
+        }
+        if(lane == 31) swarp[warp] = x;
+        __syncthreads();
+        int woff = 0, total = 0;
+#pragma unroll
+        for(int w = 0; w < kSlowBlock / 32; ++w) {
+            if(w < warp) woff += swarp[w];
+            total += swarp[w];
+        }
+        int run = woff + x - sum;
+#pragma unroll
+        for(int k = 0; k < kSlowPer; ++k) {
+            spre[t * kSlowPer + k] = run;
+            run += loc[k];
+        }
+        if(t == kSlowBlock - 1) spre[kSlowChunk] = run;
+        __syncthreads();
+        for(int j = blockIdx.x * kSlowBlock + t; j < total; j += gridDim.x * kSlowBlock) {
+            int lo = 0, hi = cnt; /* the last member whose prefix is <= j */
+            while(hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if(spre[mid] <= j)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const sfx_group_entry& e = tab[base + lo];
+            sfaces_body<D, SFX_SOLVER_EXACT, kSolveInline>(e.m, sp, e.dt,
+                                                            __ldg(e.m.slowq + (j - spre[lo])));
+        }
+        __syncthreads(); /* spre and swarp are rewritten by the next chunk */
     }
 }
 
@@ -1417,17 +1834,26 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
     const int nm = g->n_meshes;
     if(phase == 0) {
         if(g->blocks[0])
-            k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm);
+            k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm,
+                                                                (float)sp->gamma);
     } else if(phase == 1) {
         if(g->blocks[1]) {
             if(sp->kind == SFX_SOLVER_EXACT) {
-                k_group_sfaces<D, SFX_SOLVER_EXACT><<<g->blocks[1], 256, 0, s>>>(
-                        g->tab, g->pre + (nm + 1), nm, *sp);
-                k_group_sfaces_slow<D><<<kSlowGroupBlocks, 128, 0, s>>>(g->tab, nm, *sp);
+                if(g->face_variant == 1)
+                    k_group_sfaces_exact<D, 3><<<g->blocks[1], kExactBlock, 0, s>>>(
+                            g->tab, g->pre + (nm + 1), nm, *sp);
+                else
+                    k_group_sfaces_exact<D, 4><<<g->blocks[1], kExactBlock, 0, s>>>(
+                            g->tab, g->pre + (nm + 1), nm, *sp);
+                k_group_sfaces_slow<D><<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
                 sfx_count_launches(1);
             } else {
-                k_group_sfaces<D, SFX_SOLVER_HLLC><<<g->blocks[1], 256, 0, s>>>(
-                        g->tab, g->pre + (nm + 1), nm, *sp);
+                if(g->face_variant == 1)
+                    k_group_sfaces<D, SFX_SOLVER_HLLC, 3><<<g->blocks[1], 256, 0, s>>>(
+                            g->tab, g->pre + (nm + 1), nm, *sp);
+                else
+                    k_group_sfaces<D, SFX_SOLVER_HLLC, 4><<<g->blocks[1], 256, 0, s>>>(
+                            g->tab, g->pre + (nm + 1), nm, *sp);
             }
         }
     } else {

@@ -204,6 +204,11 @@ class FluxPass:
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_mesh_set_lanes(self.h, lanes), "sfx_mesh_set_lanes")
 
+    def set_face_variant(self, variant: int):
+        """split pass: register cap of the face kernel (0: 64 registers, four
+        blocks per SM; 1: 80 registers, three)"""
+        L.check(L.lib().sfx_mesh_set_face_variant(self.h, variant), "sfx_mesh_set_face_variant")
+
     def set_ranges(self, grad_cells: int, flux_faces: int, update_cells: int):
         """one part of a mesh split over several devices (plain FP64):
         gradients of cells [0, grad_cells), fluxes of faces [0, flux_faces),
@@ -302,6 +307,18 @@ class Group:
 
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_group_set_lanes(self.h, lanes), "sfx_group_set_lanes")
+
+    def tune_faces(self, reps: int = 3) -> int:
+        """time the face-kernel variants on this group's meshes (a gradient
+        launch before each timed face launch; no state changes) and keep the
+        fastest; returns it"""
+        v = C.c_int32(0)
+        L.check(L.lib().sfx_group_tune_faces(self.h, reps, C.byref(v)), "sfx_group_tune_faces")
+        return v.value
+
+    def set_face_variant(self, variant: int):
+        L.check(L.lib().sfx_group_set_face_variant(self.h, variant),
+                "sfx_group_set_face_variant")
 
     def set_steps(self, steps):
         """per-member remaining step counts on the device: a member at 0 is

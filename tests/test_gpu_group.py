@@ -85,3 +85,38 @@ def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
         Qa = _alone(pr)[1]
         err = np.abs(Q - Qa).sum(0) / np.abs(Qa).sum(0)
         assert np.all(err[[0, -1]] <= 1e-6)
+
+
+@pytest.mark.parametrize("dim,solver", [(2, "Exact"), (3, "Exact"), (3, "HLLC")])
+def test_face_variants_give_the_same_result(cuda_ok, dim, solver):
+    """the face-kernel variants differ only in their register cap: every
+    variant, and the one the face tuner keeps, reproduces the default's
+    result bit for bit"""
+    from shadowfax_b200._lib import SfxError
+    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
+    sizes = [2500, 900, 4000] if dim == 2 else [2000, 1200]
+    probs = _problems(dim, solver, sizes)
+    ctx = Context(dim, RiemannSolverFactory.generate(solver), 1)
+    results = {}
+    for v in (0, 1, "tuned"):
+        members = [FluxPass(ctx, pr.mesh) for pr in probs]
+        for fp, pr in zip(members, probs):
+            fp.set_primitive(pr.W0)
+        g = Group(ctx, members, [pr.dt for pr in probs])
+        if v == "tuned":
+            Q0 = [fp.state()[1] for fp in members]
+            assert g.tune_faces(2) in (0, 1)
+            for fp, q in zip(members, Q0):          # tuning reads the states only
+                assert np.array_equal(fp.state()[1], q)
+        else:
+            g.set_face_variant(v)
+        assert np.all(g.step(probs[0].nsteps, graph=True) == 0)
+        results[v] = [fp.state()[1] for fp in members]
+        g.close()
+        for fp in members:
+            fp.close()
+    for v in (1, "tuned"):
+        for a, b in zip(results[v], results[0]):
+            np.testing.assert_array_equal(a, b)
+    with pytest.raises(SfxError):
+        Group(ctx, [FluxPass(ctx, probs[0].mesh)], [probs[0].dt]).set_face_variant(2)
