@@ -51,6 +51,8 @@ extern "C" {
 #define SFX_ERR_CLOSED 12     /* server: shut down                         */
 #define SFX_ERR_IO 14         /* mesh file missing, truncated, corrupt or of
                                  another version                            */
+#define SFX_ERR_TIMESTEP 15   /* a local time step of zero ticks ("Timestep 0!",
+                                 TimeLine.cpp:287-290)                      */
 
 /* ---- solver kinds and precision modes ---- */
 #define SFX_SOLVER_EXACT 0 /* ExactRiemannSolver, tag "EXAC" */
@@ -189,6 +191,51 @@ int sfx_state_download(sfx_mesh* mesh, double* W, double* Q);
  * global time step dt (every cell active).  Stops at the first error and
  * reports it in stats (may be NULL).  Asynchronous unless stats != NULL. */
 int sfx_step(sfx_mesh* mesh, double dt, int32_t nsteps, sfx_stats* stats);
+/* One step of a moving mesh (plain FP64 meshes that own their geometry):
+ * the generator velocities of VorCell::get_velocity from the current state
+ * (src/VorCell.cpp:966-1008), without the fluid velocity for a generator
+ * that would leave the reflective unit box within dt (periodic = 0;
+ * src/Simulation.cpp:366-398), the face velocities of VorFace::set_v
+ * (src/VorFace.cpp:586-660), the step with every face's flux computed in
+ * its moving frame, and the drift x + dt v (src/Simulation.cpp:473-481).
+ * The tessellation is then stale: `positions` ([n_cells][dim] host, may be
+ * NULL) receives the drifted generators, from which the caller builds the
+ * next face list, as the reference re-tessellates after every drift.
+ * SFX_ERR_UNSUPPORTED for split-precision meshes, clones and parts. */
+int sfx_step_moving(sfx_mesh* mesh, double dt, int32_t periodic, double* positions,
+                    sfx_stats* stats);
+
+/* ---- local (hierarchical) time steps, plain FP64 ----
+ * Every cell advances on its own step of the integer timeline: 2^60 ticks
+ * from time 0 to t_total (TimeLine, src/TimeLine.hpp:145-178).  A cell is
+ * active at tick t_now when its step starts there.
+ * sfx_mesh_set_timesteps / _get_timesteps: each cell's step [start, end)
+ * in ticks (all 0 until set; end <= 2^60).
+ * sfx_mesh_set_gradients / _get_gradients: the stored gradients
+ * [n_cells][dim][S] (an inactive cell keeps its last ones).
+ * sfx_step_window: one system step [t_now, t_next): the cells starting at
+ * t_now set their generator velocity (VorCell::get_velocity with the
+ * reflective-box check over their own step; the mesh does not move) and
+ * their gradients; every face with an active cell gets its flux over the
+ * shorter of its cells' steps, the over-flux limiter scaled by that over the
+ * longer one (VorFace.cpp:672-697, 837-866); every cell takes its faces'
+ * dQ into Q (src/Simulation.cpp:473-483); the cells whose step ends at
+ * t_next get W (src/Simulation.cpp:791-836).  Step bounds are not changed.
+ * sfx_timestep_bins: TimeLine::calculate_timestep (src/TimeLine.cpp:233-317)
+ * for the cells whose step ends at t_next: CFL step cfl h / (|v - v_gen| +
+ * c), as a power-of-two subdivision of the timeline synchronised with the
+ * cell's end and clamped to [min_step, max_step] ticks; the cell's next step
+ * starts at its end; *system_step receives the smallest new step (the next
+ * system step).  Start a run with t_next = 0 (every cell's end is 0).
+ * SFX_ERR_UNSUPPORTED for split-precision meshes and parts. */
+int sfx_mesh_set_timesteps(sfx_mesh* mesh, const uint64_t* start, const uint64_t* end);
+int sfx_mesh_get_timesteps(sfx_mesh* mesh, uint64_t* start, uint64_t* end);
+int sfx_mesh_set_gradients(sfx_mesh* mesh, const double* grad);
+int sfx_mesh_get_gradients(sfx_mesh* mesh, double* grad);
+int sfx_step_window(sfx_mesh* mesh, double t_total, uint64_t t_now, uint64_t t_next,
+                    int32_t periodic, sfx_stats* stats);
+int sfx_timestep_bins(sfx_mesh* mesh, double t_total, double cfl, uint64_t max_step,
+                      uint64_t min_step, uint64_t t_next, uint64_t* system_step);
 
 /* sfx_step with CUDA events around every phase: kernel_ms[0..2] receive
  * the summed device time (ms) of the gradient, face and update kernels over

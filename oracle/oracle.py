@@ -85,6 +85,10 @@ class Oracle:
                                C.POINTER(C.c_double)]
         L.sfxo_riemann.argtypes = [C.c_int, P[1], C.c_int, _dp, _dp, _dp, C.c_int, _dp, _dp,
                                    _ip]
+        L.sfxo_move_velocities.argtypes = [P[0], P[1], C.c_double, C.c_int, _dp, _dp, _dp]
+        _u64 = C.POINTER(C.c_uint64)
+        L.sfxo_timestep_bins.argtypes = [P[0], P[1], _dp, _dp, _u64, _u64, C.c_uint64,
+                                         C.c_double, C.c_double, C.c_uint64, C.c_uint64, _u64]
         L.sfxo_pow.argtypes = [C.c_double, C.c_double]
         L.sfxo_pow.restype = C.c_double
         L.sfxo_pow_fast.argtypes = [C.c_double, C.c_double]
@@ -157,6 +161,37 @@ class Oracle:
         return dict(W=W, Q=Q, status=rc, steps=steps.value, seconds=secs.value, grad=grad,
                     dQ=dQc)
 
+    def run_moving(self, mesh, p: Params, dt: float, W: np.ndarray, periodic: bool):
+        """one step with moving generators (the reference built without
+        -DSTATIC): generator and face velocities, the step with the fluxes in
+        the faces' frames, the drift; returns (W, Q, status, positions)"""
+        W = np.array(W, np.float64, copy=True, order="C")
+        vgen = np.empty((mesh.n_cells, mesh.dim))
+        vface = np.empty((mesh.n_faces, mesh.dim))
+        self.L.sfxo_move_velocities(C.byref(self._mesh(mesh)), C.byref(p.c()), dt,
+                                    int(periodic), _d(W), _d(vgen), _d(vface))
+        import dataclasses
+        moved = dataclasses.replace(mesh, face_velocity=vface)
+        r = self.run(moved, p, dt, 1, W)
+        pos = mesh.cell_pos + dt * vgen
+        return r["W"], r["Q"], r["status"], pos
+
+    def timestep_bins(self, mesh, p: Params, W, vgen, start, end, t_next: int, t_total: float,
+                      cfl: float, max_step: int, min_step: int):
+        """TimeLine::calculate_timestep for the cells ending at t_next:
+        returns (start, end, smallest new step, status)"""
+        W = np.ascontiguousarray(W, np.float64)
+        vgen = np.ascontiguousarray(vgen, np.float64)
+        s = np.array(start, np.uint64, copy=True, order="C")
+        e = np.array(end, np.uint64, copy=True, order="C")
+        smin = C.c_uint64(0)
+        u = C.POINTER(C.c_uint64)
+        rc = self.L.sfxo_timestep_bins(C.byref(self._mesh(mesh)), C.byref(p.c()), _d(W),
+                                       _d(vgen), s.ctypes.data_as(u), e.ctypes.data_as(u),
+                                       int(t_next), t_total, cfl, int(max_step), int(min_step),
+                                       C.byref(smin))
+        return s, e, int(smin.value), rc
+
     def riemann(self, dim: int, p: Params, WL, WR, normal, reflective: bool = False):
         WL = np.ascontiguousarray(WL, np.float64)
         WR = np.ascontiguousarray(WR, np.float64)
@@ -178,19 +213,21 @@ class Oracle:
 
 # ---------------------------------------------------------------- reference
 
-def ref_binary(dim: int, pow_kind: str = "libm") -> Path:
-    return REF_DIR / f"refharness_{dim}d_{pow_kind}"
+def ref_binary(dim: int, pow_kind: str = "libm", moving: bool = False) -> Path:
+    return REF_DIR / f"refharness_{dim}d{'_moving' if moving else ''}_{pow_kind}"
 
 
-def reference_available(dim: int = 2, pow_kind: str = "libm") -> bool:
-    return ref_binary(dim, pow_kind).exists()
+def reference_available(dim: int = 2, pow_kind: str = "libm", moving: bool = False) -> bool:
+    return ref_binary(dim, pow_kind, moving).exists()
 
 
-def _write_mesh_input(f, mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray):
+def _write_mesh_input(f, mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray,
+                      moving: bool = False, local: dict | None = None):
     m = mesh.normalized()
     f.write(b"SFXMESH1")
-    np.array([m.dim, m.n_cells, m.n_faces, m.nnz, SOLVERS[p.solver], nsteps, 0, 0],
-             np.int32).tofile(f)
+    mode = 2 if local is not None else int(moving)
+    np.array([m.dim, m.n_cells, m.n_faces, m.nnz, SOLVERS[p.solver], nsteps, mode,
+              int(m.periodic)], np.int32).tofile(f)
     np.array([p.gamma, p.tolerance, p.cutoff, dt], np.float64).tofile(f)
     vel = m.face_velocity if m.face_velocity is not None else np.zeros_like(m.face_midpoint)
     for a in (m.cell_pos, m.cell_centroid, m.cell_volume, m.cell_total_area,
@@ -198,12 +235,26 @@ def _write_mesh_input(f, mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray
               m.face_right, m.face_kind, m.face_right_pos, vel,
               np.ascontiguousarray(W0, np.float64)):
         np.ascontiguousarray(a).tofile(f)
+    if local is not None:
+        np.ascontiguousarray(local["start"], np.uint64).tofile(f)
+        np.ascontiguousarray(local["end"], np.uint64).tofile(f)
+        np.array([local["t_now"], local["t_next"]], np.uint64).tofile(f)
+        np.array([local["t_total"]], np.float64).tofile(f)
+        np.ascontiguousarray(local["grad0"], np.float64).tofile(f)
 
 
 def run_reference(mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray,
-                  pow_kind: str = "libm", timeout: float | None = None) -> dict:
-    """Run the reference CPU pass (unmodified Shadowfax sources) for nsteps."""
-    exe = ref_binary(mesh.dim, pow_kind)
+                  pow_kind: str = "libm", timeout: float | None = None,
+                  moving: bool = False, local: dict | None = None) -> dict:
+    """Run the reference CPU pass (unmodified Shadowfax sources) for nsteps.
+    moving=True: the build without -DSTATIC, one step with moving generators
+    (VorCell::get_velocity, VorFace::set_v, the drift); the result then also
+    holds the drifted generator positions ("pos").
+    local={start, end, t_now, t_next, t_total, grad0}: one system step of
+    local time steps on the 2^60-tick timeline (each particle's step bounds,
+    the stored gradients of the inactive ones); the result also holds the
+    velocities the active particles set ("vel", zero for the others)."""
+    exe = ref_binary(mesh.dim, pow_kind, moving)
     if not exe.exists():
         raise FileNotFoundError(f"{exe} not built (oracle/build.py needs the reference tree)")
     S = mesh.dim + 2
@@ -211,7 +262,7 @@ def run_reference(mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray,
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         with open(fin, "wb") as f:
-            _write_mesh_input(f, mesh, p, dt, nsteps, W0)
+            _write_mesh_input(f, mesh, p, dt, nsteps, W0, moving, local)
         subprocess.run([str(exe), fin, fout, "step"], check=True, timeout=timeout)
         raw = open(fout, "rb").read()
     hdr = np.frombuffer(raw, np.int32, 4)
@@ -222,9 +273,14 @@ def run_reference(mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray,
     W = body[o:o + n * S].reshape(n, S).copy(); o += n * S
     Q = body[o:o + n * S].reshape(n, S).copy(); o += n * S
     grad = body[o:o + n * mesh.dim * S].reshape(n, mesh.dim, S).copy(); o += n * mesh.dim * S
-    dQ = body[o:o + n * S].reshape(n, S).copy()
-    return dict(status=int(hdr[0]), steps=int(hdr[1]), seconds=secs, step_seconds=step_secs,
-                W=W, Q=Q, grad=grad, dQ=dQ)
+    dQ = body[o:o + n * S].reshape(n, S).copy(); o += n * S
+    out = dict(status=int(hdr[0]), steps=int(hdr[1]), seconds=secs, step_seconds=step_secs,
+               W=W, Q=Q, grad=grad, dQ=dQ)
+    if local is not None:
+        out["vel"] = body[o:o + n * mesh.dim].reshape(n, mesh.dim).copy(); o += n * mesh.dim
+    if moving:
+        out["pos"] = body[o:o + n * mesh.dim].reshape(n, mesh.dim).copy()
+    return out
 
 
 def riemann_reference(dim: int, p: Params, WL, WR, normal, reflective: bool = False,

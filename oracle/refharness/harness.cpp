@@ -80,6 +80,13 @@ TimeLine::TimeLine(double maxtime, double, double cfl, double,
     _iotimer = NULL;
 }
 
+/* TimeLine::set_time(unsigned long) is the other member the harness needs
+ * (local time steps start a system step at a given tick); TimeLine.cpp is
+ * not linked, so the harness supplies it: the current tick becomes `time`. */
+void TimeLine::set_time(unsigned long time) {
+    _current_time = time;
+}
+
 namespace {
 
 struct Reader {
@@ -114,7 +121,21 @@ int run_steps(Reader& in, const char* outpath) {
      * VorFace::set_v, and the drift after the update (src/Simulation.cpp:
      * 473-481).  One step per tessellation, as in the reference, where the
      * mesh is rebuilt after every drift. */
-    const int moving = hdr[6], periodic = hdr[7];
+    const int moving = hdr[6] == 1, periodic = hdr[7];
+    /* local (hierarchical) time steps: mode 2, one system step [t_now,
+     * t_next) with every particle's step bounds, and the stored gradients of
+     * the inactive ones, given in the input (the static build) */
+    const int local = hdr[6] == 2;
+#ifndef STATIC
+    if(local) {
+        fprintf(stderr, "harness: local time steps use the static build\n");
+        return 5;
+    }
+#endif
+    if(local && nsteps != 1) {
+        fprintf(stderr, "harness: local time steps take one system step\n");
+        return 5;
+    }
 #ifdef STATIC
     if(moving) {
         fprintf(stderr, "harness: moving generators need a build without -DSTATIC\n");
@@ -147,6 +168,20 @@ int run_steps(Reader& in, const char* outpath) {
     std::vector<double> frpos = in.vec<double>((size_t)nface * dim);
     std::vector<double> fvel = in.vec<double>((size_t)nface * dim);
     std::vector<double> W0 = in.vec<double>((size_t)ncell * S);
+    std::vector<uint64_t> tstart, tend;
+    std::vector<double> grad0;
+    uint64_t t_now = 0, t_next = 0;
+    double t_total = dt;
+    if(local) {
+        tstart = in.vec<uint64_t>(ncell);
+        tend = in.vec<uint64_t>(ncell);
+        uint64_t tw[2];
+        in.read(tw, 2);
+        t_now = tw[0];
+        t_next = tw[1];
+        in.read(&t_total, 1);
+        grad0 = in.vec<double>((size_t)ncell * dim * S);
+    }
 
     RiemannSolver* solver;
     if(solverkind == 0) {
@@ -169,8 +204,8 @@ int run_steps(Reader& in, const char* outpath) {
         VorGen* g = new VorGen(x[0], x[1]);
 #endif
         GasParticle* gp = new GasParticle(p);
-        gp->set_starttime(0);
-        gp->set_endtime(1ul << 60);
+        gp->set_starttime(local ? tstart[i] : 0);
+        gp->set_endtime(local ? tend[i] : 1ul << 60);
         g->set_particle(gp);
         g->set_particle_id(i);
         g->set_id(2);
@@ -245,9 +280,11 @@ int run_steps(Reader& in, const char* outpath) {
     }
 
     char dummy[64] = {0};
-    TimeLine* tl = new TimeLine(dt, dt, 0.4, 0., *(ParticleVector*)dummy,
-                                "", "", *(UnitSet*)dummy, *(UnitSet*)dummy,
-                                false, false, NULL, false, 0., 0., 0, false);
+    TimeLine* tl = new TimeLine(local ? t_total : dt, local ? t_total : dt, 0.4, 0.,
+                                *(ParticleVector*)dummy, "", "", *(UnitSet*)dummy,
+                                *(UnitSet*)dummy, false, false, NULL, false, 0., 0., 0, false);
+    if(local) tl->set_time((unsigned long)t_now);
+    std::vector<double> vel_out((size_t)ncell * dim, 0.);
 
     std::vector<double> grad_last((size_t)ncell * dim * S, 0.);
     std::vector<double> dQ_last((size_t)ncell * S, 0.);
@@ -282,10 +319,49 @@ int run_steps(Reader& in, const char* outpath) {
                 }
             }
 #endif
-            for(int i = 0; i < ncell; ++i) {
-                StateVector gradients[3];
-                cells[i]->estimate_gradient(gradients);
-                parts[i]->set_gradients(gradients);
+            if(local) {
+                /* the first kick (src/Simulation.cpp:366-398): the particles
+                 * starting a step set their velocity; then gradients of the
+                 * active particles, the stored ones of the others */
+                for(int i = 0; i < ncell; ++i) {
+                    if(parts[i]->get_starttime() != t_now) continue;
+                    StateVector Wgas = parts[i]->get_Wvec();
+                    Vec v = cells[i]->get_velocity();
+                    if(!periodic) {
+                        double dti = tl->get_realtime_interval(parts[i]->get_endtime() -
+                                                              parts[i]->get_starttime());
+                        Vec newx = parts[i]->get_position() + dti * v;
+                        bool inside = true;
+                        for(unsigned int l = 0; l < ndim_; l++)
+                            if(fabs(0.5 - newx[l]) > 1. / 2) inside = false;
+                        if(!inside) {
+                            v[0] -= Wgas[1];
+                            v[1] -= Wgas[2];
+#if ndim_ == 3
+                            v[2] -= Wgas[3];
+#endif
+                        }
+                    }
+                    parts[i]->set_velocity(v);
+                    for(int l = 0; l < dim; ++l) vel_out[(size_t)i * dim + l] = v[l];
+                }
+                for(int i = 0; i < ncell; ++i) {
+                    StateVector gradients[3];
+                    if(parts[i]->get_starttime() == t_now) {
+                        cells[i]->estimate_gradient(gradients);
+                    } else {
+                        for(int l = 0; l < dim; ++l)
+                            for(int k = 0; k < S; ++k)
+                                gradients[l][k] = grad0[((size_t)i * dim + l) * S + k];
+                    }
+                    parts[i]->set_gradients(gradients);
+                }
+            } else {
+                for(int i = 0; i < ncell; ++i) {
+                    StateVector gradients[3];
+                    cells[i]->estimate_gradient(gradients);
+                    parts[i]->set_gradients(gradients);
+                }
             }
             for(int f = 0; f < nface; ++f) {
                 faces[f]->set_v();
@@ -309,6 +385,8 @@ int run_steps(Reader& in, const char* outpath) {
                 parts[i]->update_Q();
             }
             for(int i = 0; i < ncell; ++i) {
+                /* with local steps only the particles ending their step */
+                if(local && parts[i]->get_endtime() != t_next) continue;
                 StateVector W = solver->get_W(cvol[i], parts[i]->get_Qvec());
                 parts[i]->set_W(W);
                 parts[i]->set_soundspeed(solver->get_soundspeed(W));
@@ -343,6 +421,7 @@ int run_steps(Reader& in, const char* outpath) {
     fwrite(buf.data(), sizeof(double), buf.size(), out);
     fwrite(grad_last.data(), sizeof(double), grad_last.size(), out);
     fwrite(dQ_last.data(), sizeof(double), dQ_last.size(), out);
+    if(local) fwrite(vel_out.data(), sizeof(double), vel_out.size(), out);
     if(moving) {
         /* generator positions after the drift */
         std::vector<double> pb((size_t)ncell * dim);

@@ -7,7 +7,7 @@
  * dimension restatement (each routine cites the reference file:line).
  *
  * Build: gcc -O2 -ffp-contract=off -fno-builtin -std=c99 -shared -fPIC
- * (oracle/build_oracle.sh).  -ffp-contract=off keeps every a*b+c as two
+ * (oracle/build.py).  -ffp-contract=off keeps every a*b+c as two
  * roundings, as the reference's own x86-64 build does.
  */
 #define _POSIX_C_SOURCE 200809L
@@ -70,6 +70,8 @@ double sfxo_pow_fast(double x, double y) {
 }
 
 #define opow sfxo_pow
+/* the value of M_PI in the reference's <cmath> (not defined under -std=c99) */
+#define SFXO_PI 3.14159265358979323846
 
 #define D 2
 #define FN(x) x##_2d
@@ -137,6 +139,25 @@ int sfxo_run(const sfxo_mesh* m, const sfxo_params* p, double dt, int nsteps,
     if(!dQ_last) free(dQc);
     free(dQL);
     return rc;
+}
+
+int sfxo_move_velocities(const sfxo_mesh* m, const sfxo_params* p, double dt, int periodic,
+                         const double* W, double* vgen, double* vface) {
+    if(m->dim == 3)
+        move_velocities_3d(m, p, dt, periodic, W, vgen, vface);
+    else
+        move_velocities_2d(m, p, dt, periodic, W, vgen, vface);
+    return SFXO_OK;
+}
+
+int sfxo_timestep_bins(const sfxo_mesh* m, const sfxo_params* p, const double* W,
+                       const double* vgen, uint64_t* start, uint64_t* end, uint64_t t_next,
+                       double t_total, double cfl, uint64_t max_step, uint64_t min_step,
+                       uint64_t* smin) {
+    return m->dim == 3 ? timestep_bins_3d(m, p, W, vgen, start, end, t_next, t_total, cfl,
+                                          max_step, min_step, smin)
+                       : timestep_bins_2d(m, p, W, vgen, start, end, t_next, t_total, cfl,
+                                          max_step, min_step, smin);
 }
 
 int sfxo_riemann(int dim, const sfxo_params* p, int n, const double* WL,

@@ -13,6 +13,8 @@
 #ifndef SFX_ORACLE_H
 #define SFX_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -63,6 +65,17 @@ int sfxo_apply(const sfxo_mesh* m, const sfxo_params* p, const double* dQL,
 int sfxo_run(const sfxo_mesh* m, const sfxo_params* p, double dt, int nsteps,
              double* W, double* Q, double* grad_last, double* dQ_last,
              int* steps_done, double* seconds);
+/* local time steps: new steps of the cells ending at t_next
+ * (TimeLine::calculate_timestep); returns 0 or 15 (a zero step) */
+int sfxo_timestep_bins(const sfxo_mesh* m, const sfxo_params* p, const double* W,
+                       const double* vgen, uint64_t* start, uint64_t* end, uint64_t t_next,
+                       double t_total, double cfl, uint64_t max_step, uint64_t min_step,
+                       uint64_t* smin);
+/* moving generators: generator velocities [ncell][dim] (VorCell::get_velocity
+ * with the reflective-box check) and face velocities [nface][dim]
+ * (VorFace::set_v) from the state W */
+int sfxo_move_velocities(const sfxo_mesh* m, const sfxo_params* p, double dt, int periodic,
+                         const double* W, double* vgen, double* vface);
 int sfxo_riemann(int dim, const sfxo_params* p, int n, const double* WL,
                  const double* WR, const double* normal, int reflective,
                  double* half, double* flux, int* code);

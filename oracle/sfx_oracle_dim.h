@@ -1314,4 +1314,144 @@ static int FN(riemann)(const sfxo_params* p, int n, const double* WLa,
     return worst;
 }
 
+
+/* ---- moving generators (the reference built without -DSTATIC) ----
+ * Generator velocities: VorCell::get_velocity (src/VorCell.cpp:966-1008)
+ * from the state W and the stored sound speed sqrt(gamma p / rho), then the
+ * reflective-box check of src/Simulation.cpp:366-398 (a generator that would
+ * leave the unit box, RectangularBox::inside, src/RectangularBox.cpp:91-99,
+ * loses the fluid velocity).  Face velocities: VorFace::set_v
+ * (src/VorFace.cpp:586-660).  vgen [ncell][D], vface [nface][D]. */
+static void FN(move_velocities)(const sfxo_mesh* m, const sfxo_params* p, double dt,
+                                int periodic, const double* Wall, double* vgen,
+                                double* vface) {
+    for(int i = 0; i < m->ncell; ++i) {
+        const double* W = Wall + (size_t)i * S;
+        const double* x = m->cell_pos + (size_t)i * D;
+        double vel[D];
+        for(int l = 0; l < D; ++l) vel[l] = 0.;
+        if(W[0]) {
+            double d[D];
+            for(int l = 0; l < D; ++l) d[l] = m->cell_centroid[(size_t)i * D + l] - x[l];
+            double Ri = m->cell_volume[i];
+            double csnd = sqrt(p->gamma * W[D + 1] / W[0]);
+#if D == 3
+            Ri = sfx_cbrt(3. * Ri / 4. / SFXO_PI);
+            double dn = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+#else
+            Ri = sqrt(Ri / SFXO_PI);
+            double dn = sqrt(d[0] * d[0] + d[1] * d[1]);
+#endif
+            double check = 4. * dn / Ri;
+            if(check > 0.9) {
+                if(check < 1.1) {
+                    double fac = csnd / dn * (dn - 0.9 * 0.25 * Ri) / (0.2 * 0.25 * Ri);
+                    for(int l = 0; l < D; ++l) vel[l] = fac * d[l];
+                } else {
+                    double fac = csnd / dn;
+                    for(int l = 0; l < D; ++l) vel[l] = fac * d[l];
+                }
+            }
+        }
+        double v[D];
+        for(int l = 0; l < D; ++l) v[l] = W[1 + l] + vel[l];
+        if(W[0] < 1.e-10) {
+            double fac = W[0] * 1.e10;
+            for(int l = 0; l < D; ++l) v[l] = fac * v[l];
+        }
+        if(!periodic) {
+            int inside = 1;
+            for(int l = 0; l < D; ++l)
+                if(fabs(0.5 - (x[l] + dt * v[l])) > 0.5) inside = 0;
+            if(!inside)
+                for(int l = 0; l < D; ++l) v[l] -= W[1 + l];
+        }
+        for(int l = 0; l < D; ++l) vgen[(size_t)i * D + l] = v[l];
+    }
+    for(int f = 0; f < m->nface; ++f) {
+        const int L = m->face_left[f];
+        const double* xl = m->cell_pos + (size_t)L * D;
+        const double* xr = m->face_right_pos + (size_t)f * D;
+        const double* mid = m->face_midpoint + (size_t)f * D;
+        const double* vl = vgen + (size_t)L * D;
+        double vr[D];
+        double* out = vface + (size_t)f * D;
+        if(m->face_kind[f] != 2) {
+            for(int l = 0; l < D; ++l) vr[l] = vgen[(size_t)m->face_right[f] * D + l];
+        } else {
+#if D == 3
+            for(int l = 0; l < D; ++l) out[l] = 0.;
+            continue;
+#else
+            double Wd[4] = {0., vl[0], vl[1], 0.};
+            FN(mirror_state)(Wd, xl, xr);
+            vr[0] = Wd[1];
+            vr[1] = Wd[2];
+#endif
+        }
+        double rRL[D + 1];
+        for(int l = 0; l < D; ++l) rRL[l] = xr[l] - xl[l];
+#if D == 3
+        rRL[3] = rRL[0] * rRL[0] + rRL[1] * rRL[1] + rRL[2] * rRL[2];
+#else
+        rRL[2] = rRL[0] * rRL[0] + rRL[1] * rRL[1];
+#endif
+        double fac = (vl[0] - vr[0]) * (mid[0] - 0.5 * (xl[0] + xr[0]));
+        for(int l = 1; l < D; ++l) fac += (vl[l] - vr[l]) * (mid[l] - 0.5 * (xl[l] + xr[l]));
+        fac /= rRL[D];
+        for(int l = 0; l < D; ++l) out[l] = 0.5 * (vl[l] + vr[l]) + fac * rRL[l];
+    }
+}
+
+/* ---- local time steps: TimeLine::calculate_timestep (src/TimeLine.cpp:
+ * 233-317) for the gas cells whose step ends at t_next, on the timeline of
+ * 2^60 ticks spanning t_total: h (VorCell::get_h, src/VorCell.cpp:948-956),
+ * the CFL step h / (|v - v_gen| + c), S = cfl x that; max_step when that is
+ * shorter than S, otherwise the largest power-of-two number of ticks not
+ * longer than S, halved until 2^60 - end is a multiple of it, clamped to
+ * [min_step, max_step]; the cell's next step is [end, end + step).  *smin
+ * receives the smallest new step (max_step when no cell ends at t_next). */
+static int FN(timestep_bins)(const sfxo_mesh* m, const sfxo_params* p, const double* Wall,
+                             const double* vgen, uint64_t* start, uint64_t* end,
+                             uint64_t t_next, double t_total, double cfl, uint64_t max_step,
+                             uint64_t min_step, uint64_t* smin) {
+    const uint64_t ticks = (uint64_t)1 << 60;
+    uint64_t best = max_step;
+    for(int i = 0; i < m->ncell; ++i) {
+        if(end[i] != t_next) continue;
+        const double* W = Wall + (size_t)i * S;
+        const double V = m->cell_volume[i];
+#if D == 3
+        const double h = sfx_cbrt(V * 3. / 4. / SFXO_PI);
+#else
+        const double h = sqrt(V / SFXO_PI);
+#endif
+        double v[D];
+        for(int l = 0; l < D; ++l) v[l] = W[1 + l] - vgen[(size_t)i * D + l];
+#if D == 3
+        const double vi = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#else
+        const double vi = sqrt(v[0] * v[0] + v[1] * v[1]);
+#endif
+        const double ci = W[0] ? sqrt(p->gamma * W[D + 1] / W[0]) : 0.;
+        const double Sreal = cfl * (h / (vi + ci));
+        uint64_t S2;
+        if(t_total * ((double)max_step / (double)ticks) < Sreal) {
+            S2 = max_step;
+        } else {
+            S2 = ticks;
+            while(S2 && t_total * ((double)S2 / (double)ticks) > Sreal) S2 >>= 1;
+            if(!S2) return 15; /* SFX_ERR_TIMESTEP */
+            while((ticks - end[i]) % S2) S2 >>= 1;
+            if(S2 < min_step) S2 = min_step;
+            if(S2 > max_step) S2 = max_step;
+        }
+        start[i] = end[i];
+        end[i] = end[i] + S2;
+        if(S2 < best) best = S2;
+    }
+    *smin = best;
+    return SFXO_OK;
+}
+
 #undef S

@@ -20,12 +20,12 @@ STATUS_NAMES = {
     4: "SFX_ERR_NAN_FLUX", 5: "SFX_ERR_NEG_STATE", 6: "SFX_ERR_NOCONV",
     7: "SFX_ERR_BOUNDS", 8: "SFX_ERR_UNSUPPORTED", 9: "SFX_ERR_MESH",
     10: "SFX_ERR_NOMEM", 11: "SFX_ERR_NOT_READY", 12: "SFX_ERR_CLOSED",
-    13: "SFX_ERR_TOO_LARGE", 14: "SFX_ERR_IO",
+    13: "SFX_ERR_TOO_LARGE", 14: "SFX_ERR_IO", 15: "SFX_ERR_TIMESTEP",
 }
 SFX_ERR_INVALID, SFX_ERR_CUDA, SFX_ERR_RIEMANN, SFX_ERR_NAN_FLUX = 1, 2, 3, 4
 SFX_ERR_NEG_STATE, SFX_ERR_NOCONV, SFX_ERR_BOUNDS, SFX_ERR_UNSUPPORTED = 5, 6, 7, 8
 SFX_ERR_MESH, SFX_ERR_NOMEM, SFX_ERR_NOT_READY, SFX_ERR_CLOSED = 9, 10, 11, 12
-SFX_ERR_TOO_LARGE, SFX_ERR_IO = 13, 14
+SFX_ERR_TOO_LARGE, SFX_ERR_IO, SFX_ERR_TIMESTEP = 13, 14, 15
 
 SOLVER_EXACT, SOLVER_HLLC = 0, 1
 PREC_FP64, PREC_SPLIT = 0, 1
@@ -52,6 +52,7 @@ class sfx_config(C.Structure):
 
 
 _dp = C.POINTER(C.c_double)
+_u64p = C.POINTER(C.c_uint64)
 _ip = C.POINTER(C.c_int32)
 
 
@@ -135,6 +136,15 @@ PROTOTYPES = {
                                     _ip, _ip, _dp, _dp]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_mesh_set_face_variant": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sfx_step_moving": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, _dp, C.c_void_p]),
+    "sfx_mesh_set_timesteps": (C.c_int, [C.c_void_p, _u64p, _u64p]),
+    "sfx_mesh_get_timesteps": (C.c_int, [C.c_void_p, _u64p, _u64p]),
+    "sfx_mesh_set_gradients": (C.c_int, [C.c_void_p, _dp]),
+    "sfx_mesh_get_gradients": (C.c_int, [C.c_void_p, _dp]),
+    "sfx_step_window": (C.c_int, [C.c_void_p, C.c_double, C.c_uint64, C.c_uint64, C.c_int32,
+                                  C.c_void_p]),
+    "sfx_timestep_bins": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_uint64, C.c_uint64,
+                                    C.c_uint64, C.POINTER(C.c_uint64)]),
     "sfx_mesh_set_ranges": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sfx_mesh_pack_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                       C.c_void_p]),

@@ -36,6 +36,8 @@ struct sfx_mesh {
     sfx_group_entry* self_tab = nullptr;
     int32_t* self_pre = nullptr;
     float self_dt = 0.f; /* time step held in self_tab (0: none yet) */
+    bool clone = false;  /* geometry shared with the base mesh */
+    unsigned long long* d_smin = nullptr; /* local time steps: smallest new step */
 };
 
 namespace {
@@ -180,6 +182,10 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     m->ctx = ctx;
     ctx->live_meshes++;
     m->d = b; /* geometry pointers shared with the base */
+    m->clone = true;
+    m->d.vgen = m->d.newpos = nullptr;
+    m->d.tstart = m->d.tend = nullptr;
+    m->d_smin = nullptr;
     sfx_dmesh& d = m->d;
     const int64_t n = d.n_cells, F = d.n_faces;
     const int S = d.S, dim = d.dim;
@@ -187,7 +193,7 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     d.branch = nullptr;
     d.err = nullptr;
     d.totals_scratch = nullptr;
-    d.cw = d.cg = nullptr;
+    d.cw = d.cg = d.cdw = nullptr;
     d.dqm = nullptr;
     d.dqv = nullptr;
     d.slowq = nullptr;
@@ -206,6 +212,7 @@ int clone_impl(sfx_ctx* ctx, sfx_mesh* base, cudaStream_t s, bool wait, sfx_mesh
     if(split) {
         A(&d.cw, 2 * n);
         A(&d.cg, (size_t)sfx_split_grad_vec4(dim) * n);
+        A(&d.cdw, (size_t)sfx_split_dwdt_vec4(dim) * n);
         A(&d.dqm, F);
         A(&d.dqv, (size_t)dim * F);
         d.slowq_cap = slowq_capacity(F);
@@ -362,7 +369,8 @@ int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
     if(precision == SFX_PREC_SPLIT) {
         /* fg, fi, fsh, an, dqm, dqv, queue; cw, cg, cx, self table; nbe */
         bytes += F * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + 4 * slowq_capacity(F) + 4;
-        bytes += n * (32 + 16 * sfx_split_grad_vec4((int)dim) + 16) + 256;
+        bytes += n * (32 + 16 * (sfx_split_grad_vec4((int)dim) + sfx_split_dwdt_vec4((int)dim)) +
+                      16) + 256;
         bytes += nnz * 4;
     }
     return bytes;
@@ -536,6 +544,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         A(&d.fsh, F);
         A(&d.cw, 2 * n);
         A(&d.cg, (size_t)sfx_split_grad_vec4(dim) * n);
+        A(&d.cdw, (size_t)sfx_split_dwdt_vec4(dim) * n);
         A(&d.cx, n);
         A(&d.nbe, nnz);
         A(&d.an, (size_t)dim * F);
@@ -674,6 +683,167 @@ int sfx_step(sfx_mesh* m, double dt, int32_t nsteps, sfx_stats* st) {
     return rc != SFX_OK ? rc : rt;
 }
 
+int sfx_step_moving(sfx_mesh* m, double dt, int32_t periodic, double* positions,
+                    sfx_stats* st) {
+    if(!m || !(dt > 0.)) return SFX_ERR_INVALID;
+    sfx_ctx* c = m->ctx;
+    if(c->cfg.precision != SFX_PREC_FP64 || m->clone || m->d.ranged) return SFX_ERR_UNSUPPORTED;
+    cudaStream_t s = c->stream;
+    sfx_dmesh& d = m->d;
+    const int64_t n = d.n_cells, F = d.n_faces;
+    const int D = d.dim;
+    if(!d.vgen) SFX_TRY(dalloc(m, &d.vgen, (size_t)D * n));
+    if(!d.newpos) SFX_TRY(dalloc(m, &d.newpos, (size_t)D * n));
+    if(!d.vel) SFX_TRY(dalloc(m, &d.vel, (size_t)D * (F > 0 ? F : 1)));
+    d.has_velocity = 1;
+    SFX_TRY(reset_err(m));
+    SFX_TRY(sfx_fp64_move_velocities(&d, c->cfg.gamma, dt, periodic ? 1 : 0, 1, s));
+    for(int ph = 0; ph < 3; ++ph) SFX_TRY(run_phase(m, ph, dt, 0, s));
+    SFX_TRY(sfx_fp64_drift(&d, dt, s));
+    if(positions) {
+        std::vector<double> t((size_t)D * n);
+        SFX_TRY(cuda_ok(cudaMemcpyAsync(t.data(), d.newpos, sizeof(double) * t.size(),
+                                        cudaMemcpyDeviceToHost, s)));
+        SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+        transpose_out(t, n, D, positions);
+    }
+    sfx_stats local;
+    sfx_stats* out = st ? st : &local;
+    std::memset(out, 0, sizeof *out);
+    int rc = check_err(m, out);
+    out->steps_done = rc == SFX_OK ? 1 : -1;
+    int rt = sfx_fp64_totals(&m->d, out->totals, s);
+    return rc != SFX_OK ? rc : rt;
+}
+
+/* local time steps: per-cell integer step bounds and generator velocities
+ * (all zero at first) */
+static int ensure_local(sfx_mesh* m) {
+    sfx_dmesh& d = m->d;
+    cudaStream_t s = m->ctx->stream;
+    const size_t n = (size_t)d.n_cells;
+    if(!d.tstart) {
+        SFX_TRY(dalloc(m, &d.tstart, n));
+        SFX_TRY(dalloc(m, &d.tend, n));
+        SFX_TRY(cuda_ok(cudaMemsetAsync(d.tstart, 0, sizeof(uint64_t) * n, s)));
+        SFX_TRY(cuda_ok(cudaMemsetAsync(d.tend, 0, sizeof(uint64_t) * n, s)));
+    }
+    if(!d.vgen) {
+        SFX_TRY(dalloc(m, &d.vgen, (size_t)d.dim * n));
+        SFX_TRY(cuda_ok(cudaMemsetAsync(d.vgen, 0, sizeof(double) * d.dim * n, s)));
+    }
+    if(!m->d_smin) SFX_TRY(dalloc(m, &m->d_smin, 1));
+    return SFX_OK;
+}
+
+static bool local_ok(const sfx_mesh* m) {
+    return m->ctx->cfg.precision == SFX_PREC_FP64 && !m->d.ranged;
+}
+
+int sfx_mesh_set_timesteps(sfx_mesh* m, const uint64_t* start, const uint64_t* end) {
+    if(!m || !start || !end) return SFX_ERR_INVALID;
+    if(!local_ok(m)) return SFX_ERR_UNSUPPORTED;
+    const int64_t n = m->d.n_cells;
+    for(int64_t i = 0; i < n; ++i)
+        if(end[i] < start[i] || end[i] > SFX_TIMELINE_TICKS) return SFX_ERR_INVALID;
+    SFX_TRY(ensure_local(m));
+    cudaStream_t s = m->ctx->stream;
+    SFX_TRY(h2d(m->d.tstart, start, (size_t)n, s));
+    SFX_TRY(h2d(m->d.tend, end, (size_t)n, s));
+    return cuda_ok(cudaStreamSynchronize(s));
+}
+
+int sfx_mesh_get_timesteps(sfx_mesh* m, uint64_t* start, uint64_t* end) {
+    if(!m || !start || !end) return SFX_ERR_INVALID;
+    if(!local_ok(m)) return SFX_ERR_UNSUPPORTED;
+    SFX_TRY(ensure_local(m));
+    cudaStream_t s = m->ctx->stream;
+    const size_t n = (size_t)m->d.n_cells;
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(start, m->d.tstart, sizeof(uint64_t) * n,
+                                    cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(end, m->d.tend, sizeof(uint64_t) * n,
+                                    cudaMemcpyDeviceToHost, s)));
+    return cuda_ok(cudaStreamSynchronize(s));
+}
+
+int sfx_mesh_set_gradients(sfx_mesh* m, const double* grad) {
+    if(!m || !grad) return SFX_ERR_INVALID;
+    if(m->ctx->cfg.precision != SFX_PREC_FP64 || !m->d.grad) return SFX_ERR_UNSUPPORTED;
+    const int64_t n = m->d.n_cells;
+    const int w = m->d.dim * m->d.S;
+    std::vector<double> t;
+    transpose_in(grad, n, w, t);
+    cudaStream_t s = m->ctx->stream;
+    SFX_TRY(h2d(m->d.grad, t.data(), t.size(), s));
+    return cuda_ok(cudaStreamSynchronize(s));
+}
+
+int sfx_mesh_get_gradients(sfx_mesh* m, double* grad) {
+    if(!m || !grad) return SFX_ERR_INVALID;
+    if(m->ctx->cfg.precision != SFX_PREC_FP64 || !m->d.grad) return SFX_ERR_UNSUPPORTED;
+    const int64_t n = m->d.n_cells;
+    const int w = m->d.dim * m->d.S;
+    std::vector<double> t((size_t)n * w);
+    cudaStream_t s = m->ctx->stream;
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(t.data(), m->d.grad, sizeof(double) * t.size(),
+                                    cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+    transpose_out(t, n, w, grad);
+    return SFX_OK;
+}
+
+int sfx_step_window(sfx_mesh* m, double t_total, uint64_t t_now, uint64_t t_next,
+                    int32_t periodic, sfx_stats* st) {
+    if(!m || !(t_total > 0.) || t_next <= t_now || t_next > SFX_TIMELINE_TICKS)
+        return SFX_ERR_INVALID;
+    if(!local_ok(m)) return SFX_ERR_UNSUPPORTED;
+    SFX_TRY(ensure_local(m));
+    sfx_ctx* c = m->ctx;
+    cudaStream_t s = c->stream;
+    sfx_dmesh& d = m->d;
+    d.local = 1;
+    d.t_now = t_now;
+    d.t_next = t_next;
+    d.t_total = t_total;
+    int rc = reset_err(m);
+    /* the cells starting a step set their generator velocity (the mesh stays) */
+    if(!rc) rc = sfx_fp64_move_velocities(&d, c->cfg.gamma, 0., periodic ? 1 : 0, 0, s);
+    for(int ph = 0; ph < 3 && !rc; ++ph) rc = run_phase(m, ph, 1., 0, s);
+    d.local = 0;
+    if(rc) return rc;
+    sfx_stats local;
+    sfx_stats* out = st ? st : &local;
+    std::memset(out, 0, sizeof *out);
+    rc = check_err(m, out);
+    out->steps_done = rc == SFX_OK ? 1 : -1;
+    int rt = sfx_fp64_totals(&m->d, out->totals, s);
+    return rc != SFX_OK ? rc : rt;
+}
+
+int sfx_timestep_bins(sfx_mesh* m, double t_total, double cfl, uint64_t max_step,
+                      uint64_t min_step, uint64_t t_next, uint64_t* system_step) {
+    if(!m || !(t_total > 0.) || !(cfl > 0.) || max_step == 0 || max_step > SFX_TIMELINE_TICKS ||
+       min_step > max_step || !system_step)
+        return SFX_ERR_INVALID;
+    if(!local_ok(m)) return SFX_ERR_UNSUPPORTED;
+    SFX_TRY(ensure_local(m));
+    sfx_ctx* c = m->ctx;
+    cudaStream_t s = c->stream;
+    sfx_dmesh& d = m->d;
+    d.t_next = t_next;
+    d.t_total = t_total;
+    SFX_TRY(reset_err(m));
+    const unsigned long long smax = max_step;
+    SFX_TRY(h2d(m->d_smin, &smax, 1, s));
+    SFX_TRY(sfx_fp64_timestep_bins(&d, c->cfg.gamma, cfl, max_step, min_step, m->d_smin, s));
+    unsigned long long out = 0;
+    SFX_TRY(cuda_ok(cudaMemcpyAsync(&out, m->d_smin, sizeof out, cudaMemcpyDeviceToHost, s)));
+    SFX_TRY(cuda_ok(cudaStreamSynchronize(s)));
+    SFX_TRY(check_err(m, nullptr));
+    *system_step = out;
+    return SFX_OK;
+}
+
 int sfx_step_timed(sfx_mesh* m, double dt, int32_t nsteps, float* kernel_ms,
                    int32_t* launches) {
     if(!m || nsteps < 0 || !(dt > 0.) || !kernel_ms) return SFX_ERR_INVALID;
@@ -798,7 +968,8 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision) {
     const int64_t n = b.n_cells, F = b.n_faces, S = b.S, D = b.dim;
     int64_t bytes = n * S * 16 + (S + 1) * 1024 * 8 + 64;
     if(precision == SFX_PREC_SPLIT)
-        bytes += n * 32 + n * 16 * sfx_split_grad_vec4((int)D) + F * 8 + F * D * 8 +
+        bytes += n * 32 + n * 16 * (sfx_split_grad_vec4((int)D) + sfx_split_dwdt_vec4((int)D)) +
+                 F * 8 + F * D * 8 +
                  4 * (int64_t)slowq_capacity(F) + 4 + (int64_t)sizeof(sfx_group_entry) + 24;
     else
         bytes += n * D * S * 8 + F * 4 +

@@ -187,6 +187,8 @@ __global__ void __launch_bounds__(128) k_gradients(sfx_dmesh m) {
     constexpr int S = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= sfx_grad_cells(m) || failed(m.err)) return;
+    /* local time steps: an inactive cell keeps its gradients (src/Simulation.cpp:414-420) */
+    if(m.local && m.tstart[i] != m.t_now) return;
     const int n = m.n_cells, F = m.n_faces;
     double W[S], xi[D], Wmax[S], Wmin[S], delta[D][S];
 #pragma unroll
@@ -359,6 +361,7 @@ __global__ void __launch_bounds__(kGradBlock, 8) k_grad_sum(sfx_dmesh m) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (int)(t / S), k = (int)(t % S);
     if(i >= sfx_grad_cells(m) || failed(m.err)) return;
+    if(m.local && m.tstart[i] != m.t_now) return;
     const int n = m.n_cells, F = m.n_faces;
     const double W = m.W[(size_t)k * n + i];
     double delta[D];
@@ -1088,6 +1091,27 @@ __global__ void __launch_bounds__(128) k_faces(sfx_dmesh m, sfx_solver_params sp
     const int kind = m.kind[f];
     const bool has_right = kind != SFX_FACE_MIRROR;
     const int iR = has_right ? m.right[f] : 0;
+    /* local time steps (VorFace.cpp:672-697): a face is computed when its
+     * left cell is active, or (with a right cell) either cell is; its time
+     * step is the shorter of the two cells' steps */
+    double dtmax = dt;
+    if(m.local) {
+        const bool aL = m.tstart[iL] == m.t_now;
+        const bool aR = has_right && m.tstart[iR] == m.t_now;
+        if(!aL && !aR) {
+#pragma unroll
+            for(int k = 0; k < S; ++k) m.dQf[(size_t)k * F + f] = 0.;
+            if(write_branch) m.branch[f] = SFX_BRANCH_SKIPPED;
+            return;
+        }
+        dt = sfx_realtime(m.t_total, m.tend[iL] - m.tstart[iL]);
+        dtmax = dt;
+        if(has_right) {
+            const double dtR = sfx_realtime(m.t_total, m.tend[iR] - m.tstart[iR]);
+            dt = fmin(dt, dtR);
+            dtmax = fmax(dtmax, dtR);
+        }
+    }
     double v[D], mid[D], xL[D], xRi[D], cenL[D];
 #pragma unroll
     for(int l = 0; l < D; ++l) {
@@ -1181,9 +1205,10 @@ __global__ void __launch_bounds__(128) k_faces(sfx_dmesh m, sfx_solver_params sp
         dQL[k] = dt * A * flux[k];
         dQR[k] = -dt * A * flux[k];
     }
-    /* over-flux limiter (VorFace.cpp:837-866); one global dt, timefac = dt/dt */
+    /* over-flux limiter (VorFace.cpp:837-866): timefac = dt / (the longer
+     * of the two cells' steps); dt / dt with one global step */
     double timefac = 1.;
-    if(has_right) timefac = dt / dt;
+    if(has_right) timefac = dt / dtmax;
     double areafac = A / m.tarea[iL];
     areafac = areafac * timefac;
     const double QLm = m.Q[iL];
@@ -1271,6 +1296,14 @@ __global__ void __launch_bounds__(128) k_apply(sfx_dmesh m, double gamma) {
     for(int k = 0; k < S; ++k) Q[k] = m.Q[(size_t)k * n + i] - dQ[k];
     if(Q[0] < 0. || Q[D + 1] < 0.) {
         report_cell(m.err, i, SFX_ERR_NEG_STATE);
+        return;
+    }
+    if(m.local && m.tend[i] != m.t_next) {
+        /* local time steps: a cell in the middle of its step takes the flux
+         * of its active neighbours into Q; its W waits for the end of its
+         * step (src/Simulation.cpp:791-836) */
+#pragma unroll
+        for(int k = 0; k < S; ++k) m.Q[(size_t)k * n + i] = Q[k];
         return;
     }
     get_W<D>(gamma, m.vol[i], Q, W);
@@ -1426,6 +1459,238 @@ inline int cuda_status(cudaError_t e) {
     return e == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
 }
 
+/* --------------------------- moving generators ---------------------------
+ * One step of a moving mesh (a build of the reference without -DSTATIC):
+ * every generator gets the velocity of VorCell::get_velocity
+ * (src/VorCell.cpp:966-1008: the fluid velocity plus a term that steers the
+ * generator towards its cell's centroid, at the sound speed when the offset
+ * exceeds 1/4 of the cell radius, ramped in between; suppressed linearly
+ * below density 1e-10), without the fluid velocity when a reflective unit
+ * box would be left within dt (src/Simulation.cpp:366-398, RectangularBox::
+ * inside); every face the velocity of VorFace::set_v
+ * (src/VorFace.cpp:586-660: the mean of its generators' velocities plus the
+ * part that keeps the face between them; a 3D mirror face does not move, a
+ * 2D mirror generator moves as the mirror image of its cell's generator);
+ * after the update the generators drift, x + dt v (Particle::drift,
+ * src/utilities/Particle.cpp:281-283).  Same IEEE operations in the same
+ * order as the reference, cube roots by sfx_cbrt. */
+constexpr double kPi = 3.14159265358979323846;
+
+template <int D>
+__global__ void __launch_bounds__(128) k_gen_velocity(sfx_dmesh m, double gamma, double dt,
+                                                      int periodic) {
+    constexpr int S = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    /* local time steps: only the cells starting a step set their velocity
+     * (the first kick of src/Simulation.cpp:366-398) */
+    if(m.local && m.tstart[i] != m.t_now) return;
+    const int n = m.n_cells;
+    double W[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) W[k] = m.W[(size_t)k * n + i];
+    double vel[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l) vel[l] = 0.;
+    if(W[0] != 0.) {
+        double d[D];
+#pragma unroll
+        for(int l = 0; l < D; ++l) d[l] = m.cen[(size_t)l * n + i] - m.pos[(size_t)l * n + i];
+        double Ri = m.vol[i];
+        /* GasParticle::get_soundspeed: the solver's sqrt(gamma p / rho) */
+        const double csnd = sqrt(gamma * W[D + 1] / W[0]);
+        if(D == 3)
+            Ri = sfx_cbrt(3. * Ri / 4. / kPi);
+        else
+            Ri = sqrt(Ri / kPi);
+        const double dn = norm<D>(d);
+        const double check = 4. * dn / Ri;
+        if(check > 0.9) {
+            double fac;
+            if(check < 1.1)
+                fac = csnd / dn * (dn - 0.9 * 0.25 * Ri) / (0.2 * 0.25 * Ri);
+            else
+                fac = csnd / dn;
+#pragma unroll
+            for(int l = 0; l < D; ++l) vel[l] = fac * d[l];
+        }
+    }
+    double v[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l) v[l] = W[1 + l] + vel[l];
+    if(W[0] < 1.e-10) {
+        const double fac = W[0] * 1.e10;
+#pragma unroll
+        for(int l = 0; l < D; ++l) v[l] = fac * v[l];
+    }
+    if(!periodic) {
+        /* with local time steps, the cell's own step
+         * (get_realtime_interval(end - start)) */
+        const double dti = m.local ? sfx_realtime_interval(m.t_total, m.tend[i] - m.tstart[i]) : dt;
+        bool inside = true;
+#pragma unroll
+        for(int l = 0; l < D; ++l) {
+            const double nx = m.pos[(size_t)l * n + i] + dti * v[l];
+            if(fabs(0.5 - nx) > 0.5) inside = false;
+        }
+        if(!inside) {
+#pragma unroll
+            for(int l = 0; l < D; ++l) v[l] -= W[1 + l];
+        }
+    }
+#pragma unroll
+    for(int l = 0; l < D; ++l) m.vgen[(size_t)l * n + i] = v[l];
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_face_velocity(sfx_dmesh m) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= m.n_faces) return;
+    const int n = m.n_cells, F = m.n_faces;
+    const int iL = m.left[f];
+    const int kind = m.kind[f];
+    double xl[D], xr[D], mid[D], vl[D], vr[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        xl[l] = m.pos[(size_t)l * n + iL];
+        xr[l] = m.rpos[(size_t)l * F + f];
+        mid[l] = m.mid[(size_t)l * F + f];
+        vl[l] = m.vgen[(size_t)l * n + iL];
+    }
+    if(kind != SFX_FACE_MIRROR) {
+        const int iR = m.right[f];
+#pragma unroll
+        for(int l = 0; l < D; ++l) vr[l] = m.vgen[(size_t)l * n + iR];
+    } else if(D == 3) {
+#pragma unroll
+        for(int l = 0; l < D; ++l) m.vel[(size_t)l * F + f] = 0.;
+        return;
+    } else {
+        double Wd[4] = {0., vl[0], vl[1], 0.};
+        mirror_state<2>(Wd, xl, xr);
+        vr[0] = Wd[1];
+        vr[1] = Wd[2];
+    }
+    double rRL[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l) rRL[l] = xr[l] - xl[l];
+    double r2 = rRL[0] * rRL[0] + rRL[1] * rRL[1];
+    if(D == 3) r2 = r2 + rRL[2] * rRL[2];
+    double fac = (vl[0] - vr[0]) * (mid[0] - 0.5 * (xl[0] + xr[0]));
+#pragma unroll
+    for(int l = 1; l < D; ++l) fac += (vl[l] - vr[l]) * (mid[l] - 0.5 * (xl[l] + xr[l]));
+    fac /= r2;
+#pragma unroll
+    for(int l = 0; l < D; ++l) m.vel[(size_t)l * F + f] = 0.5 * (vl[l] + vr[l]) + fac * rRL[l];
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_drift(sfx_dmesh m, double dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    const int n = m.n_cells;
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+        m.newpos[(size_t)l * n + i] = m.pos[(size_t)l * n + i] + dt * m.vgen[(size_t)l * n + i];
+}
+
+/* ---------------------------- local time steps ----------------------------
+ * TimeLine::calculate_timestep (src/TimeLine.cpp:233-317, the gas particles
+ * of a run without gravity or a global step) for the cells whose step ends
+ * at t_next: h = VorCell::get_h (src/VorCell.cpp:948-956), the CFL step
+ * h / (|v - v_gen| + c) with the generator velocity set at the start of the
+ * step, S = cfl x that; the step is max_step when max_step is shorter than
+ * S, otherwise the largest power-of-two fraction of the timeline not longer
+ * than S, halved until the timeline's end is a whole number of steps from
+ * the cell's end (synchronisation), then clamped to [min_step, max_step].
+ * The cell's next step is [end, end + step).  A zero step (the reference's
+ * "Timestep 0!" exit) is SFX_ERR_TIMESTEP. */
+template <int D>
+__global__ void __launch_bounds__(128) k_timestep_bins(sfx_dmesh m, double gamma, double cfl,
+                                                       unsigned long long max_step,
+                                                       unsigned long long min_step,
+                                                       unsigned long long* smin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m.n_cells) return;
+    const uint64_t end = m.tend[i];
+    if(end != m.t_next) return;
+    const int n = m.n_cells;
+    const double V = m.vol[i];
+    const double h = D == 3 ? sfx_cbrt(V * 3. / 4. / kPi) : sqrt(V / kPi);
+    const double rho = m.W[i], p = m.W[(size_t)(D + 1) * n + i];
+    double v[D];
+#pragma unroll
+    for(int l = 0; l < D; ++l)
+        v[l] = m.W[(size_t)(1 + l) * n + i] - (m.vgen ? m.vgen[(size_t)l * n + i] : 0.);
+    double v2 = v[0] * v[0] + v[1] * v[1];
+    if(D == 3) v2 = v2 + v[2] * v[2];
+    const double vi = sqrt(v2);
+    const double ci = rho != 0. ? sqrt(gamma * p / rho) : 0.;
+    const double S = cfl * (h / (vi + ci));
+    const uint64_t Smax = max_step;
+    uint64_t S2;
+    if(sfx_realtime_interval(m.t_total, Smax) < S) {
+        S2 = Smax;
+    } else {
+        S2 = SFX_TIMELINE_TICKS;
+        while(S2 && sfx_realtime_interval(m.t_total, S2) > S) S2 >>= 1;
+        if(!S2) {
+            report_cell(m.err, i, SFX_ERR_TIMESTEP);
+            return;
+        }
+        while((SFX_TIMELINE_TICKS - end) % S2) S2 >>= 1;
+        S2 = S2 > min_step ? S2 : min_step;
+        S2 = S2 < Smax ? S2 : Smax;
+    }
+    m.tstart[i] = end;
+    m.tend[i] = end + S2;
+    atomicMin(smin, (unsigned long long)S2);
+}
+
+}  // namespace
+
+int sfx_fp64_timestep_bins(const sfx_dmesh* m, double gamma, double cfl, uint64_t max_step,
+                           uint64_t min_step, unsigned long long* d_smin, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int gc = (m->n_cells + 127) / 128;
+    if(m->dim == 3)
+        k_timestep_bins<3><<<gc, 128, 0, s>>>(*m, gamma, cfl, max_step, min_step, d_smin);
+    else
+        k_timestep_bins<2><<<gc, 128, 0, s>>>(*m, gamma, cfl, max_step, min_step, d_smin);
+    sfx_count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+}
+
+namespace {
+}  // namespace
+
+int sfx_fp64_move_velocities(const sfx_dmesh* m, double gamma, double dt, int periodic,
+                             int faces, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int gc = (m->n_cells + 127) / 128, gf = faces ? (m->n_faces + 127) / 128 : 0;
+    if(m->dim == 3) {
+        k_gen_velocity<3><<<gc, 128, 0, s>>>(*m, gamma, dt, periodic);
+        if(gf) k_face_velocity<3><<<gf, 128, 0, s>>>(*m);
+    } else {
+        k_gen_velocity<2><<<gc, 128, 0, s>>>(*m, gamma, dt, periodic);
+        if(gf) k_face_velocity<2><<<gf, 128, 0, s>>>(*m);
+    }
+    sfx_count_launches(gf ? 2 : 1);
+    return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+}
+
+int sfx_fp64_drift(const sfx_dmesh* m, double dt, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int gc = (m->n_cells + 127) / 128;
+    if(m->dim == 3)
+        k_drift<3><<<gc, 128, 0, s>>>(*m, dt);
+    else
+        k_drift<2><<<gc, 128, 0, s>>>(*m, dt);
+    sfx_count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? SFX_OK : SFX_ERR_CUDA;
+}
+
+namespace {
 }  // namespace
 
 void sfx_solver_params_init(sfx_solver_params* p, int kind, double g, double tol,

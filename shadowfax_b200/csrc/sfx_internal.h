@@ -71,10 +71,11 @@ struct sfx_dmesh {
      * fi [F] int2: {L, R}; R = -1 mirror, R | 1<<30 periodic image;
      * fsh [F]: periodic image shift, 2 bits per axis (0, +1, -1 box);
      * cw [2n] float4 cell record {rho, v.., p | Q.m, total area ..};
-     * cg [G*n] float4 per-cell record: the limited gradients [dim][S], then
-     *     dW/dt [S] (the Euler Jacobian at the cell state times those
-     *     gradients, the MUSCL-Hancock prediction every face of the cell
-     *     shares), zero padded (G = sfx_split_grad_vec4(dim): 5 in 3D, 3 in 2D);
+     * cg [G*n] float4 gradients (G = 4 in 3D, 2 in 2D: 64 / 32 bytes, so a
+     *     record never straddles more 32-byte sectors than it fills);
+     * cdw [H*n] float4 dW/dt (the Euler Jacobian at the cell state times its
+     *     gradients: the MUSCL-Hancock prediction every face of the cell
+     *     shares), read by the exact solver's face kernels (H = 2 in 3D, 1 in 2D);
      * cx [n] float4 {x - centroid, volume};
      * an [dim][F] FP64 area vector A n (n from x_L to x_R), for the pressure
      *     force, so that the forces on a cell cancel to FP64 round-off in a
@@ -86,8 +87,23 @@ struct sfx_dmesh {
     uint8_t* fsh;
     float4* cw;
     float4* cg;
+    float4* cdw;
     float4* cx;
     int32_t* nbe; /* [nnz] neighbour cell of each CSR entry (-1 mirror) */
+    /* moving generators (plain FP64, sfx_step_moving; allocated on first
+     * use): generator velocities [dim][n], drifted positions [dim][n] */
+    double* vgen;
+    double* newpos;
+    /* local (hierarchical) time steps, plain FP64 (sfx_step_window): the
+     * start and end of every cell's step on the integer timeline of 2^60
+     * ticks spanning t_total; with `local` set a cell is active when its
+     * start is t_now (gradients, fluxes of its faces) and gets get_W when its
+     * end is t_next */
+    uint64_t* tstart;
+    uint64_t* tend;
+    int32_t local;
+    uint64_t t_now, t_next;
+    double t_total;
     double* an;
     float2* dqm;
     double* dqv;
@@ -110,6 +126,20 @@ struct sfx_dmesh {
 SFX_RANGE_HD int sfx_grad_cells(const sfx_dmesh& m) { return m.ranged ? m.r_grad : m.n_cells; }
 SFX_RANGE_HD int sfx_flux_faces(const sfx_dmesh& m) { return m.ranged ? m.r_flux : m.n_faces; }
 SFX_RANGE_HD int sfx_update_cells(const sfx_dmesh& m) { return m.ranged ? m.r_upd : m.n_cells; }
+
+/* the integer timeline of local time steps: 2^60 ticks from time 0 to
+ * t_total (TimeLine, src/TimeLine.hpp:145-178) */
+#define SFX_TIMELINE_TICKS (1ull << 60)
+/* TimeLine::get_realtime (the timeline starts at 0) */
+SFX_RANGE_HD double sfx_realtime(double t_total, uint64_t ticks) {
+    const double t = (double)ticks / (double)SFX_TIMELINE_TICKS;
+    return t_total * t + 0.;
+}
+/* TimeLine::get_realtime_interval */
+SFX_RANGE_HD double sfx_realtime_interval(double t_total, uint64_t ticks) {
+    const double dt = (double)ticks / (double)SFX_TIMELINE_TICKS;
+    return t_total * dt;
+}
 
 /* one mesh of a launch group (device table entry); steps_left, when not
  * NULL, is the member's remaining step count: the kernels skip a member at 0
@@ -157,6 +187,20 @@ int sfx_fp64_pack_cells(const sfx_dmesh* m, const int32_t* idx, int count, doubl
                         void* stream);
 int sfx_fp64_unpack_cells(const sfx_dmesh* m, const int32_t* idx, int count, const double* in,
                           void* stream);
+/* moving generators: generator velocities (VorCell::get_velocity with the
+ * reflective-box check) into m->vgen, then (faces != 0) face velocities
+ * (VorFace::set_v) into m->vel; with m->local only the cells starting a step
+ * at t_now, each with its own step in the box check */
+int sfx_fp64_move_velocities(const sfx_dmesh* m, double gamma, double dt, int periodic,
+                             int faces, void* stream);
+/* m->newpos = m->pos + dt m->vgen (Particle::drift) */
+int sfx_fp64_drift(const sfx_dmesh* m, double dt, void* stream);
+/* TimeLine::calculate_timestep for the cells whose step ends at t_next: the
+ * CFL step h / (|v - v_gen| + c), its power-of-two subdivision of the
+ * timeline, synchronised with the end, clamped to [min_step, max_step];
+ * start <- end, end <- end + step; *d_smin (device) receives the smallest */
+int sfx_fp64_timestep_bins(const sfx_dmesh* m, double gamma, double cfl, uint64_t max_step,
+                           uint64_t min_step, unsigned long long* d_smin, void* stream);
 int sfx_fp64_riemann(int dim, const sfx_solver_params* sp, int n,
                      const double* dWL, const double* dWR, const double* dn,
                      int reflective, double* dhalf, double* dflux,
@@ -204,10 +248,14 @@ int sfx_mesh_clone_async(sfx_ctx* ctx, sfx_mesh* base, void* stream, sfx_mesh** 
  * tuning, the same for a mesh alone and in a group: one in 2D (about six
  * faces per cell), four in 3D (about sixteen); measured fastest on 300,000-cell
  * meshes */
-/* float4s of the split pass's per-cell gradient record (cg) */
+/* float4s of the split pass's per-cell gradient record (cg) and of its
+ * per-cell dW/dt record (cdw) */
 inline int sfx_split_grad_vec4(int dim) {
     const int S = dim + 2;
-    return (dim * S + S + 3) / 4;
+    return (dim * S + 3) / 4;
+}
+inline int sfx_split_dwdt_vec4(int dim) {
+    return (dim + 2 + 3) / 4;
 }
 
 inline int sfx_default_lanes(int dim) {

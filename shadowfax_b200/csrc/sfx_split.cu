@@ -101,28 +101,33 @@ __device__ __forceinline__ void store_cell(float4* cw, int i, const float* W, fl
     }
 }
 
-/* per-cell gradient record: g[l][k] at flat l*S+k, then dW/dt[k] at
- * D*S+k, padded to float4s (GradVec4<D>::value of them) */
+/* per-cell gradient record: g[l][k] at flat l*S+k, padded to float4s
+ * (GradVec4<D>::value of them); dW/dt in a record of its own
+ * (DwdtVec4<D>::value float4s) */
 template <int D>
 struct GradVec4 {
-    static constexpr int value = (D * (D + 2) + (D + 2) + 3) / 4;
+    static constexpr int value = (D * (D + 2) + 3) / 4;
+};
+template <int D>
+struct DwdtVec4 {
+    static constexpr int value = (D + 2 + 3) / 4;
 };
 
 template <int D>
 __device__ __forceinline__ void sdwdt(float gamma, const float* W, const float (*g)[D + 2],
                                       float* dW);
 
-/* a cell's gradients and dW/dt: with STORED the record's dW/dt, otherwise
- * only the gradient float4s are read and dW/dt is formed here (the HLLC face
- * kernel, which is closer to the memory bound than to the issue bound) */
+/* a cell's gradients and dW/dt: with STORED dW/dt from its record (the
+ * exact solver's kernels, bound by instruction issue), otherwise formed here
+ * (the HLLC face kernel, closer to the memory bound) */
 template <int D, bool STORED>
-__device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i, float gamma,
+__device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
+                                          const float4* __restrict__ cdw, int i, float gamma,
                                           const float* W, float (*g)[D + 2], float* dWdt) {
-    constexpr int S = D + 2, G = GradVec4<D>::value;
-    constexpr int GL = STORED ? G : (D * S + 3) / 4;
+    constexpr int S = D + 2, G = GradVec4<D>::value, H = DwdtVec4<D>::value;
     float t[4 * G];
 #pragma unroll
-    for(int q = 0; q < GL; ++q) {
+    for(int q = 0; q < G; ++q) {
         const float4 v = __ldg(cg + (size_t)G * i + q);
         t[4 * q] = v.x;
         t[4 * q + 1] = v.y;
@@ -134,8 +139,17 @@ __device__ __forceinline__ void load_grad(const float4* __restrict__ cg, int i, 
 #pragma unroll
         for(int k = 0; k < S; ++k) g[l][k] = t[l * S + k];
     if(STORED) {
+        float u[4 * H];
 #pragma unroll
-        for(int k = 0; k < S; ++k) dWdt[k] = t[D * S + k];
+        for(int q = 0; q < H; ++q) {
+            const float4 v = __ldg(cdw + (size_t)H * i + q);
+            u[4 * q] = v.x;
+            u[4 * q + 1] = v.y;
+            u[4 * q + 2] = v.z;
+            u[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for(int k = 0; k < S; ++k) dWdt[k] = u[k];
     } else {
         sdwdt<D>(gamma, W, g, dWdt);
     }
@@ -415,10 +429,11 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
 #pragma unroll
     for(int k = 0; k < S; ++k) alpha[k] = seg_min<LPC>(alpha[k]);
     if(!live) return;
-    /* lane q % LPC writes float4 q of the gradient record: the limited
-     * gradients, then dW/dt at the cell state (every face of the cell
-     * predicts its half step with it) */
-    float out[4 * G];
+    /* lane q % LPC writes float4 q of the gradient record, lane (G + q) % LPC
+     * float4 q of the dW/dt record (dW/dt at the cell state: every face of
+     * the cell predicts its half step with it) */
+    constexpr int H = DwdtVec4<D>::value;
+    float out[4 * G], dw[4 * H];
     float lg[D][S];
 #pragma unroll
     for(int l = 0; l < D; ++l)
@@ -427,9 +442,16 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
             lg[l][k] = delta[l][k] * alpha[k];
             out[l * S + k] = lg[l][k];
         }
-    sdwdt<D>(gamma, W, lg, out + D * S);
 #pragma unroll
-    for(int q = D * S + S; q < 4 * G; ++q) out[q] = 0.f;
+    for(int q = D * S; q < 4 * G; ++q) out[q] = 0.f;
+    sdwdt<D>(gamma, W, lg, dw);
+#pragma unroll
+    for(int q = S; q < 4 * H; ++q) dw[q] = 0.f;
+#pragma unroll
+    for(int q = 0; q < H; ++q)
+        if(lane == (G + q) % LPC)
+            m.cdw[(size_t)H * i + q] = make_float4(dw[4 * q], dw[4 * q + 1], dw[4 * q + 2],
+                                                   dw[4 * q + 3]);
 #pragma unroll
     for(int q = 0; q < G; ++q)
         if(lane == q % LPC)
@@ -1208,7 +1230,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         }
         rr = sqrtf(cd2);
         float gR[D][S], dWR[S];
-        load_grad<D, STORED>(m.cg, iR, gamma, w.WR, gR, dWR);
+        load_grad<D, STORED>(m.cg, m.cdw, iR, gamma, w.WR, gR, dWR);
 #pragma unroll
         for(int k = 0; k < S; ++k) WRr[k] = w.WR[k];
         spredict<D>(hdt, WRr, w.WR, w.WL, gR, dWR, dR, true, rr);
@@ -1217,7 +1239,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         float dL[D], gL[D][S], dWL[S];
 #pragma unroll
         for(int l = 0; l < D; ++l) dL[l] = c[l] + xmcL[l] - 0.5f * r[l];
-        load_grad<D, STORED>(m.cg, iL, gamma, w.WL, gL, dWL);
+        load_grad<D, STORED>(m.cg, m.cdw, iL, gamma, w.WL, gL, dWL);
 #pragma unroll
         for(int k = 0; k < S; ++k) WLr[k] = w.WL[k];
         spredict<D>(hdt, WLr, w.WL, w.WR, gL, dWL, dL, !w.mirror, rr);

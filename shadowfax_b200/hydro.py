@@ -204,6 +204,79 @@ class FluxPass:
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_mesh_set_lanes(self.h, lanes), "sfx_mesh_set_lanes")
 
+    # ---- local (hierarchical) time steps, plain FP64 ----
+    def set_timesteps(self, start, end) -> None:
+        """each cell's step [start, end) in ticks of the 2^60-tick timeline"""
+        s = np.ascontiguousarray(start, np.uint64)
+        e = np.ascontiguousarray(end, np.uint64)
+        L.check(L.lib().sfx_mesh_set_timesteps(self.h, s.ctypes.data_as(L._u64p),
+                                               e.ctypes.data_as(L._u64p)),
+                "sfx_mesh_set_timesteps")
+
+    def timesteps(self) -> tuple[np.ndarray, np.ndarray]:
+        n = self.mesh.n_cells
+        s, e = np.empty(n, np.uint64), np.empty(n, np.uint64)
+        L.check(L.lib().sfx_mesh_get_timesteps(self.h, s.ctypes.data_as(L._u64p),
+                                               e.ctypes.data_as(L._u64p)),
+                "sfx_mesh_get_timesteps")
+        return s, e
+
+    def set_gradients(self, grad) -> None:
+        g = np.ascontiguousarray(grad, np.float64)
+        L.check(L.lib().sfx_mesh_set_gradients(self.h, L.dptr(g)), "sfx_mesh_set_gradients")
+
+    def gradients(self) -> np.ndarray:
+        g = np.empty((self.mesh.n_cells, self.mesh.dim, self.S))
+        L.check(L.lib().sfx_mesh_get_gradients(self.h, L.dptr(g)), "sfx_mesh_get_gradients")
+        return g
+
+    def step_window(self, t_total: float, t_now: int, t_next: int, periodic: bool):
+        """one system step [t_now, t_next) of local time steps (sfx_step_window)"""
+        st = L.sfx_stats()
+        rc = L.lib().sfx_step_window(self.h, t_total, int(t_now), int(t_next), int(periodic),
+                                     C.byref(st))
+        if rc:
+            raise L.SfxError(rc, "sfx_step_window",
+                             st.bad_face if st.bad_face >= 0 else st.bad_cell)
+        return st
+
+    def timestep_bins(self, t_total: float, cfl: float, max_step: int, min_step: int,
+                      t_next: int) -> int:
+        """new steps for the cells ending at t_next; returns the next system step"""
+        out = C.c_uint64(0)
+        L.check(L.lib().sfx_timestep_bins(self.h, t_total, cfl, int(max_step), int(min_step),
+                                          int(t_next), C.byref(out)), "sfx_timestep_bins")
+        return int(out.value)
+
+    def run_local(self, t_total: float, n_system_steps: int, cfl: float = 0.4,
+                  max_step: int = 1 << 60, min_step: int = 0, periodic: bool = True,
+                  t0: int = 0) -> int:
+        """n_system_steps of local time stepping from tick t0 (0: every cell
+        starts a step there), each followed by the new steps of the cells it
+        ends (the reference's main loop for a static mesh); returns the tick
+        reached.  One 8-byte read per system step for the next system step."""
+        t = int(t0)
+        dsys = self.timestep_bins(t_total, cfl, max_step, min_step, t)
+        for _ in range(n_system_steps):
+            t_next = t + dsys
+            self.step_window(t_total, t, t_next, periodic)
+            dsys = self.timestep_bins(t_total, cfl, max_step, min_step, t_next)
+            t = t_next
+        return t
+
+    def step_moving(self, dt: float, periodic: bool) -> np.ndarray:
+        """one step of a moving mesh (sfx_step_moving): generator velocities
+        from the state, face velocities, the step in each face's frame, the
+        drift; returns the drifted generator positions [n, dim] (the next
+        tessellation's input)"""
+        pos = np.empty((self.mesh.n_cells, self.mesh.dim))
+        st = L.sfx_stats()
+        rc = L.lib().sfx_step_moving(self.h, dt, int(periodic), L.dptr(pos), C.byref(st))
+        if rc:
+            raise L.SfxError(rc, "sfx_step_moving",
+                             st.bad_face if st.bad_face >= 0 else st.bad_cell)
+        return pos
+
     def set_face_variant(self, variant: int):
         """split pass: register cap of the face kernel (0: 64 registers, four
         blocks per SM; 1: 80 registers, three)"""

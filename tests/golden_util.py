@@ -8,6 +8,10 @@ import numpy as np
 from shadowfax_b200.mesh import Mesh
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
+MOVING_CASES = [f"moving_{d}d_{b}_{s}" for d in (2, 3) for b in ("reflective", "periodic")
+                for s in ("exact", "hllc")]
+MOVING_FAILS = "moving_2d_periodic_hllc_fails"
+LOCAL_CASES = [f"local_{d}d_{s}" for d in (2, 3) for s in ("exact", "hllc")]
 MESH_CASES = ["sod2d_exact", "sod2d_hllc", "sedov3d_hllc", "random3d_exact",
               "random2d_periodic_exact"]
 
@@ -19,6 +23,8 @@ def load_case(name: str):
     meta = dict(solver=str(z["solver"]), gamma=float(z["gamma"]), dt=float(z["dt"]),
                 nsteps=int(z["nsteps"]), W0=z["W0"])
     ref = {k: z[k] for k in z.files if k.startswith("ref_")}
+    if "local_start" in z.files:
+        meta["local"] = {k[len("local_"):]: z[k] for k in z.files if k.startswith("local_")}
     return mesh, meta, ref
 
 
