@@ -632,6 +632,7 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
     segments = [s for s in np.array_split(np.arange(len(reqs)), nseg) if len(s)]
     nbytes = lambda j: bases[reqs[j].mesh].clone_bytes(L.PREC_SPLIT)  # noqa: E731
     seg_ms, face_steps, launches, roof, nwaves = [], 0, 0, None, 0
+    fvar = {}
     failed = set()
     first = True
     for seg in segments:
@@ -647,6 +648,9 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
                 inst[j] = (c, fp)
             if first:
                 roof = resident_roofline(pool, reqs, inst, classes, cctx)
+                # the face-kernel variant the tuner kept for each class
+                fvar = {c: roof["classes"][f"{c[0]}D {c[1]}"]["tuned"]["face_variant"]
+                        for c in classes if f"{c[0]}D {c[1]}" in roof["classes"]}
                 for c in classes:
                     js = [j for j in wave if inst[j][0] == c]
                     if js and warmup:
@@ -678,6 +682,7 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
                                           [pool.dts[reqs[j].mesh][reqs[j].state]
                                            for j in live[c]])
                         groups[c].set_steps([left[j] for j in live[c]])
+                        groups[c].set_face_variant(fvar.get(c, 0))
                         reused[c] = 0
                 for c in classes:
                     if groups[c] is not None:
@@ -755,6 +760,10 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
         g.step_timed(1)
         steps = 3
         ms, nl = g.step_timed(steps)
+        # the timing tuners on this class's meshes (the states are read, not
+        # changed): lanes per cell of the gradient/update kernels, register
+        # cap of the face kernel
+        tuned = {"lanes_per_cell": int(g.tune(2)), "face_variant": int(g.tune_faces(2))}
         g.close()
         per_launch = ms / steps
         alg = {k: 0 for k in names}
@@ -772,7 +781,8 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
             "achieved_gbs": {k: alg[k] / (per_launch[i] / 1e3) / 1e9 for i, k in enumerate(names)},
             "algorithmic_bytes": alg,
             "step_face_steps_per_s": faces / (per_launch.sum() / 1e3),
-            "step_frac": STEP_BYTES[("split", D)] * faces / (per_launch.sum() / 1e3) / 1e9 / peak}
+            "step_frac": STEP_BYTES[("split", D)] * faces / (per_launch.sum() / 1e3) / 1e9 / peak,
+            "tuned": tuned}
     top_c = max(per_class, key=lambda c: work[c])
     pc = per_class[top_c]
     kms = pc["kernel_ms"]

@@ -336,12 +336,27 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
      * a face of zero area), the rest are loaded again */
     __shared__ float sd[kGradSlots * D][256];
     int k0 = 0;
+    /* software pipelined: the next entry's face id and neighbour are loaded
+     * before this entry's gathers, and both gathers (face geometry, the
+     * neighbour's record) are issued before either is used */
+    unsigned e_next = 0u;
+    int nb_next = -1;
+    if(beg + lane < end) {
+        e_next = (unsigned)__ldg(m.idx + beg + lane);
+        nb_next = __ldg(m.nbe + beg + lane);
+    }
     for(int j = beg + lane; j < end; j += LPC, ++k0) {
-        const unsigned e = (unsigned)__ldg(m.idx + j);
+        const unsigned e = e_next;
+        const int nb = nb_next;
+        if(j + LPC < end) {
+            e_next = (unsigned)__ldg(m.idx + j + LPC);
+            nb_next = __ldg(m.nbe + j + LPC);
+        }
         const int f = (int)(e & ~kRightBit);
         const bool right = e & kRightBit;
         float A, c[D], r[D], rn;
         geom<D>(m.fg, f, A, c, r, rn);
+        const Cell<D> cn = load_cell<D>(m.cw, nb < 0 ? ic : nb);
         if(A == 0.f) {
             if(k0 < kGradSlots) sd[k0 * D][threadIdx.x] = __int_as_float(0x7fc00000);
             continue;
@@ -355,7 +370,6 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
 #pragma unroll
             for(int l = 0; l < D; ++l) sd[k0 * D + l][threadIdx.x] = c[l] + xmc[l] - 0.5f * r[l];
         }
-        const int nb = __ldg(m.nbe + j);
         float Wj[S];
         if(nb < 0) {
             /* reflective mirror: flip the velocity component along the face
@@ -369,7 +383,6 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
 #pragma unroll
             for(int l = 0; l < D; ++l) Wj[1 + l] = W[1 + l] - vn * r[l];
         } else {
-            const Cell<D> cn = load_cell<D>(m.cw, nb);
 #pragma unroll
             for(int k = 0; k < S; ++k) Wj[k] = cn.W[k];
         }
@@ -1732,7 +1745,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
 }
 
 template <int D, int LPC>
-__global__ void __launch_bounds__(256) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
+__global__ void __launch_bounds__(256, 4) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
                                                      int nm, float gamma) {
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
