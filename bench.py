@@ -89,9 +89,10 @@ def parse():
                     help="sedov3d / random3d solver (default: HLLC / Exact)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="serve",
-                    choices=["serve", "sedov3d", "random3d", "batch2d"],
+                    choices=["serve", "sod2d", "sedov3d", "random3d", "random2d", "batch2d"],
                     help="serve: the request stream (default); sedov3d: Sedov 3D blast "
-                         "on one mesh; random3d: periodic 3D random field, exact solver; "
+                         "on one mesh; sod2d: 2D Sod tube, 10,000 generators, exact "
+                         "solver, dt 1e-4; random3d: periodic 3D random field, exact solver; "
                          "batch2d: 1,024 2D meshes")
     ap.add_argument("--meshes", type=int, default=1024, help="batch2d: number of meshes")
     ap.add_argument("--duration", type=float, default=60.0,
@@ -107,11 +108,13 @@ def parse():
                          "writing the ones not there yet (sfx_meshfile_*)")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = {"serve": 20, "sedov3d": 50, "random3d": 10, "batch2d": 20}[a.workload]
+        a.steps = {"serve": 20, "sod2d": 100, "sedov3d": 50, "random3d": 10, "random2d": 10,
+                   "batch2d": 20}[a.workload]
     if a.n is None:
-        a.n = {"random3d": 2_097_152}.get(a.workload, N_GEN)
+        a.n = {"random3d": 2_097_152, "random2d": 2_097_152, "sod2d": 10_000}.get(a.workload,
+                                                                                  N_GEN)
     if a.solver is None:
-        a.solver = "Exact" if a.workload == "random3d" else "HLLC"
+        a.solver = "Exact" if a.workload in ("random3d", "random2d", "sod2d") else "HLLC"
     return a
 
 
@@ -254,6 +257,7 @@ def split_kernel_bytes(dim: int, n_cells: int, n_faces: int, nnz: int):
 
 # bytes per face-step of the whole step, fixed for this workload's roofline:
 # face record + per-cell data / faces per cell (2D F ~ 3N, 3D F ~ 7.8N)
+L2_BYTES = 126 << 20   # B200 L2
 STEP_BYTES = {("fp64", 2): 144, ("fp64", 3): 120, ("split", 2): 92, ("split", 3): 70}
 
 
@@ -263,23 +267,35 @@ def build_problem(args):
     from shadowfax_b200 import workloads as wl
     if args.workload == "random3d":
         return wl.random_field3d(n=args.n, seed=3, solver=args.solver)
+    if args.workload == "random2d":
+        return wl.random_field2d(n=args.n, seed=3, solver=args.solver)
+    if args.workload == "sod2d":
+        return wl.sod2d(n=args.n, seed=1, solver=args.solver)
     return wl.sedov3d(n=args.n, seed=SEED, solver=args.solver)
 
 
 def problem_text(args, pr):
     m = pr.mesh
-    if args.workload == "random3d":
-        return (f"random3d {pr.solver}, {m.n_cells} generators (seed 3), {m.n_active_faces} "
-                f"faces, periodic unit cube, log-normal density, Gaussian velocities, CFL-0.4 dt")
+    if args.workload in ("random3d", "random2d"):
+        box = "cube" if m.dim == 3 else "square"
+        return (f"{args.workload} {pr.solver}, {m.n_cells} generators (seed 3), "
+                f"{m.n_active_faces} faces, periodic unit {box}, log-normal density, Gaussian "
+                f"velocities, CFL-0.4 dt")
+    if args.workload == "sod2d":
+        return (f"sod2d {pr.solver}, {m.n_cells} generators (seed 1), {m.n_active_faces} faces, "
+                f"reflective unit square, rho/p 1/1 | 0.125/0.1 at x = 0.5, dt 1e-4")
     return (f"sedov3d {pr.solver}, {m.n_cells} generators (seed {SEED}), {m.n_active_faces} "
             f"faces, reflective unit cube, CFL-0.4 dt")
 
 
-def cpu_baseline(pr, steps: int = 3):
+def cpu_baseline(pr, steps: int | None = None):
     """reference CPU pass (oracle/_ref, unmodified Shadowfax sources), one
-    core, on the same mesh for a bounded number of steps"""
+    core, on the same mesh for a bounded number of steps (about 3e7
+    face-steps, at least 3 steps and at most 100)"""
     from oracle.oracle import Params, ref_binary, run_reference
-    exe = ref_binary(3, "libm")
+    if steps is None:
+        steps = max(3, min(100, int(3e7 // max(pr.mesh.n_active_faces, 1))))
+    exe = ref_binary(pr.mesh.dim, "libm")
     if not exe.exists():
         return None
     p = Params(solver=pr.solver, gamma=pr.gamma, use_libm_pow=True)
@@ -347,6 +363,7 @@ def bench_batch(args, rank, world, local, torch):
         members.append(fp)
     grp = Group(ctx, members, [pr.dt for pr in probs])
     lanes = grp.tune(3)
+    face_variant = grp.tune_faces(3)
     for fp, pr in zip(members, probs):   # tuning reads the states only; reset anyway
         fp.set_primitive(pr.W0)
     with torch.cuda.stream(stream), ClockSampler(local) as clk:
@@ -373,6 +390,27 @@ def bench_batch(args, rank, world, local, torch):
         st = grp.step(1, graph=False)
         assert np.all(st == 0), st
     value, ms_max, _ = reduce_over_ranks(ms, faces * args.steps, f"cuda:{local}", world)
+    # end to end through the public API with host buffers: per step every
+    # mesh's W and Q uploaded from host memory, one group step, W and Q read back
+    saved = [fp.state() for fp in members]
+    host = saved
+    e2e_steps = max(1, min(args.steps, 5))
+    nbytes = sum(W.nbytes + Q.nbytes for W, Q in host)
+    with torch.cuda.stream(stream):
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for fp, (W, Q) in zip(members, host):
+                fp.set_state(W, Q)
+            grp.step(1, graph=True, status=False)
+            host = [fp.state() for fp in members]
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+    for fp, (W, Q) in zip(members, saved):   # back to the state the accuracy check expects
+        fp.set_state(W, Q)
+    e2e_val, _, _ = reduce_over_ranks(e2e_ms, faces * e2e_steps, f"cuda:{local}", world)
     # FP64 baseline: one launch sequence per mesh
     ctx64 = Context(2, solver, L.PREC_FP64, device=local)
     ctx64.set_stream(stream.cuda_stream)
@@ -426,7 +464,8 @@ def bench_batch(args, rank, world, local, torch):
                                    f"log-uniform in [1e3, 1e5] (total {sum(p.mesh.n_cells for p in probs)}"
                                    f" cells, {faces} faces), step states, HLLC, own CFL dt each",
                        "precision": "split", "launch": "one launch group, CUDA graph of K steps",
-                       "lanes_per_cell": lanes, "l2": "working set > L2 (no flush)",
+                       "lanes_per_cell": lanes, "face_variant": face_variant,
+                       "l2": "working set > L2 (no flush)",
                        "parallelism": f"replicas x{world}", "mesh_build_s": round(t_build, 1)},
             "clocks": clk.summary(),
             "fp64_per_mesh": {"value": fp64_value, "unit": UNIT, "steps": base_steps,
@@ -439,6 +478,11 @@ def bench_batch(args, rank, world, local, torch):
                          "achieved": 92 * value / 1e9, "frac": 92 * value / 1e9 / peak,
                          "note": "bytes per face-step of the split pass, 2D (algorithmic)"},
             "cpu_baseline": cb,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+                    "note": "wall clock: per step every mesh's W and Q from host memory, one "
+                            "group step, W and Q back (sfx_state_upload_WQ / "
+                            "sfx_group_step / sfx_state_download)"},
             "gpu_launches": int(n_launches),
         }
     grp.close()
@@ -731,13 +775,31 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
             "launches": launches, "roofline": roof, "waves": nwaves, "failed": len(failed)}
 
 
-# DRAM bytes (read + write) per face of one launch, from one-kernel ncu
-# captures of a 300,000-cell periodic random-field mesh (3D, 2,396,113 faces)
-# and of a 300,000-cell periodic 2D mesh; the gathers and the per-face records
-# scale with the faces, so a launch over F faces moves about F times these
-TRAFFIC_B_PER_FACE = {("k_group_sfaces", 3, "Exact"): 106.1, ("k_group_sfaces", 3, "HLLC"): 104.3,
-                      ("k_group_sgrad", 3): 59.4, ("k_group_sapply", 3): 53.0}
-KERNELS = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces", "update": "k_group_sapply"}
+# DRAM bytes (read + write) per active face of one launch of each split
+# kernel, from one-kernel ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum) of a 300,000-cell periodic random-field mesh in 3D
+# (2,396,113 faces) and a 700,000-cell one in 2D; the gathers and the per-face
+# records scale with the faces, so a launch over F faces moves about F times
+# these
+TRAFFIC_B_PER_FACE = {("faces", 3, "Exact"): 110.1, ("faces", 3, "HLLC"): 105.5,
+                      ("gradients", 3): 61.4, ("update", 3): 52.8,
+                      ("faces", 2, "Exact"): 104.8, ("faces", 2, "HLLC"): 98.6,
+                      ("gradients", 2): 73.3, ("update", 2): 54.2}
+
+
+def split_kernel_name(role: str, solver: str) -> str:
+    if role == "faces":
+        return "k_group_sfaces_exact" if solver == "Exact" else "k_group_sfaces"
+    return {"gradients": "k_group_sgrad", "update": "k_group_sapply"}[role]
+
+
+def split_traffic(role: str, dim: int, solver: str, faces: int):
+    """DRAM bytes of one launch over ``faces`` active faces, or None where no
+    capture of that kernel exists"""
+    key = (role, dim, solver) if role == "faces" else (role, dim)
+    return TRAFFIC_B_PER_FACE[key] * faces if key in TRAFFIC_B_PER_FACE else None
+
+
 
 
 def resident_roofline(pool, reqs, inst, classes, cctx):
@@ -757,13 +819,13 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
             continue
         g = Group(cctx[c], [inst[j][1] for j in js],
                   [pool.dts[reqs[j].mesh][reqs[j].state] for j in js])
+        # the timing tuners on this class's meshes (the states are read, not
+        # changed): lanes per cell of the gradient/update kernels, the face
+        # kernel's variant; the kernels are then timed as tuned
+        tuned = {"lanes_per_cell": int(g.tune(2)), "face_variant": int(g.tune_faces(2))}
         g.step_timed(1)
         steps = 3
         ms, nl = g.step_timed(steps)
-        # the timing tuners on this class's meshes (the states are read, not
-        # changed): lanes per cell of the gradient/update kernels, register
-        # cap of the face kernel
-        tuned = {"lanes_per_cell": int(g.tune(2)), "face_variant": int(g.tune_faces(2))}
         g.close()
         per_launch = ms / steps
         alg = {k: 0 for k in names}
@@ -787,10 +849,9 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
     pc = per_class[top_c]
     kms = pc["kernel_ms"]
     top = max(names, key=lambda k: kms[k])
-    kname = KERNELS[top]
+    kname = split_kernel_name(top, top_c[1])
     D = top_c[0]
-    tkey = (kname, D, top_c[1]) if kname == "k_group_sfaces" else (kname, D)
-    traffic = TRAFFIC_B_PER_FACE[tkey] * pc["faces"] if tkey in TRAFFIC_B_PER_FACE else None
+    traffic = split_traffic(top, D, top_c[1], pc["faces"])
     roof = {"bound": "hbm", "kernel": kname,
             "class": f"{D}D {top_c[1]}, {pc['requests']} requests, {pc['faces']} faces",
             "achieved": pc["achieved_gbs"][top], "peak": peak, "unit": "GB/s",
@@ -1047,9 +1108,10 @@ def run_reference_arm(args, rank, world):
     if args.workload == "serve":
         return run_reference_serve(args)
     pr = build_problem(args)
-    steps = max(1, min(args.steps, 5))
+    # a bounded sample: 5 steps, or up to 3e6 face-steps on a small mesh
+    steps = max(1, min(args.steps, max(5, int(3e6 // pr.mesh.n_active_faces))))
     from oracle.oracle import ref_binary
-    if not ref_binary(3, "libm").exists():
+    if not ref_binary(pr.mesh.dim, "libm").exists():
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref reference harness not built (needs the reference tree)"}))
         return
@@ -1131,7 +1193,8 @@ def main():
     pr = build_problem(args)
     mesh = pr.mesh
     prec = L.PREC_FP64 if args.precision == "fp64" else L.PREC_SPLIT
-    ctx = Context(3, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec, device=local)
+    D = mesh.dim
+    ctx = Context(D, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec, device=local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     fp = FluxPass(ctx, mesh)
@@ -1143,6 +1206,12 @@ def main():
         lanes = fp.tune(dt, 3)     # lanes per cell for the gradient/update kernels
         fp.set_primitive(pr.W0)
 
+    # a mesh whose device data fit in the L2 is timed step by step, with a
+    # 256 MB write between the steps outside the timed events, so that no
+    # step starts from a warm L2
+    dev_bytes = L.lib().sfx_mesh_device_bytes(D, mesh.n_cells, mesh.n_faces, mesh.nnz, prec)
+    flush = (torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+             if dev_bytes < L2_BYTES else None)
     with torch.cuda.stream(stream), ClockSampler(local) as clk:
         clk.wait_first_sample()
         for _ in range(args.warmup):
@@ -1154,19 +1223,26 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
+        events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(1 if flush is None else args.steps)]
         clk.mark("t0")
         n_launch0 = L.lib().sfx_launch_count()
-        e0.record(stream)
-        for _ in range(args.steps):
-            fp.step(dt, 1, stats=False)
-        e1.record(stream)
+        if flush is None:
+            events[0][0].record(stream)
+            for _ in range(args.steps):
+                fp.step(dt, 1, stats=False)
+            events[0][1].record(stream)
+        else:
+            for e0, e1 in events:
+                flush.fill_(1)
+                e0.record(stream)
+                fp.step(dt, 1, stats=False)
+                e1.record(stream)
         n_launches = L.lib().sfx_launch_count() - n_launch0
         torch.cuda.synchronize()
         clk.mark("t1")
         time.sleep(0.3)
-        ms = e0.elapsed_time(e1)
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in events)
         if world > 1:
             dist.barrier()
         st = fp.step(dt, 1)  # status check after the timed region
@@ -1180,24 +1256,25 @@ def main():
     per_launch = kms / args.steps
     top = int(np.argmax(per_launch))
     if args.precision == "split":
-        alg = split_kernel_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz)
-        kname = {"gradients": "k_group_sgrad", "faces": "k_group_sfaces",
-                 "update": "k_group_sapply"}[names[top]]
+        alg = split_kernel_bytes(D, mesh.n_cells, mesh.n_faces, mesh.nnz)
+        kname = split_kernel_name(names[top], pr.solver)
+        traffic = split_traffic(names[top], D, pr.solver, mesh.n_active_faces)
     else:
-        alg = algorithmic_bytes(3, mesh.n_cells, mesh.n_faces, mesh.nnz, args.precision)
+        alg = algorithmic_bytes(D, mesh.n_cells, mesh.n_faces, mesh.nnz, args.precision)
         kname = {"gradients": "k_grad_terms + k_grad_sum", "faces": "k_faces",
                  "update": "k_apply"}[names[top]]
+        traffic = None
     peak, peak_kind = peaks()
     achieved = alg[names[top]] / (per_launch[top] / 1e3) / 1e9
     step_bytes = sum(alg.values())
     roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
-            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "peak_source": f"hbm_gbs {peak_kind}",
             "algorithmic_bytes_per_launch": alg[names[top]],
             "kernel_ms": {n: float(v) for n, v in zip(names, per_launch)},
             "step_achieved_gbs": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
-            "step_bytes_per_face": STEP_BYTES[(args.precision, 3)],
-            "step_frac": STEP_BYTES[(args.precision, 3)] * value / 1e9 / peak}
+            "step_bytes_per_face": STEP_BYTES[(args.precision, D)],
+            "step_frac": STEP_BYTES[(args.precision, D)] * value / 1e9 / peak}
 
     # end to end through the C ABI with host buffers: per step upload W and Q
     # from host memory, one step, download W and Q
@@ -1235,7 +1312,9 @@ def main():
             "config": {"workload": problem_text(args, pr),
                        "solver": pr.solver, "precision": args.precision,
                        "lanes_per_cell": lanes,
-                       "l2": "working set > L2 (no flush)",
+                       "l2": ("working set > L2 (no flush)" if flush is None else
+                              "L2 flushed between steps (256 MB write outside the timed "
+                              "events; step times summed)"),
                        "parallelism": f"replicas x{world}"},
             "clocks": clk.summary(),
             "roofline": roof,

@@ -201,7 +201,9 @@ int sfx_step(sfx_mesh* mesh, double dt, int32_t nsteps, sfx_stats* stats);
  * The tessellation is then stale: `positions` ([n_cells][dim] host, may be
  * NULL) receives the drifted generators, from which the caller builds the
  * next face list, as the reference re-tessellates after every drift.
- * SFX_ERR_UNSUPPORTED for split-precision meshes, clones and parts. */
+ * Split-precision meshes take the boost into the face frame in FP32 and the
+ * reference's de-boost of each solver's flux; the velocities and the drift
+ * stay FP64.  SFX_ERR_UNSUPPORTED for clones and parts. */
 int sfx_step_moving(sfx_mesh* mesh, double dt, int32_t periodic, double* positions,
                     sfx_stats* stats);
 
@@ -274,10 +276,16 @@ int64_t sfx_mesh_clone_bytes(sfx_mesh* base, int32_t precision);
  * kernels (1, 2, 4, 8 or 16; default 1 in 2D, 4 in 3D).  Changes the summation
  * tree of the per-cell sums, not the algorithm. */
 int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
-/* split pass: register cap of the face kernel, 0 (64 registers, four
- * 256-thread blocks per SM; the default) or 1 (80 registers, three blocks).
- * Changes the schedule only, not the results. */
-#define SFX_FACE_VARIANTS 2
+/* split pass: face-kernel variant: 0 (64 registers, four 256-thread blocks
+ * per SM; the default), 1 (80 registers, three blocks), 2 (HLLC: the
+ * half-step prediction's dW/dt read from the per-cell record instead of
+ * formed per face; exact solver with gamma = 5/3: the p* step's powers as a
+ * fifth root by Newton's method and the sampling's powers as integer powers;
+ * other gamma: as 0), 3 (exact solver with gamma = 5/3: 2 with 80
+ * registers; other gamma and HLLC: as 1).  Variants 0 and 1 change the
+ * schedule only, not the results; 2 and 3 change round-off within the split
+ * pass's tolerance. */
+#define SFX_FACE_VARIANTS 4
 int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
 
 /* ---- one mesh over several devices (plain FP64) ----

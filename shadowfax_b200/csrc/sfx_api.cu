@@ -142,6 +142,8 @@ int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t 
         g.dim = m->d.dim;
         g.lanes = m->d.lanes;
         g.face_variant = m->d.face_variant;
+        g.moving = m->d.vel != nullptr ? 1 : 0; /* split meshes get face velocities
+                                                   only from sfx_step_moving */
         sfx_split_blocks(m->d.dim, m->d.lanes, m->d.n_cells, m->d.n_faces, g.blocks);
         return sfx_split_group_phase(&g, phase, &c->sp, s);
     }
@@ -687,16 +689,23 @@ int sfx_step_moving(sfx_mesh* m, double dt, int32_t periodic, double* positions,
                     sfx_stats* st) {
     if(!m || !(dt > 0.)) return SFX_ERR_INVALID;
     sfx_ctx* c = m->ctx;
-    if(c->cfg.precision != SFX_PREC_FP64 || m->clone || m->d.ranged) return SFX_ERR_UNSUPPORTED;
+    if(m->clone || m->d.ranged) return SFX_ERR_UNSUPPORTED;
+    const bool split = c->cfg.precision == SFX_PREC_SPLIT;
     cudaStream_t s = c->stream;
     sfx_dmesh& d = m->d;
     const int64_t n = d.n_cells, F = d.n_faces;
     const int D = d.dim;
     if(!d.vgen) SFX_TRY(dalloc(m, &d.vgen, (size_t)D * n));
     if(!d.newpos) SFX_TRY(dalloc(m, &d.newpos, (size_t)D * n));
-    if(!d.vel) SFX_TRY(dalloc(m, &d.vel, (size_t)D * (F > 0 ? F : 1)));
+    const bool fresh = d.vel == nullptr;
+    if(fresh) SFX_TRY(dalloc(m, &d.vel, (size_t)D * (F > 0 ? F : 1)));
     d.has_velocity = 1;
     SFX_TRY(reset_err(m));
+    /* the split pass keeps the state in FP32 cell records: the FP64 W the
+     * velocity kernels read is exported from them first; the device copy of
+     * the mesh (the one-member group table) learns the face velocities */
+    if(split) SFX_TRY(sfx_split_export_W(&d, s));
+    if(split && fresh) SFX_TRY(setup_self(m, s));
     SFX_TRY(sfx_fp64_move_velocities(&d, c->cfg.gamma, dt, periodic ? 1 : 0, 1, s));
     for(int ph = 0; ph < 3; ++ph) SFX_TRY(run_phase(m, ph, dt, 0, s));
     SFX_TRY(sfx_fp64_drift(&d, dt, s));

@@ -344,7 +344,12 @@ extern "C" int sfx_group_tune_faces(sfx_group* g, int32_t reps, int32_t* variant
     int best = g->dev.face_variant;
     float best_ms = 1e30f;
     int rc = SFX_OK;
+    bool timed[SFX_FACE_VARIANTS] = {};
     for(int v = 0; v < SFX_FACE_VARIANTS && !rc; ++v) {
+        /* a variant that runs an already timed kernel is not timed again */
+        const int k = sfx_split_face_variant_kernel(sp, v);
+        if(timed[k]) continue;
+        timed[k] = true;
         g->dev.face_variant = v;
         float total = 0.f;
         /* every face launch follows a gradient launch, which also empties

@@ -159,7 +159,8 @@ struct sfx_group_dev {
     int32_t n_meshes;
     int32_t dim;
     int32_t lanes; /* lanes per cell of the gradient and update kernels */
-    int32_t face_variant; /* 0: 64 registers (4 blocks per SM), 1: 80 (3 blocks) */
+    int32_t face_variant; /* SFX_FACE_VARIANTS (include/sfxflux.h) */
+    int32_t moving;       /* a moving mesh stepped alone: face kernels with the boost */
     int32_t blocks[3];
 };
 
@@ -264,6 +265,9 @@ inline int sfx_default_lanes(int dim) {
 
 /* grouped launches (sfx_split.cu) */
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);
+/* the face-kernel variant that variant `variant` runs for this solver (the
+ * variants that do not apply to it run another one's kernel) */
+int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant);
 int sfx_split_group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                           void* stream);
 int sfx_split_group_reset(const sfx_group_dev* g, void* stream);

@@ -123,7 +123,8 @@ __device__ __forceinline__ void sdwdt(float gamma, const float* W, const float (
 template <int D, bool STORED>
 __device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
                                           const float4* __restrict__ cdw, int i, float gamma,
-                                          const float* W, float (*g)[D + 2], float* dWdt) {
+                                          const float* W, float (*g)[D + 2], float* dWdt,
+                                          bool boosted = false) {
     constexpr int S = D + 2, G = GradVec4<D>::value, H = DwdtVec4<D>::value;
     float t[4 * G];
 #pragma unroll
@@ -138,7 +139,7 @@ __device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
     for(int l = 0; l < D; ++l)
 #pragma unroll
         for(int k = 0; k < S; ++k) g[l][k] = t[l * S + k];
-    if(STORED) {
+    if(STORED && !boosted) {
         float u[4 * H];
 #pragma unroll
         for(int q = 0; q < H; ++q) {
@@ -594,8 +595,12 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
     for(int l = 0; l < D; ++l) F.mv[l] = zero;
     if(WL[0] == zero && (reflective || WRin[0] == zero)) return;
     /* the reflective right state is the left state with its normal velocity
-     * reversed (only u_R enters below) */
-    const T* WR = reflective ? WL : WRin;
+     * reversed (only u_R enters below).  States are selected by value, element
+     * by element: a select between two arrays' addresses would keep both
+     * arrays in local memory */
+    T WR[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) WR[k] = reflective ? WL[k] : WRin[k];
     T uL = zero, uR = zero;
 #pragma unroll
     for(int l = 0; l < D; ++l) uL += WL[1 + l] * n[l];
@@ -613,9 +618,8 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
         T sol[S], vhalf = zero;
         const T tdgp1 = two / (g + one), gm1dgp1 = gm1 / (g + one);
         bool vac = false, fan = false;
-        const T* Ws = WL;
+        bool sright = false; /* the sampled state is the right one */
         if(WR[0] == zero) {
-            Ws = WL;
             if(aL > uL) {
                 if(uL + two * aL / gm1 > zero) {
                     /* base > 0 in exact arithmetic on this branch */
@@ -631,7 +635,7 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
                 }
             }
         } else if(WL[0] == zero) {
-            Ws = WR;
+            sright = true;
             if(-uR < aR) {
                 if(uR - two * aR / gm1 >= zero) {
                     vac = true;
@@ -650,7 +654,6 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
             if(SR > zero && SL < zero) {
                 vac = true;
             } else if(SL >= zero) {
-                Ws = WL;
                 if(aL > uL) {
                     const T base = R::max_(zero, tdgp1 + gm1dgp1 / aL * uL);
                     vhalf = tdgp1 * (aL + half * gm1 * uL) - uL;
@@ -661,7 +664,7 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
                     fan = true;
                 }
             } else {
-                Ws = WR;
+                sright = true;
                 if(-uR < aR) {
                     const T base = R::max_(zero, tdgp1 - gm1dgp1 / aR * uR);
                     vhalf = tdgp1 * (-aR + half * gm1 * uR) - uR;
@@ -676,7 +679,7 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
         if(vac) return;
         if(!fan) {
 #pragma unroll
-            for(int k = 0; k < S; ++k) sol[k] = Ws[k];
+            for(int k = 0; k < S; ++k) sol[k] = sright ? WR[k] : WL[k];
         }
 #pragma unroll
         for(int l = 0; l < D; ++l) sol[1 + l] += vhalf * n[l];
@@ -709,7 +712,9 @@ __device__ __forceinline__ void thllc(T g, const T* WL, const T* WRin, const T* 
     const T Sstar = (WR[D + 1] - WL[D + 1] + WL[0] * uL * (SL - uL) - WR[0] * uR * (SR - uR)) /
                     (WL[0] * (SL - uL) - WR[0] * (SR - uR));
     const bool left = Sstar >= zero;
-    const T* Wk = left ? WL : WR;
+    T Wk[S];
+#pragma unroll
+    for(int k = 0; k < S; ++k) Wk[k] = left ? WL[k] : WR[k];
     const T uk = left ? uL : uR;
     const T Sk = left ? SL : SR;
     T v2 = zero;
@@ -764,16 +769,15 @@ __device__ __noinline__ SFlux<D> shllc_fp64(float g, FaceStates<D> in, bool refl
     return F;
 }
 
-/* FP32 HLLC; a face whose FP32 flux is not finite is solved again in FP64 */
-template <int D>
-__device__ __forceinline__ void shllc(float g, const float* WL, const float* WR, const float* n,
+/* HLLC on the predicted FP32 states.  kSolveDefer: in FP32; false when
+ * that flux is not finite, and the face is then queued for the FP64 solve
+ * (k_group_sfaces_slow).  kSolveInline: in FP64 (the queued faces).  The
+ * FP64 solve stays out of the FP32 kernel: a call from it, or its code
+ * inline, costs that kernel a stack frame and spills on every face. */
+template <int D, int MODE>
+__device__ __forceinline__ bool shllc(float g, const float* WL, const float* WR, const float* n,
                                       bool reflective, SFlux<D>& F) {
-    TFlux<D, float> G;
-    thllc<D, float>(g, WL, WR, n, reflective, G);
-    float mvs = 0.f;
-#pragma unroll
-    for(int l = 0; l < D; ++l) mvs += G.mv[l];
-    if(__builtin_expect(!finite4(G.m, G.P, G.E, mvs), 0)) {
+    if(MODE == kSolveInline) {
         FaceStates<D> in;
 #pragma unroll
         for(int k = 0; k < D + 2; ++k) {
@@ -783,13 +787,20 @@ __device__ __forceinline__ void shllc(float g, const float* WL, const float* WR,
 #pragma unroll
         for(int l = 0; l < D; ++l) in.n[l] = n[l];
         F = shllc_fp64<D>(g, in, reflective);
-        return;
+        return true;
     }
+    TFlux<D, float> G;
+    thllc<D, float>(g, WL, WR, n, reflective, G);
+    float mvs = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) mvs += G.mv[l];
+    if(__builtin_expect(!finite4(G.m, G.P, G.E, mvs), 0)) return false;
     F.m = G.m;
 #pragma unroll
     for(int l = 0; l < D; ++l) F.mv[l] = G.mv[l];
     F.P = G.P;
     F.E = G.E;
+    return true;
 }
 
 /* exact solver half state in FP64 (ExactRiemannSolver.cpp:108-446, 644-673,
@@ -847,8 +858,25 @@ struct XS {
  * takes a Newton step to (nearly) zero pressure (where the reference's
  * iteration can stop at p = 0), when the FP64 step is not small, or when it
  * moves a side between shock and rarefaction. */
+/* x^(1/5) for normal x > 0 without a division or a power: w ~ x^(-1/5) from
+ * the FP32 hardware log2/exp2, two Newton steps for w^-5 = x, w <- w (6 -
+ * x w^5) / 5 (quadratic convergence from ~1e-7 to below 1e-16), then
+ * x w^4 = x^(1/5) */
+__device__ __forceinline__ double fifth_root(double x) {
+    double w = (double)exp2f(-0.2f * __log2f((float)x));
+#pragma unroll
+    for(int it = 0; it < 2; ++it) {
+        const double w2 = w * w;
+        w = w * (6. - x * (w2 * w2 * w)) * 0.2;
+    }
+    const double w2 = w * w;
+    return x * (w2 * w2);
+}
+
 /* f_K, f_K' and z_K = (p/p_K)^((g-1)/(2g)) (rarefaction side) of one side in
- * FP64 (XS::side without the shared power) */
+ * FP64 (XS::side without the shared power); G53: gamma = 5/3, where the
+ * exponent is 1/5 and z_K is a fifth root */
+template <bool G53 = false>
 __device__ __forceinline__ void side64(const sfx_solver_params& s, double p, double rho,
                                        double pK, double a, double& f, double& fp, double& z) {
     if(p > pK) {
@@ -858,10 +886,12 @@ __device__ __forceinline__ void side64(const sfx_solver_params& s, double p, dou
         fp = (1. - 0.5 * (p - pK) / (B + p)) * q;
         z = 0.;
     } else {
+        /* p is a positive FP32 root and p_K < 1e12 (fast_root's range), so
+         * r > 1e-57: no zero-pressure branch (and no power call for it) */
         const double r = p / pK;
-        z = xpow(r, s.gm1d2g);
+        z = G53 ? fifth_root(r) : xpow(r, s.gm1d2g);
         f = s.tdgm1 * a * (z - 1.);
-        fp = r > 0. ? z / (r * (rho * a)) : 1. / (rho * a) * xpow(r, -s.gp1d2g);
+        fp = z / (r * (rho * a));
     }
 }
 
@@ -878,6 +908,7 @@ __device__ __forceinline__ void side64(const sfx_solver_params& s, double p, dou
  * takes a Newton step to (nearly) zero pressure (where the reference's
  * iteration can stop at p = 0), when the FP64 step is not small, or when it
  * moves a side between shock and rarefaction. */
+template <bool G53 = false>
 __device__ __forceinline__ bool fast_root(const sfx_solver_params& s, double rL, double pL,
                                           double rR, double pR, double aL, double aR, double vL,
                                           double vR, double& p, double& fL, double& fR,
@@ -933,8 +964,8 @@ __device__ __forceinline__ bool fast_root(const sfx_solver_params& s, double rL,
     }
     const double p0 = (double)pg;
     double fpl, fpr;
-    side64(s, p0, rL, pL, aL, fL, fpl, zL);
-    side64(s, p0, rR, pR, aR, fR, fpr, zR);
+    side64<G53>(s, p0, rL, pL, aL, fL, fpl, zL);
+    side64<G53>(s, p0, rR, pR, aR, fR, fpr, zR);
     const double dp = -(fL + fR + (vR - vL)) / (fpl + fpr);
     const double p1 = p0 + dp;
     if(!(fabs(dp) <= 1e-5 * p0) || (p0 > pL) != (p1 > pL) || (p0 > pR) != (p1 > pR))
@@ -984,9 +1015,8 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
         else
             side = -aR < vR ? 4 : 3;
         if(side == 0) return SFX_OK;
-        const double* Ws = side <= 2 ? WL : WR;
 #pragma unroll
-        for(int k = 0; k < S; ++k) sol[k] = Ws[k];
+        for(int k = 0; k < S; ++k) sol[k] = side <= 2 ? WL[k] : WR[k];
         if(side == 2) {
             const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
             sol[0] = WL[0] * xpow(base, s.tdgm1);
@@ -1178,12 +1208,13 @@ template <int D>
 struct FaceWork {
     float WL[D + 2], WR[D + 2], n[D];
     float A, limL, limR;
+    float v[D]; /* face velocity (moving mesh; 0 on a static one) */
     bool mirror;
 };
 
 /* false: nothing to solve (a face past the end, or of zero area, whose dQ is
  * written as zero here) */
-template <int D, bool STORED>
+template <int D, bool STORED, bool MOVING = false>
 __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma, const float hdt,
                                           const int f, FaceWork<D>& w) {
     constexpr int S = D + 2;
@@ -1212,6 +1243,14 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         w.WR[k] = 0.f;
         WRr[k] = 0.f;
     }
+    /* a moving mesh: both states in the face's frame (WL -= v, WR -= v,
+     * VorFace.cpp:703-710); dW/dt then at the boosted states, per face */
+    constexpr bool moving = MOVING;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        w.v[l] = MOVING ? (float)__ldg(m.vel + (size_t)l * m.n_faces + f) : 0.f;
+        if(MOVING) w.WL[1 + l] -= w.v[l];
+    }
     w.limL = w.A / cL.tarea * cL.Qm;
     w.limR = 0.f;
     float rr = 1.f;
@@ -1221,6 +1260,10 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         const float xmcR[3] = {xR.x, xR.y, xR.z};
 #pragma unroll
         for(int k = 0; k < S; ++k) w.WR[k] = cR.W[k];
+        if(MOVING) {
+#pragma unroll
+            for(int l = 0; l < D; ++l) w.WR[1 + l] -= w.v[l];
+        }
         w.limR = w.A / cR.tarea * cR.Qm;
         /* centroid difference (unshifted centroids, as the reference) */
         float sh[D];
@@ -1243,7 +1286,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         }
         rr = sqrtf(cd2);
         float gR[D][S], dWR[S];
-        load_grad<D, STORED>(m.cg, m.cdw, iR, gamma, w.WR, gR, dWR);
+        load_grad<D, STORED>(m.cg, m.cdw, iR, gamma, w.WR, gR, dWR, moving);
 #pragma unroll
         for(int k = 0; k < S; ++k) WRr[k] = w.WR[k];
         spredict<D>(hdt, WRr, w.WR, w.WL, gR, dWR, dR, true, rr);
@@ -1252,7 +1295,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         float dL[D], gL[D][S], dWL[S];
 #pragma unroll
         for(int l = 0; l < D; ++l) dL[l] = c[l] + xmcL[l] - 0.5f * r[l];
-        load_grad<D, STORED>(m.cg, m.cdw, iL, gamma, w.WL, gL, dWL);
+        load_grad<D, STORED>(m.cg, m.cdw, iL, gamma, w.WL, gL, dWL, moving);
 #pragma unroll
         for(int k = 0; k < S; ++k) WLr[k] = w.WL[k];
         spredict<D>(hdt, WLr, w.WL, w.WR, gL, dWL, dL, !w.mirror, rr);
@@ -1272,27 +1315,50 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
  * :815-880) from its half state */
 template <int D>
 __device__ __forceinline__ void exact_flux(double gamma, const double* h, const double* dn,
-                                           SFlux<D>& F) {
+                                           const float* v, bool moving, SFlux<D>& F) {
+    /* h is the half state in the face's frame; the lab-frame velocity is
+     * h + v: mass flux rho (h.n), momentum (rho h.n)(h + v) + p n, energy
+     * (h.n) e_lab + p (h + v).n (ExactRiemannSolver::get_flux with the face
+     * velocity) */
     F.m = 0.f;
     F.P = 0.f;
     F.E = 0.f;
 #pragma unroll
     for(int l = 0; l < D; ++l) F.mv[l] = 0.f;
     if(h[0] != 0.) {
-        double un = 0., v2 = 0.;
+        double un = 0., v2 = 0., vn = 0.;
+        double hl[D];
 #pragma unroll
         for(int l = 0; l < D; ++l) {
+            hl[l] = h[1 + l] + (double)v[l];
             un += h[1 + l] * dn[l];
-            v2 += h[1 + l] * h[1 + l];
+            vn += (double)v[l] * dn[l];
+            v2 += hl[l] * hl[l];
         }
         const double e = 0.5 * h[0] * v2 + h[D + 1] / (gamma - 1.);
         const double mf = h[0] * un;
         F.m = (float)mf;
 #pragma unroll
-        for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * h[1 + l]);
+        for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * hl[l]);
         F.P = (float)h[D + 1];
-        F.E = (float)((e + h[D + 1]) * un);
+        F.E = moving ? (float)(e * un + h[D + 1] * (un + vn)) : (float)((e + h[D + 1]) * un);
     }
+}
+
+/* the reference's HLLC de-boost (HLLCRiemannSolver.cpp:392-400): the
+ * momentum flux gains v F_m, then the energy flux gains v . (the updated
+ * momentum flux) + v^2 F_m / 2 */
+template <int D>
+__device__ __forceinline__ void hllc_deboost_split(const float* v, const float* n,
+                                                   SFlux<D>& F) {
+    float vm = 0.f, v2 = 0.f;
+#pragma unroll
+    for(int l = 0; l < D; ++l) {
+        F.mv[l] += v[l] * F.m;
+        vm += v[l] * (F.mv[l] + F.P * n[l]);
+        v2 += v[l] * v[l];
+    }
+    F.E += vm + 0.5f * v2 * F.m;
 }
 
 /* Last phase of every face kernel: dt A flux with the over-flux limiter, the
@@ -1342,18 +1408,23 @@ __device__ __forceinline__ void face_dq(const sfx_dmesh& m, const float dt, cons
     if(status != SFX_OK) report_face(m.err, f, status);
 }
 
-template <int D, int SOLVER, int MODE>
-__device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
+/* one face; true when the face is left for the queued-face kernel (HLLC in
+ * kSolveDefer mode whose FP32 flux is not finite) */
+template <int D, int SOLVER, int MODE, bool STORED_DW = SOLVER != SFX_SOLVER_HLLC,
+          bool MOVING = false>
+__device__ __forceinline__ bool sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
                                             const float dt, const int f) {
     constexpr int S = D + 2;
-    if(f >= m.n_faces || failed(m.err)) return;
+    if(f >= m.n_faces || failed(m.err)) return false;
     FaceWork<D> w;
-    /* HLLC forms dW/dt itself; the exact solver's kernels read it */
-    if(!face_work<D, SOLVER != SFX_SOLVER_HLLC>(m, (float)sp.gamma, 0.5f * dt, f, w)) return;
+    /* by default HLLC forms dW/dt itself and the exact solver's kernels read
+     * it (STORED_DW: from the per-cell record) */
+    if(!face_work<D, STORED_DW, MOVING>(m, (float)sp.gamma, 0.5f * dt, f, w)) return false;
     SFlux<D> F;
     int status = SFX_OK;
-    if(SOLVER == SFX_SOLVER_HLLC) {
-        shllc<D>((float)sp.gamma, w.WL, w.WR, w.n, w.mirror, F);
+    if constexpr(SOLVER == SFX_SOLVER_HLLC) {
+        if(!shllc<D, MODE>((float)sp.gamma, w.WL, w.WR, w.n, w.mirror, F)) return true;
+        if(MOVING) hllc_deboost_split<D>(w.v, w.n, F);
     } else {
         double dWL[S], dWR[S], dn[D], h[S];
 #pragma unroll
@@ -1365,9 +1436,10 @@ __device__ __forceinline__ void sfaces_body(const sfx_dmesh& m, const sfx_solver
         }
         static_assert(MODE == kSolveInline, "queued faces come from k_group_sfaces_exact");
         status = sexact<D, MODE>(sp, dWL, dWR, dn, w.mirror, h);
-        exact_flux<D>(sp.gamma, h, dn, F);
+        exact_flux<D>(sp.gamma, h, dn, w.v, MOVING, F);
     }
     face_dq<D>(m, dt, f, w, F, status);
+    return false;
 }
 
 /* -------------------- exact solver: faces sorted by wave pattern --------------------
@@ -1429,13 +1501,18 @@ __device__ __forceinline__ int wave_class(const sfx_solver_params& s, const Face
 /* phase 3: p* by fast_root and the sampled half state; kDefer when the face
  * needs the FP64 iteration or is a vacuum case, SFX_ERR_RIEMANN for an
  * unphysical half state, SFX_OK otherwise */
-template <int D>
+/* G53: gamma = 5/3, where the sampling's powers are integers in z_K or in
+ * the fan's base: (p/p_K)^(1/g) = z_K^3, base^(2/(g-1)) = base^3,
+ * base^(2g/(g-1)) = base^5 */
+template <int D, bool G53 = false>
 __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const FaceWork<D>& w,
-                                          SFlux<D>& F) {
+                                          bool moving, SFlux<D>& F) {
     /* a reflective right state is the left state with the normal velocity
      * reversed: only its normal velocity enters, and of its flux only the
      * pressure survives (face_dq) */
-    const float* WRf = w.mirror ? w.WL : w.WR;
+    float WRf[D + 2];
+#pragma unroll
+    for(int k = 0; k < D + 2; ++k) WRf[k] = w.mirror ? w.WL[k] : w.WR[k];
     double vL = 0., vR = 0.;
 #pragma unroll
     for(int l = 0; l < D; ++l) {
@@ -1449,7 +1526,7 @@ __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const Face
     const double aR = sqrt(g * pR / rR);
     if(s.tdgm1 * (aL + aR) <= vR - vL) return kDefer;
     double p, fL, fR, zL, zR;
-    if(!fast_root(s, rL, pL, rR, pR, aL, aR, vL, vR, p, fL, fR, zL, zR)) return kDefer;
+    if(!fast_root<G53>(s, rL, pL, rR, pR, aL, aR, vL, vR, p, fL, fR, zL, zR)) return kDefer;
     /* sampling at x/t = 0 (ExactRiemannSolver.cpp:178-265): the side, the
      * half state's density and pressure, and its velocity shift along n */
     const double u = 0.5 * (vL + vR) + 0.5 * (fR - fL);
@@ -1466,11 +1543,12 @@ __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const Face
         } else if(vR + aR > 0.) {
             if(u + aR * zR <= 0.) {
                 const double base = s.tdgp1 - s.gm1dgp1 / aR * vR;
-                srho = rR * xpow(base, s.tdgm1);
+                const double b3 = base * base * base;
+                srho = rR * (G53 ? b3 : xpow(base, s.tdgm1));
                 vhalf = s.tdgp1 * (-aR + s.gm1d2 * vR) - vR;
-                spr = pR * xpow(base, s.tgdgm1);
+                spr = pR * (G53 ? b3 * base * base : xpow(base, s.tgdgm1));
             } else {
-                srho = rR * xpow(r, s.ginv);
+                srho = rR * (G53 ? zR * zR * zR : xpow(r, s.ginv));
                 spr = p;
                 vhalf = u - vR;
             }
@@ -1486,26 +1564,29 @@ __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const Face
         } else if(vL - aL < 0.) {
             if(u - aL * zL > 0.) {
                 const double base = s.tdgp1 + s.gm1dgp1 / aL * vL;
-                srho = rL * xpow(base, s.tdgm1);
+                const double b3 = base * base * base;
+                srho = rL * (G53 ? b3 : xpow(base, s.tdgm1));
                 vhalf = s.tdgp1 * (aL + s.gm1d2 * vL) - vL;
-                spr = pL * xpow(base, s.tgdgm1);
+                spr = pL * (G53 ? b3 * base * base : xpow(base, s.tgdgm1));
             } else {
-                srho = rL * xpow(r, s.ginv);
+                srho = rL * (G53 ? zL * zL * zL : xpow(r, s.ginv));
                 spr = p;
                 vhalf = u - vL;
             }
         }
     }
-    /* the half state's velocity and its flux (ExactRiemannSolver::get_flux
-     * contracted with n, :815-880) */
-    const float* Wk = right ? WRf : w.WL;
-    double hv[D], un = 0., v2 = 0.;
+    /* the half state's velocity (in the face's frame; + v in the lab frame)
+     * and its flux (ExactRiemannSolver::get_flux contracted with n,
+     * :815-880) */
+    double hv[D], un = 0., v2 = 0., vn = 0.;
     bool bad = !(srho >= 0.) || !(spr >= 0.);
 #pragma unroll
     for(int l = 0; l < D; ++l) {
-        hv[l] = (double)Wk[1 + l] + vhalf * (double)w.n[l];
+        hv[l] = (double)(right ? WRf[1 + l] : w.WL[1 + l]) + vhalf * (double)w.n[l];
         bad |= hv[l] != hv[l];
         un += hv[l] * (double)w.n[l];
+        hv[l] += (double)w.v[l];
+        vn += (double)w.v[l] * (double)w.n[l];
         v2 += hv[l] * hv[l];
     }
     F.m = 0.f;
@@ -1520,7 +1601,7 @@ __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const Face
 #pragma unroll
         for(int l = 0; l < D; ++l) F.mv[l] = (float)(mf * hv[l]);
         F.P = (float)spr;
-        F.E = (float)((e + spr) * un);
+        F.E = moving ? (float)(e * un + spr * (un + vn)) : (float)((e + spr) * un);
     }
     return bad ? SFX_ERR_RIEMANN : SFX_OK;
 }
@@ -1648,7 +1729,7 @@ __device__ __forceinline__ bool member_done(const sfx_group_entry* tab, int mi) 
     return sl && *(volatile const int32_t*)sl <= 0;
 }
 
-template <int D, int MINB>
+template <int D, int MINB, bool MOVING = false, bool G53 = false>
 __global__ void __launch_bounds__(kExactBlock, MINB)
         k_group_sfaces_exact(const sfx_group_entry* tab, const int* pre, int nm,
                              sfx_solver_params sp) {
@@ -1658,6 +1739,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
      * (bit 31: mirror) */
     __shared__ float sW[2 * S][kExactBlock];
     __shared__ float sn[D][kExactBlock];
+    __shared__ float sv[MOVING ? D : 1][MOVING ? kExactBlock : 1];
     __shared__ float sA[kExactBlock], sLL[kExactBlock], sLR[kExactBlock];
     __shared__ int sf[kExactBlock];
     __shared__ int sbase[kNClass][NW];
@@ -1672,7 +1754,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     FaceWork<D> w;
     int cls = kClassNone;
     if(f < m.n_faces && !failed(m.err) &&
-       face_work<D, true>(m, (float)sp.gamma, 0.5f * dt, f, w))
+       face_work<D, true, MOVING>(m, (float)sp.gamma, 0.5f * dt, f, w))
         cls = wave_class<D>(sp, w);
     queue_faces(m, cls == kClassQueue, f);
     /* phase 2: counting sort by class */
@@ -1708,7 +1790,10 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
             sW[S + k][slot] = w.WR[k];
         }
 #pragma unroll
-        for(int l = 0; l < D; ++l) sn[l][slot] = w.n[l];
+        for(int l = 0; l < D; ++l) {
+            sn[l][slot] = w.n[l];
+            if(MOVING) sv[MOVING ? l : 0][MOVING ? slot : 0] = w.v[l];
+        }
         sA[slot] = w.A;
         sLL[slot] = w.limL;
         sLR[slot] = w.limR;
@@ -1727,7 +1812,10 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
             v.WR[k] = sW[S + k][t];
         }
 #pragma unroll
-        for(int l = 0; l < D; ++l) v.n[l] = sn[l][t];
+        for(int l = 0; l < D; ++l) {
+            v.n[l] = sn[l][t];
+            v.v[l] = MOVING ? sv[MOVING ? l : 0][MOVING ? t : 0] : 0.f;
+        }
         v.A = sA[t];
         v.limL = sLL[t];
         v.limR = sLR[t];
@@ -1735,7 +1823,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
         v.mirror = e < 0;
         fq = e & 0x7fffffff;
         SFlux<D> F;
-        const int st = exact_fast<D>(sp, v, F);
+        const int st = exact_fast<D, G53>(sp, v, MOVING, F);
         if(st == kDefer)
             push = true;
         else
@@ -1753,26 +1841,33 @@ __global__ void __launch_bounds__(256, 4) k_group_sgrad(const sfx_group_entry* t
                        (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
-template <int D, int SOLVER, int MINB>
+template <int D, int SOLVER, int MINB, bool STORED_DW = SOLVER != SFX_SOLVER_HLLC,
+          bool MOVING = false>
 __global__ void __launch_bounds__(256, MINB)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
+    static_assert(SOLVER == SFX_SOLVER_HLLC, "the exact solver has k_group_sfaces_exact");
     const int mi = group_mesh_of_block(pre, nm);
-    if(member_done(tab, mi)) return;
-    sfaces_body<D, SOLVER, kSolveInline>(
-            tab[mi].m, sp, tab[mi].dt, (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+    if(member_done(tab, mi)) return; /* the same for every thread of the block */
+    const sfx_dmesh& m = tab[mi].m;
+    const int f = (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x;
+    const bool push =
+            sfaces_body<D, SOLVER, kSolveDefer, STORED_DW, MOVING>(m, sp, tab[mi].dt, f);
+    queue_faces(m, push, f);
 }
 
-/* The queued exact-solver faces of every member, one per thread: the FP64
- * iteration from the reference's guess (the monotone Newton search where
- * the reference runs Brent's method) and the vacuum cases.  Each block reads
+/* The queued faces of every member, one per thread.  Exact solver: the
+ * FP64 iteration from the reference's guess (the monotone Newton search
+ * where the reference runs Brent's method) and the vacuum cases.  HLLC: the
+ * FP64 solve of faces whose FP32 flux was not finite.  Each block reads
  * the members' queue lengths (kSlowChunk members at a time, in parallel),
  * forms their prefix sums in shared memory and strides over the flattened
  * list, finding a slot's member by binary search: no thread walks the
  * member list. */
 constexpr int kSlowBlock = 128, kSlowChunk = 2048, kSlowPer = kSlowChunk / kSlowBlock;
 
-template <int D>
+template <int D, bool MOVING = false, int SOLVER = SFX_SOLVER_EXACT,
+          bool STORED_DW = SOLVER == SFX_SOLVER_EXACT>
 __global__ void __launch_bounds__(kSlowBlock) k_group_sfaces_slow(const sfx_group_entry* tab,
                                                                  int nm, sfx_solver_params sp) {
     __shared__ int spre[kSlowChunk + 1];
@@ -1827,8 +1922,8 @@ __global__ void __launch_bounds__(kSlowBlock) k_group_sfaces_slow(const sfx_grou
                     hi = mid;
             }
             const sfx_group_entry& e = tab[base + lo];
-            sfaces_body<D, SFX_SOLVER_EXACT, kSolveInline>(e.m, sp, e.dt,
-                                                            __ldg(e.m.slowq + (j - spre[lo])));
+            sfaces_body<D, SOLVER, kSolveInline, STORED_DW, MOVING>(
+                    e.m, sp, e.dt, __ldg(e.m.slowq + (j - spre[lo])));
         }
         __syncthreads(); /* spre and swarp are rewritten by the next chunk */
     }
@@ -1873,22 +1968,56 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                                                                 (float)sp->gamma);
     } else if(phase == 1) {
         if(g->blocks[1]) {
-            if(sp->kind == SFX_SOLVER_EXACT) {
-                if(g->face_variant == 1)
+            const int* pre1 = g->pre + (nm + 1);
+            if(g->moving) {
+                /* a moving mesh stepped alone: the face kernels with the boost */
+                if(sp->kind == SFX_SOLVER_EXACT) {
+                    k_group_sfaces_exact<D, 4, true><<<g->blocks[1], kExactBlock, 0, s>>>(
+                            g->tab, pre1, nm, *sp);
+                    k_group_sfaces_slow<D, true><<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(
+                            g->tab, nm, *sp);
+                } else {
+                    k_group_sfaces<D, SFX_SOLVER_HLLC, 4, false, true>
+                            <<<g->blocks[1], 256, 0, s>>>(g->tab, pre1, nm, *sp);
+                    k_group_sfaces_slow<D, true, SFX_SOLVER_HLLC>
+                            <<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
+                }
+                sfx_count_launches(1);
+            } else if(sp->kind == SFX_SOLVER_EXACT) {
+                const int v = sfx_split_face_variant_kernel(sp, g->face_variant);
+                if(v == 3)
+                    k_group_sfaces_exact<D, 3, false, true><<<g->blocks[1], kExactBlock, 0, s>>>(
+                            g->tab, pre1, nm, *sp);
+                else if(v == 2)
+                    k_group_sfaces_exact<D, 4, false, true><<<g->blocks[1], kExactBlock, 0, s>>>(
+                            g->tab, pre1, nm, *sp);
+                else if(v == 1)
                     k_group_sfaces_exact<D, 3><<<g->blocks[1], kExactBlock, 0, s>>>(
-                            g->tab, g->pre + (nm + 1), nm, *sp);
+                            g->tab, pre1, nm, *sp);
                 else
                     k_group_sfaces_exact<D, 4><<<g->blocks[1], kExactBlock, 0, s>>>(
-                            g->tab, g->pre + (nm + 1), nm, *sp);
+                            g->tab, pre1, nm, *sp);
                 k_group_sfaces_slow<D><<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
                 sfx_count_launches(1);
             } else {
-                if(g->face_variant == 1)
-                    k_group_sfaces<D, SFX_SOLVER_HLLC, 3><<<g->blocks[1], 256, 0, s>>>(
-                            g->tab, g->pre + (nm + 1), nm, *sp);
-                else
-                    k_group_sfaces<D, SFX_SOLVER_HLLC, 4><<<g->blocks[1], 256, 0, s>>>(
-                            g->tab, g->pre + (nm + 1), nm, *sp);
+                /* HLLC; then the faces whose FP32 flux was not finite, in FP64 */
+                const int v = sfx_split_face_variant_kernel(sp, g->face_variant);
+                if(v == 2) {
+                    k_group_sfaces<D, SFX_SOLVER_HLLC, 4, true><<<g->blocks[1], 256, 0, s>>>(
+                            g->tab, pre1, nm, *sp);
+                    k_group_sfaces_slow<D, false, SFX_SOLVER_HLLC, true>
+                            <<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
+                } else {
+                    if(v == 1)
+                        k_group_sfaces<D, SFX_SOLVER_HLLC, 3><<<g->blocks[1], 256, 0, s>>>(
+                                g->tab, pre1, nm, *sp);
+                    else
+                        k_group_sfaces<D, SFX_SOLVER_HLLC, 4><<<g->blocks[1], 256, 0, s>>>(
+                                g->tab, pre1, nm, *sp);
+                    k_group_sfaces_slow<D, false, SFX_SOLVER_HLLC>
+                            <<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
+                }
+                sfx_count_launches(1);
             }
         }
     } else {
@@ -1952,6 +2081,16 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
     else
         k_export_dQ<2><<<grid_for(m->n_faces, 256), 256, 0, s>>>(*m);
     return launched(1);
+}
+
+int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant) {
+    if(variant < 0 || variant >= SFX_FACE_VARIANTS) return 0;
+    if(sp->kind == SFX_SOLVER_EXACT) {
+        /* the gamma = 5/3 forms (2: 64 registers, 3: 80) exist for that gamma only */
+        if(sp->gamma != 5. / 3. && variant >= 2) return variant - 2;
+        return variant;
+    }
+    return variant == 3 ? 1 : variant; /* HLLC: 3 is 1 */
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {

@@ -8,6 +8,7 @@ asks for a mesh cache (serve_pool's cache_dir).
   sod2d           2D Sod tube, reflective unit square, exact solver, dt = 1e-4, 100 steps
   sedov3d         3D Sedov-type blast, reflective unit cube, HLLC, global CFL 0.4, 50 steps
   random_field3d  3D supersonic random field, periodic unit cube, exact solver, one pass
+  random_field2d  the same field on a 2D periodic mesh
   batch2d         1,024 independent 2D step-state meshes, HLLC, 20 steps at own CFL dt
   serve_stream    Poisson request stream of static meshes (serving)
 """
@@ -87,6 +88,16 @@ def random_field3d(n: int = 2_097_152, seed: int = 3, solver: str = "Exact",
     W[:, 1:4] = rng.normal(0.0, 1.0, (n, 3))
     W[:, 4] = 1.0
     return Problem("random3d", mesh, W, solver, cfl_dt(mesh, W), nsteps)
+
+
+def random_field2d(n: int = 2_097_152, seed: int = 3, solver: str = "Exact",
+                   nsteps: int = 1) -> Problem:
+    """the random field on a 2D periodic mesh (the serving stream's 2D
+    requests' states): ln rho ~ N(-1/2, 1), p = 1, v_k ~ N(0, 1)"""
+    pos = random_generators(n, 2, seed)
+    mesh = build_voronoi(pos, periodic=True)
+    W = random_field_state(mesh, seed + 1000)
+    return Problem("random2d", mesh, W, solver, cfl_dt(mesh, W), nsteps)
 
 
 def step_state2d(n: int, seed: int, solver: str = "HLLC", nsteps: int = 20) -> Problem:

@@ -5,7 +5,7 @@ drift, against the reference built without -DSTATIC
 (tests/golden/moving_*.npz): drifted positions, W and Q bit for bit with
 sfx_pow and sfx_cbrt, within 1e-12 per field of the reference with glibc's
 pow and cbrt; the case where the reference throws UpdateQException fails
-with SFX_ERR_NEG_STATE."""
+with SFX_ERR_NEG_STATE; the split pass's moving step within 1e-6 of FP64."""
 import numpy as np
 import pytest
 
@@ -51,16 +51,31 @@ def test_moving_step_fails_where_the_reference_fails(cuda_ok):
     ctx.close()
 
 
-def test_moving_step_is_refused_where_unsupported(cuda_ok):
-    """split precision and clones share or lack what a moving step rewrites"""
-    from shadowfax_b200 import _lib as L
-    mesh, meta, _ = load_case(MOVING_CASES[0])
+@pytest.mark.parametrize("name", MOVING_CASES)
+def test_split_moving_step_within_tolerance_of_fp64(cuda_ok, name):
+    """the FP32/FP64 split pass with the boost: within 1e-6 relative L1 of the
+    plain FP64 moving step per conserved field, the drifted positions within
+    1e-9 (the velocities are formed in FP64 from the FP32-rounded state)"""
+    mesh, meta, ref = load_case(name)
     ctx, fp = _pass(mesh, meta, precision=1)
-    with pytest.raises(L.SfxError) as ei:
-        fp.step_moving(meta["dt"], mesh.periodic)
-    assert ei.value.status == L.SFX_ERR_UNSUPPORTED
+    pos = fp.step_moving(meta["dt"], mesh.periodic)
+    Q = fp.state()[1]
+    Q64 = ref["ref_sfxpow_Q"]
+    D = mesh.dim
+    den = np.abs(Q64).sum(0)
+    den[1:D + 1] = np.sqrt((Q64[:, 1:D + 1] ** 2).sum(1)).sum()
+    err = np.abs(Q - Q64).sum(0) / den
+    assert np.all(err <= 1e-6), err
+    assert np.abs(pos - ref["ref_sfxpow_pos"]).max() <= 1e-9
+    assert abs(Q[:, 0].sum() - Q64[:, 0].sum()) <= 1e-13 * Q64[:, 0].sum()
     fp.close()
     ctx.close()
+
+
+def test_moving_step_is_refused_on_clones(cuda_ok):
+    """a clone shares its base's geometry, which a moving step rewrites"""
+    from shadowfax_b200 import _lib as L
+    mesh, meta, _ = load_case(MOVING_CASES[0])
     ctx, fp = _pass(mesh, meta)
     clone = fp.clone(ctx)
     with pytest.raises(L.SfxError) as ei:
