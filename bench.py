@@ -464,7 +464,8 @@ def bench_batch(args, rank, world, local, torch):
                                    f"log-uniform in [1e3, 1e5] (total {sum(p.mesh.n_cells for p in probs)}"
                                    f" cells, {faces} faces), step states, HLLC, own CFL dt each",
                        "precision": "split", "launch": "one launch group, CUDA graph of K steps",
-                       "lanes_per_cell": lanes, "face_variant": face_variant,
+                       "lanes_per_cell": lanes, "grad_variant": grp.grad_variant,
+                       "face_variant": face_variant,
                        "l2": "working set > L2 (no flush)",
                        "parallelism": f"replicas x{world}", "mesh_build_s": round(t_build, 1)},
             "clocks": clk.summary(),
@@ -546,17 +547,23 @@ def max_rel_fields(a, b):
     return np.array([e[0], e[1:D + 1].max(), e[D + 1]])
 
 
-def run_served(pool, reqs, precision, chunk, keep_states=False, device=0, at_once=False):
+def run_served(pool, reqs, precision, chunk, keep_states=False, device=0, at_once=False,
+               tuning=None):
     """serve requests through the request server (C ABI, host states in and
     out): submitted at their arrival times from a feeder thread (at_once:
     all at time 0, a saturated server), completions collected concurrently;
     returns per-request results (with states when keep_states), launches and
-    server stats"""
+    server stats.  tuning: {(dim, solver): the tuners' choices} for the split
+    server's launch groups"""
     from shadowfax_b200 import _lib as L
     from shadowfax_b200.serve import Server
     srv = Server(precision=precision, memory_budget=SERVE_BUDGET, chunk_steps=chunk,
                  device=device)
     try:
+        if precision == L.PREC_SPLIT:
+            for (d, solver), t in (tuning or {}).items():
+                srv.set_tuning(d, solver, t["lanes_per_cell"], t["grad_variant"],
+                               t["face_variant"])
         ids = {j: srv.add_mesh(m) for j, m in enumerate(pool.meshes) if m is not None}
         # warm-up: a short request per class on the smallest meshes present
         warm = []
@@ -676,7 +683,7 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
     segments = [s for s in np.array_split(np.arange(len(reqs)), nseg) if len(s)]
     nbytes = lambda j: bases[reqs[j].mesh].clone_bytes(L.PREC_SPLIT)  # noqa: E731
     seg_ms, face_steps, launches, roof, nwaves = [], 0, 0, None, 0
-    fvar = {}
+    tuning = {}
     failed = set()
     first = True
     for seg in segments:
@@ -692,9 +699,9 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
                 inst[j] = (c, fp)
             if first:
                 roof = resident_roofline(pool, reqs, inst, classes, cctx)
-                # the face-kernel variant the tuner kept for each class
-                fvar = {c: roof["classes"][f"{c[0]}D {c[1]}"]["tuned"]["face_variant"]
-                        for c in classes if f"{c[0]}D {c[1]}" in roof["classes"]}
+                # what the tuners kept for each class
+                tuning = {c: roof["classes"][f"{c[0]}D {c[1]}"]["tuned"]
+                          for c in classes if f"{c[0]}D {c[1]}" in roof["classes"]}
                 for c in classes:
                     js = [j for j in wave if inst[j][0] == c]
                     if js and warmup:
@@ -726,7 +733,11 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
                                           [pool.dts[reqs[j].mesh][reqs[j].state]
                                            for j in live[c]])
                         groups[c].set_steps([left[j] for j in live[c]])
-                        groups[c].set_face_variant(fvar.get(c, 0))
+                        t = tuning.get(c)
+                        if t:
+                            groups[c].set_lanes(t["lanes_per_cell"])
+                            groups[c].set_grad_variant(t["grad_variant"])
+                            groups[c].set_face_variant(t["face_variant"])
                         reused[c] = 0
                 for c in classes:
                     if groups[c] is not None:
@@ -772,7 +783,8 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
     for c in pool_ctx.values():
         c.close()
     return {"face_steps": face_steps, "ms": float(sum(seg_ms)), "segment_ms": seg_ms,
-            "launches": launches, "roofline": roof, "waves": nwaves, "failed": len(failed)}
+            "launches": launches, "roofline": roof, "waves": nwaves, "failed": len(failed),
+            "tuning": tuning}
 
 
 # DRAM bytes (read + write) per active face of one launch of each split
@@ -822,7 +834,9 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
         # the timing tuners on this class's meshes (the states are read, not
         # changed): lanes per cell of the gradient/update kernels, the face
         # kernel's variant; the kernels are then timed as tuned
-        tuned = {"lanes_per_cell": int(g.tune(2)), "face_variant": int(g.tune_faces(2))}
+        lanes = int(g.tune(2))
+        tuned = {"lanes_per_cell": lanes, "grad_variant": int(g.grad_variant),
+                 "face_variant": int(g.tune_faces(2))}
         g.step_timed(1)
         steps = 3
         ms, nl = g.step_timed(steps)
@@ -943,7 +957,8 @@ def bench_serve(args, rank, world, local, torch):
         log(f"[bench] resident {res['face_steps'] / res['ms'] * 1e3:.3e} face-steps/s "
             f"({time.time() - t0:.0f} s)")
         t0 = time.time()
-        res32, launches, st32 = run_served(pool, reqs, L.PREC_SPLIT, args.chunk, False, local)
+        res32, launches, st32 = run_served(pool, reqs, L.PREC_SPLIT, args.chunk, False, local,
+                                           tuning=res["tuning"])
         clk.mark("t1")
         log(f"[bench] served ({time.time() - t0:.0f} s)")
         time.sleep(0.3)
@@ -957,7 +972,8 @@ def bench_serve(args, rank, world, local, torch):
     if sub:
         t0 = time.time()
         res64, _, st64 = run_served(pool, sub, L.PREC_FP64, args.chunk, True, local, at_once=True)
-        sub32, _, sts = run_served(pool, sub, L.PREC_SPLIT, args.chunk, True, local, at_once=True)
+        sub32, _, sts = run_served(pool, sub, L.PREC_SPLIT, args.chunk, True, local, at_once=True,
+                                   tuning=res["tuning"])
         log(f"[bench] fp64 sample {len(sub)} requests ({time.time() - t0:.0f} s)")
         fp64s, splits = served_summary(res64, st64), served_summary(sub32, sts)
         for j, (a, b) in enumerate(zip(sub32, res64)):
@@ -1311,7 +1327,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": problem_text(args, pr),
                        "solver": pr.solver, "precision": args.precision,
-                       "lanes_per_cell": lanes,
+                       "lanes_per_cell": lanes, "grad_variant": fp.grad_variant,
                        "l2": ("working set > L2 (no flush)" if flush is None else
                               "L2 flushed between steps (256 MB write outside the timed "
                               "events; step times summed)"),

@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -90,12 +91,21 @@ struct PoolMesh {
     std::vector<sfx_mesh*> cache[2]; /* idle instances per solver */
 };
 
+/* kernel settings of a class's launch group (sfx_server_set_tuning) */
+struct Tuning {
+    int32_t lanes = 0; /* 0: the library's default */
+    int32_t grad_variant = 0, face_variant = 0;
+};
+
 struct Class {
     sfx_ctx* ctx = nullptr;
     std::vector<Request*> members;
     sfx_group* group = nullptr;
     bool dirty = false;
     int reused = 0; /* rounds the current membership has run */
+    std::atomic<int> tune_gen{0}; /* bumped by sfx_server_set_tuning */
+    int applied_gen = 0;          /* worker thread: the tuning the group has */
+    Tuning tune;                  /* under sfx_server::mu */
 };
 
 }  // namespace
@@ -369,7 +379,25 @@ void join_arrivals(sfx_server* s) {
     s->up.used = 0;
 }
 
-int rebuild_group(Class& c) {
+int rebuild_group(sfx_server* s, Class& c);
+
+int apply_tuning(sfx_server* s, Class& c) {
+    const int gen = c.tune_gen.load();
+    if(!c.group || gen == c.applied_gen) return SFX_OK;
+    Tuning t;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        t = c.tune;
+    }
+    int rc = t.lanes ? sfx_group_set_lanes(c.group, t.lanes) : SFX_OK;
+    if(!rc) rc = sfx_group_set_grad_variant(c.group, t.grad_variant);
+    if(!rc) rc = sfx_group_set_face_variant(c.group, t.face_variant);
+    c.applied_gen = gen;
+    c.reused = 0; /* the captured graph holds the old kernels */
+    return rc;
+}
+
+int rebuild_group(sfx_server* s, Class& c) {
     c.dirty = false;
     c.reused = 0;
     std::vector<sfx_mesh*> ms;
@@ -381,9 +409,17 @@ int rebuild_group(Class& c) {
         steps.push_back(r->remaining);
     }
     const int32_t n = (int32_t)ms.size();
-    if(c.group) return sfx_group_set_members(c.group, n, ms.data(), dts.data(), steps.data());
+    if(c.group) {
+        const int rc = sfx_group_set_members(c.group, n, ms.data(), dts.data(), steps.data());
+        return rc ? rc : apply_tuning(s, c);
+    }
     int rc = sfx_group_create(c.ctx, n, ms.data(), dts.data(), &c.group);
     if(!rc) rc = sfx_group_set_steps(c.group, steps.data());
+    c.applied_gen = 0;
+    if(!rc && c.tune_gen.load() != 0) {
+        c.applied_gen = -1; /* a new group: apply whatever tuning there is */
+        rc = apply_tuning(s, c);
+    }
     return rc;
 }
 
@@ -399,7 +435,13 @@ void launch_split(sfx_server* s) {
         for(Class& c : row) {
             if(c.members.empty()) continue;
             if(c.dirty || !c.group) {
-                const int rc = rebuild_group(c);
+                const int rc = rebuild_group(s, c);
+                if(rc) {
+                    fail_class(s, c, rc);
+                    continue;
+                }
+            } else if(c.tune_gen.load() != c.applied_gen) {
+                const int rc = apply_tuning(s, c);
                 if(rc) {
                     fail_class(s, c, rc);
                     continue;
@@ -579,6 +621,26 @@ extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out)
     }
     s->worker = std::thread(worker_main, s);
     *out = s;
+    return SFX_OK;
+}
+
+extern "C" int sfx_server_set_tuning(sfx_server* s, int32_t dim, int32_t solver, int32_t lanes,
+                                     int32_t grad_variant, int32_t face_variant) {
+    if(!s || (dim != 2 && dim != 3) ||
+       (solver != SFX_SOLVER_EXACT && solver != SFX_SOLVER_HLLC) ||
+       (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) ||
+       grad_variant < 0 || grad_variant >= SFX_GRAD_VARIANTS || face_variant < 0 ||
+       face_variant >= SFX_FACE_VARIANTS)
+        return SFX_ERR_INVALID;
+    if(s->cfg.precision != SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    Class& c = s->cls[dim - 2][solver];
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        c.tune.lanes = lanes;
+        c.tune.grad_variant = grad_variant;
+        c.tune.face_variant = face_variant;
+    }
+    c.tune_gen.fetch_add(1); /* the worker applies it before the class's next round */
     return SFX_OK;
 }
 

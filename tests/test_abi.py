@@ -64,3 +64,16 @@ def test_server_rejects_bad_config():
         assert not h.value
     assert L.lib().sfx_server_poll(None, 1, None, None, None) == L.SFX_ERR_INVALID
     assert L.lib().sfx_server_shutdown(None) == L.SFX_ERR_INVALID
+
+
+def test_variant_counts_match_the_header():
+    """the Python constants that drive the tuners match include/sfxflux.h"""
+    from shadowfax_b200 import _lib as L
+    h = (ROOT / "include" / "sfxflux.h").read_text()
+    assert int(re.search(r"#define SFX_FACE_VARIANTS (\d+)", h).group(1)) == L.FACE_VARIANTS
+    assert int(re.search(r"#define SFX_GRAD_VARIANTS (\d+)", h).group(1)) == L.GRAD_VARIANTS
+
+
+def test_server_tuning_rejects_bad_arguments_without_a_server():
+    from shadowfax_b200 import _lib as L
+    assert L.lib().sfx_server_set_tuning(None, 2, 0, 0, 0, 0) == L.SFX_ERR_INVALID

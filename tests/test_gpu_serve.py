@@ -30,10 +30,12 @@ def _alone(pr, precision):
     return fp.state()
 
 
-def _serve(probs, precision, chunk_steps=4, **kw):
+def _serve(probs, precision, chunk_steps=4, tuning=None, **kw):
     from shadowfax_b200.serve import Server
     srv = Server(precision=precision, chunk_steps=chunk_steps, **kw)
     try:
+        for (d, solver), t in (tuning or {}).items():
+            srv.set_tuning(d, solver, *t)
         ids = [srv.add_mesh(pr.mesh) for pr in probs]
         rids = [srv.submit(i, pr.W0, pr.solver, pr.dt, pr.nsteps) for i, pr in zip(ids, probs)]
         assert srv.drain(120.0)
@@ -56,6 +58,28 @@ def test_requests_in_a_mix_equal_requests_alone(cuda_ok, precision):
         np.testing.assert_array_equal(r.W, W)
         assert r.face_steps == pr.nsteps * pr.mesh.n_active_faces
         assert r.t_submit <= r.t_admit <= r.t_done
+
+
+def test_tuned_server(cuda_ok):
+    """kernel settings per class: the pipelined gradient kernel and the
+    80-register face kernels change the schedule only (bitwise the same
+    results as alone); the gamma = 5/3 exact forms stay within the split
+    pass's round-off; an FP64 server refuses tuning"""
+    from shadowfax_b200._lib import SfxError
+    probs = _problems()
+    classes = [(d, s) for d in (2, 3) for s in ("Exact", "HLLC")]
+    res, st = _serve(probs, 1, tuning={c: (0, 1, 1) for c in classes})
+    assert st.completed == len(probs) and st.failed == 0
+    for pr, r in zip(probs, res):
+        np.testing.assert_array_equal(r.Q, _alone(pr, 1)[1])
+    res, _ = _serve(probs, 1, tuning={c: (2, 1, 3) for c in classes})
+    for pr, r in zip(probs, res):
+        assert r.status == 0
+        Q = _alone(pr, 1)[1]
+        err = np.abs(r.Q - Q).sum(0) / np.abs(Q).sum(0)
+        assert np.all(err[[0, -1]] <= 1e-6), err
+    with pytest.raises(SfxError):
+        _serve(probs[:1], 0, tuning={(2, "HLLC"): (0, 0, 0)})
 
 
 def test_one_request_alone_and_in_mix(cuda_ok):
