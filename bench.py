@@ -464,8 +464,7 @@ def bench_batch(args, rank, world, local, torch):
                                    f"log-uniform in [1e3, 1e5] (total {sum(p.mesh.n_cells for p in probs)}"
                                    f" cells, {faces} faces), step states, HLLC, own CFL dt each",
                        "precision": "split", "launch": "one launch group, CUDA graph of K steps",
-                       "lanes_per_cell": lanes, "grad_variant": grp.grad_variant,
-                       "face_variant": face_variant,
+                       "lanes_per_cell": lanes, "face_variant": face_variant,
                        "l2": "working set > L2 (no flush)",
                        "parallelism": f"replicas x{world}", "mesh_build_s": round(t_build, 1)},
             "clocks": clk.summary(),
@@ -562,8 +561,7 @@ def run_served(pool, reqs, precision, chunk, keep_states=False, device=0, at_onc
     try:
         if precision == L.PREC_SPLIT:
             for (d, solver), t in (tuning or {}).items():
-                srv.set_tuning(d, solver, t["lanes_per_cell"], t["grad_variant"],
-                               t["face_variant"])
+                srv.set_tuning(d, solver, t["lanes_per_cell"], t["face_variant"])
         ids = {j: srv.add_mesh(m) for j, m in enumerate(pool.meshes) if m is not None}
         # warm-up: a short request per class on the smallest meshes present
         warm = []
@@ -736,7 +734,6 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
                         t = tuning.get(c)
                         if t:
                             groups[c].set_lanes(t["lanes_per_cell"])
-                            groups[c].set_grad_variant(t["grad_variant"])
                             groups[c].set_face_variant(t["face_variant"])
                         reused[c] = 0
                 for c in classes:
@@ -834,9 +831,7 @@ def resident_roofline(pool, reqs, inst, classes, cctx):
         # the timing tuners on this class's meshes (the states are read, not
         # changed): lanes per cell of the gradient/update kernels, the face
         # kernel's variant; the kernels are then timed as tuned
-        lanes = int(g.tune(2))
-        tuned = {"lanes_per_cell": lanes, "grad_variant": int(g.grad_variant),
-                 "face_variant": int(g.tune_faces(2))}
+        tuned = {"lanes_per_cell": int(g.tune(2)), "face_variant": int(g.tune_faces(2))}
         g.step_timed(1)
         steps = 3
         ms, nl = g.step_timed(steps)
@@ -1327,7 +1322,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": problem_text(args, pr),
                        "solver": pr.solver, "precision": args.precision,
-                       "lanes_per_cell": lanes, "grad_variant": fp.grad_variant,
+                       "lanes_per_cell": lanes,
                        "l2": ("working set > L2 (no flush)" if flush is None else
                               "L2 flushed between steps (256 MB write outside the timed "
                               "events; step times summed)"),

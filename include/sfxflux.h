@@ -287,13 +287,6 @@ int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
  * pass's tolerance. */
 #define SFX_FACE_VARIANTS 4
 int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
-/* split pass: gradient-kernel variant: 0 (one neighbour's gathers in flight
- * per lane, 64 registers; the default), 1 (two-stage pipeline: the next
- * face's geometry and neighbour gathered while this face is summed, 80
- * registers).  The same arithmetic in the same order: bitwise the same
- * results. */
-#define SFX_GRAD_VARIANTS 2
-int sfx_mesh_set_grad_variant(sfx_mesh* mesh, int32_t variant);
 
 /* ---- one mesh over several devices (plain FP64) ----
  * Replaces the reference's MPI halo updates for the flux pass
@@ -339,10 +332,6 @@ int sfx_group_step(sfx_group* group, int32_t nsteps, int32_t use_graph,
  * this group (reads the states, changes none) and keep the fastest for the
  * gradient and update kernels; *lanes receives it */
 int sfx_group_tune(sfx_group* group, int32_t reps, int32_t* lanes);
-/* the gradient variant (SFX_GRAD_VARIANTS): sfx_group_tune times every
- * lanes setting with each and keeps the fastest pair */
-int sfx_group_set_grad_variant(sfx_group* group, int32_t variant);
-int sfx_group_get_grad_variant(sfx_group* group, int32_t* variant);
 int sfx_group_set_lanes(sfx_group* group, int32_t lanes);
 /* time each face-kernel variant (SFX_FACE_VARIANTS) on this group, every
  * timed face launch after a gradient launch (the states are read, none
@@ -449,11 +438,12 @@ typedef struct sfx_server_stats {
 
 int sfx_server_create(const sfx_server_config* cfg, sfx_server** out);
 /* split servers: the kernel settings of the launch group of one (dim, solver)
- * class (lanes 0: the default; SFX_GRAD_VARIANTS, SFX_FACE_VARIANTS), e.g.
- * what sfx_group_tune / sfx_group_tune_faces kept on meshes like the pool's;
- * applied before the class's next round.  SFX_ERR_UNSUPPORTED for FP64. */
+ * class (lanes per cell, 0: the default; face variant, SFX_FACE_VARIANTS),
+ * e.g. what sfx_group_tune / sfx_group_tune_faces kept on meshes like the
+ * pool's; applied before the class's next round.  SFX_ERR_UNSUPPORTED for
+ * FP64. */
 int sfx_server_set_tuning(sfx_server* srv, int32_t dim, int32_t solver, int32_t lanes,
-                          int32_t grad_variant, int32_t face_variant);
+                          int32_t face_variant);
 /* add a mesh to the device pool (upload once); *mesh_id identifies it */
 int sfx_server_add_mesh(sfx_server* srv, const sfx_mesh_desc* desc, int32_t* mesh_id);
 /* queue a request; W0 [n_cells][S] is copied; returns at once */

@@ -29,7 +29,7 @@ SFX_ERR_TOO_LARGE, SFX_ERR_IO, SFX_ERR_TIMESTEP = 13, 14, 15
 
 SOLVER_EXACT, SOLVER_HLLC = 0, 1
 PREC_FP64, PREC_SPLIT = 0, 1
-FACE_VARIANTS, GRAD_VARIANTS = 4, 2  # SFX_FACE_VARIANTS, SFX_GRAD_VARIANTS
+FACE_VARIANTS = 4  # SFX_FACE_VARIANTS
 FACE_REAL, FACE_PERIODIC, FACE_MIRROR = 0, 1, 2
 
 
@@ -137,7 +137,6 @@ PROTOTYPES = {
                                     _ip, _ip, _dp, _dp]),
     "sfx_mesh_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_mesh_set_face_variant": (C.c_int, [C.c_void_p, C.c_int32]),
-    "sfx_mesh_set_grad_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_step_moving": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, _dp, C.c_void_p]),
     "sfx_mesh_set_timesteps": (C.c_int, [C.c_void_p, _u64p, _u64p]),
     "sfx_mesh_get_timesteps": (C.c_int, [C.c_void_p, _u64p, _u64p]),
@@ -161,7 +160,7 @@ PROTOTYPES = {
                                        C.POINTER(C.c_int32)]),
     "sfx_server_create": (C.c_int, [C.POINTER(sfx_server_config), C.POINTER(C.c_void_p)]),
     "sfx_server_add_mesh": (C.c_int, [C.c_void_p, C.POINTER(sfx_mesh_desc), _ip]),
-    "sfx_server_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+    "sfx_server_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                         C.c_int32]),
     "sfx_server_submit": (C.c_int, [C.c_void_p, C.c_int32, _dp, C.c_int32, C.c_double,
                                     C.c_int32, C.POINTER(C.c_int64)]),
@@ -178,8 +177,6 @@ PROTOTYPES = {
     "sfx_group_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
     "sfx_group_tune_faces": (C.c_int, [C.c_void_p, C.c_int32, _ip]),
     "sfx_group_set_face_variant": (C.c_int, [C.c_void_p, C.c_int32]),
-    "sfx_group_set_grad_variant": (C.c_int, [C.c_void_p, C.c_int32]),
-    "sfx_group_get_grad_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "sfx_group_free": (C.c_int, [C.c_void_p]),
     "sfx_flux_pass_noalloc": (C.c_int, [C.POINTER(sfx_device_mesh), C.POINTER(sfx_config),
                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -142,7 +142,6 @@ int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t 
         g.dim = m->d.dim;
         g.lanes = m->d.lanes;
         g.face_variant = m->d.face_variant;
-        g.grad_variant = m->d.grad_variant;
         g.moving = m->d.vel != nullptr ? 1 : 0; /* split meshes get face velocities
                                                    only from sfx_step_moving */
         sfx_split_blocks(m->d.dim, m->d.lanes, m->d.n_cells, m->d.n_faces, g.blocks);
@@ -997,12 +996,6 @@ int sfx_mesh_set_lanes(sfx_mesh* m, int32_t lanes) {
 int sfx_mesh_set_face_variant(sfx_mesh* m, int32_t variant) {
     if(!m || variant < 0 || variant >= SFX_FACE_VARIANTS) return SFX_ERR_INVALID;
     m->d.face_variant = variant;
-    return SFX_OK;
-}
-
-int sfx_mesh_set_grad_variant(sfx_mesh* m, int32_t variant) {
-    if(!m || variant < 0 || variant >= SFX_GRAD_VARIANTS) return SFX_ERR_INVALID;
-    m->d.grad_variant = variant;
     return SFX_OK;
 }
 

@@ -162,19 +162,6 @@ extern "C" int sfx_group_set_face_variant(sfx_group* g, int32_t variant) {
     return SFX_OK;
 }
 
-extern "C" int sfx_group_set_grad_variant(sfx_group* g, int32_t variant) {
-    if(!g || variant < 0 || variant >= SFX_GRAD_VARIANTS) return SFX_ERR_INVALID;
-    g->dev.grad_variant = variant;
-    drop_graph(g);
-    return SFX_OK;
-}
-
-extern "C" int sfx_group_get_grad_variant(sfx_group* g, int32_t* variant) {
-    if(!g || !variant) return SFX_ERR_INVALID;
-    *variant = g->dev.grad_variant;
-    return SFX_OK;
-}
-
 extern "C" int sfx_group_set_lanes(sfx_group* g, int32_t lanes) {
     if(!g || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16))
         return SFX_ERR_INVALID;
@@ -316,13 +303,11 @@ extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
         return SFX_ERR_CUDA;
     }
     const int cand[5] = {1, 2, 4, 8, 16};
-    int best = g->dev.lanes, best_v = g->dev.grad_variant;
+    int best = g->dev.lanes;
     float best_ms = 1e30f;
     int rc = SFX_OK;
-    /* every lanes-per-cell setting with every gradient variant */
-    for(int c = 0; c < 5 * SFX_GRAD_VARIANTS && !rc; ++c) {
-        rc = sfx_group_set_lanes(g, cand[c % 5]);
-        if(!rc) rc = sfx_group_set_grad_variant(g, c / 5);
+    for(int c = 0; c < 5 && !rc; ++c) {
+        rc = sfx_group_set_lanes(g, cand[c]);
         if(rc) break;
         /* timed on the gradient kernel, which only reads the states (the
          * update kernel shares the setting); one untimed launch, then reps */
@@ -336,14 +321,12 @@ extern "C" int sfx_group_tune(sfx_group* g, int32_t reps, int32_t* lanes_out) {
         if(!rc) rc = cuda_ok(cudaEventElapsedTime(&ms, e0, e1));
         if(!rc && ms < best_ms) {
             best_ms = ms;
-            best = cand[c % 5];
-            best_v = c / 5;
+            best = cand[c];
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int r2 = sfx_group_set_lanes(g, best);
-    if(!r2) r2 = sfx_group_set_grad_variant(g, best_v);
     if(lanes_out) *lanes_out = best;
     return rc ? rc : r2;
 }

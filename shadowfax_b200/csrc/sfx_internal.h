@@ -30,7 +30,6 @@ struct sfx_dmesh {
     int32_t has_velocity;
     int32_t lanes; /* split pass: lanes per cell of the gradient/update kernels */
     int32_t face_variant; /* split pass: register cap of the face kernel (sfx_split.cu) */
-    int32_t grad_variant; /* split pass: 1 = two-stage gather pipeline in the gradient kernel */
     /* cells */
     double* pos;    /* [dim][n]  */
     double* cen;    /* [dim][n]  */
@@ -161,7 +160,6 @@ struct sfx_group_dev {
     int32_t dim;
     int32_t lanes; /* lanes per cell of the gradient and update kernels */
     int32_t face_variant; /* SFX_FACE_VARIANTS (include/sfxflux.h) */
-    int32_t grad_variant; /* SFX_GRAD_VARIANTS (include/sfxflux.h) */
     int32_t moving;       /* a moving mesh stepped alone: face kernels with the boost */
     int32_t blocks[3];
 };

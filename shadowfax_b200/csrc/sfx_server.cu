@@ -94,7 +94,7 @@ struct PoolMesh {
 /* kernel settings of a class's launch group (sfx_server_set_tuning) */
 struct Tuning {
     int32_t lanes = 0; /* 0: the library's default */
-    int32_t grad_variant = 0, face_variant = 0;
+    int32_t face_variant = 0;
 };
 
 struct Class {
@@ -390,7 +390,6 @@ int apply_tuning(sfx_server* s, Class& c) {
         t = c.tune;
     }
     int rc = t.lanes ? sfx_group_set_lanes(c.group, t.lanes) : SFX_OK;
-    if(!rc) rc = sfx_group_set_grad_variant(c.group, t.grad_variant);
     if(!rc) rc = sfx_group_set_face_variant(c.group, t.face_variant);
     c.applied_gen = gen;
     c.reused = 0; /* the captured graph holds the old kernels */
@@ -625,19 +624,17 @@ extern "C" int sfx_server_create(const sfx_server_config* cfg, sfx_server** out)
 }
 
 extern "C" int sfx_server_set_tuning(sfx_server* s, int32_t dim, int32_t solver, int32_t lanes,
-                                     int32_t grad_variant, int32_t face_variant) {
+                                     int32_t face_variant) {
     if(!s || (dim != 2 && dim != 3) ||
        (solver != SFX_SOLVER_EXACT && solver != SFX_SOLVER_HLLC) ||
        (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) ||
-       grad_variant < 0 || grad_variant >= SFX_GRAD_VARIANTS || face_variant < 0 ||
-       face_variant >= SFX_FACE_VARIANTS)
+       face_variant < 0 || face_variant >= SFX_FACE_VARIANTS)
         return SFX_ERR_INVALID;
     if(s->cfg.precision != SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
     Class& c = s->cls[dim - 2][solver];
     {
         std::lock_guard<std::mutex> lk(s->mu);
         c.tune.lanes = lanes;
-        c.tune.grad_variant = grad_variant;
         c.tune.face_variant = face_variant;
     }
     c.tune_gen.fetch_add(1); /* the worker applies it before the class's next round */

@@ -310,7 +310,7 @@ __device__ __forceinline__ double seg_sum(double v) {
     return v;
 }
 
-template <int D, int LPC, bool PIPE = false>
+template <int D, int LPC>
 __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma, const int t) {
     constexpr int S = D + 2, G = GradVec4<D>::value;
     const int i = t / LPC, lane = t % LPC;
@@ -337,14 +337,30 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
      * a face of zero area), the rest are loaded again */
     __shared__ float sd[kGradSlots * D][256];
     int k0 = 0;
-    /* one face of the cell: its contribution to the gradient sums and the
-     * neighbour extremes (geometry and neighbour state already gathered) */
-    auto accumulate = [&](unsigned e, int nb, float A, float* c, float* r, float rn,
-                          const float* Wn) {
+    /* software pipelined: the next entry's face id and neighbour are loaded
+     * before this entry's gathers, and both gathers (face geometry, the
+     * neighbour's record) are issued before either is used */
+    unsigned e_next = 0u;
+    int nb_next = -1;
+    if(beg + lane < end) {
+        e_next = (unsigned)__ldg(m.idx + beg + lane);
+        nb_next = __ldg(m.nbe + beg + lane);
+    }
+    for(int j = beg + lane; j < end; j += LPC, ++k0) {
+        const unsigned e = e_next;
+        const int nb = nb_next;
+        if(j + LPC < end) {
+            e_next = (unsigned)__ldg(m.idx + j + LPC);
+            nb_next = __ldg(m.nbe + j + LPC);
+        }
+        const int f = (int)(e & ~kRightBit);
         const bool right = e & kRightBit;
+        float A, c[D], r[D], rn;
+        geom<D>(m.fg, f, A, c, r, rn);
+        const Cell<D> cn = load_cell<D>(m.cw, nb < 0 ? ic : nb);
         if(A == 0.f) {
             if(k0 < kGradSlots) sd[k0 * D][threadIdx.x] = __int_as_float(0x7fc00000);
-            return;
+            continue;
         }
         if(right) {
 #pragma unroll
@@ -369,7 +385,7 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
             for(int l = 0; l < D; ++l) Wj[1 + l] = W[1 + l] - vn * r[l];
         } else {
 #pragma unroll
-            for(int k = 0; k < S; ++k) Wj[k] = Wn[k];
+            for(int k = 0; k < S; ++k) Wj[k] = cn.W[k];
         }
         const float s = A / rn;
 #pragma unroll
@@ -380,106 +396,6 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
             for(int l = 0; l < D; ++l) delta[l][k] += s * (dW * c[l] - sW * r[l]);
             Wmax[k] = fmaxf(Wmax[k], Wj[k]);
             Wmin[k] = fminf(Wmin[k], Wj[k]);
-        }
-    };
-    if constexpr(!PIPE) {
-        /* software pipelined: the next entry's face id and neighbour are
-         * loaded before this entry's gathers, and both gathers (face
-         * geometry, the neighbour's record) are issued before either is used */
-        unsigned e_next = 0u;
-        int nb_next = -1;
-        if(beg + lane < end) {
-            e_next = (unsigned)__ldg(m.idx + beg + lane);
-            nb_next = __ldg(m.nbe + beg + lane);
-        }
-        for(int j = beg + lane; j < end; j += LPC, ++k0) {
-            const unsigned e = e_next;
-            const int nb = nb_next;
-            if(j + LPC < end) {
-                e_next = (unsigned)__ldg(m.idx + j + LPC);
-                nb_next = __ldg(m.nbe + j + LPC);
-            }
-            float A, c[D], r[D], rn;
-            geom<D>(m.fg, (int)(e & ~kRightBit), A, c, r, rn);
-            const Cell<D> cn = load_cell<D>(m.cw, nb < 0 ? ic : nb);
-            accumulate(e, nb, A, c, r, rn, cn.W);
-        }
-    } else {
-        /* two stages: entry j's gathers are in flight while entry j - LPC is
-         * summed, and entry j + LPC's ids while those gathers wait; the raw
-         * records of the entry in flight stay in registers (the neighbour's
-         * W only: 13 floats in 3D, 12 in 2D) */
-        int j = beg + lane;
-        unsigned e1 = 0u, e2 = 0u;
-        int nb1 = -1, nb2 = -1;
-        float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0, w0 = g0;
-        float w4 = 0.f;
-        if(j < end) {
-            e1 = (unsigned)__ldg(m.idx + j);
-            nb1 = __ldg(m.nbe + j);
-        }
-        if(j + LPC < end) {
-            e2 = (unsigned)__ldg(m.idx + j + LPC);
-            nb2 = __ldg(m.nbe + j + LPC);
-        }
-        if(j < end) {
-            const int f = (int)(e1 & ~kRightBit);
-            const int cc = nb1 < 0 ? ic : nb1;
-            g0 = __ldg(m.fg + 2 * (size_t)f);
-            g1 = __ldg(m.fg + 2 * (size_t)f + 1);
-            w0 = __ldg(m.cw + 2 * cc);
-            if(D == 3) w4 = __ldg(reinterpret_cast<const float*>(m.cw + 2 * cc + 1));
-        }
-        for(; j < end; j += LPC, ++k0) {
-            /* issue the next entry's gathers and the ids after it */
-            float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = h0, v0 = h0;
-            float v4 = 0.f;
-            if(j + LPC < end) {
-                const int f = (int)(e2 & ~kRightBit);
-                const int cc = nb2 < 0 ? ic : nb2;
-                h0 = __ldg(m.fg + 2 * (size_t)f);
-                h1 = __ldg(m.fg + 2 * (size_t)f + 1);
-                v0 = __ldg(m.cw + 2 * cc);
-                if(D == 3) v4 = __ldg(reinterpret_cast<const float*>(m.cw + 2 * cc + 1));
-            }
-            unsigned e3 = 0u;
-            int nb3 = -1;
-            if(j + 2 * LPC < end) {
-                e3 = (unsigned)__ldg(m.idx + j + 2 * LPC);
-                nb3 = __ldg(m.nbe + j + 2 * LPC);
-            }
-            /* this entry, from the registers (geom's and load_cell's field
-             * order) */
-            float A, c[D], r[D], rn;
-            A = g0.x;
-            c[0] = g0.y;
-            c[1] = g0.z;
-            if(D == 3) {
-                c[D - 1] = g0.w;
-                r[0] = g1.x;
-                r[1] = g1.y;
-                r[D - 1] = g1.z;
-                rn = g1.w;
-            } else {
-                r[0] = g0.w;
-                r[1] = g1.x;
-                rn = g1.y;
-            }
-            float Wn[S];
-            Wn[0] = w0.x;
-            Wn[1] = w0.y;
-            Wn[2] = w0.z;
-            Wn[3] = w0.w;
-            if(D == 3) Wn[S - 1] = w4;
-            accumulate(e1, nb1, A, c, r, rn, Wn);
-            e1 = e2;
-            nb1 = nb2;
-            e2 = e3;
-            nb2 = nb3;
-            g0 = h0;
-            g1 = h1;
-            w0 = v0;
-            w4 = v4;
         }
     }
     const float iv = 1.f / xv.w;
@@ -1588,23 +1504,37 @@ __device__ __forceinline__ int wave_class(const sfx_solver_params& s, const Face
 /* G53: gamma = 5/3, where the sampling's powers are integers in z_K or in
  * the fan's base: (p/p_K)^(1/g) = z_K^3, base^(2/(g-1)) = base^3,
  * base^(2g/(g-1)) = base^5 */
-template <int D, bool G53 = false>
-__device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const FaceWork<D>& w,
-                                          bool moving, SFlux<D>& F) {
-    /* a reflective right state is the left state with the normal velocity
-     * reversed: only its normal velocity enters, and of its flux only the
-     * pressure survives (face_dq) */
-    float WRf[D + 2];
-#pragma unroll
-    for(int k = 0; k < D + 2; ++k) WRf[k] = w.mirror ? w.WL[k] : w.WR[k];
+/* phase 3 reads its face from the block's class-ordered lists in shared
+ * memory where each value is used, not all at once into registers: the
+ * FP64 solve then fits 64 registers with fewer spills */
+template <int D, bool MOVING>
+struct SortedFace {
+    const float (*W)[kExactBlock]; /* [2 S][block]: left states, then right ones */
+    const float (*n)[kExactBlock]; /* [D][block] */
+    const float (*v)[kExactBlock]; /* [D][block] (MOVING) */
+    int t;
+    bool mirror;
+    __device__ float WL(int k) const { return W[k][t]; }
+    /* a reflective right state is the left state (its normal velocity
+     * reversed by the caller) */
+    __device__ float WR(int k) const { return W[mirror ? k : D + 2 + k][t]; }
+    __device__ float N(int l) const { return n[l][t]; }
+    __device__ float V(int l) const { return MOVING ? v[l][t] : 0.f; }
+};
+
+template <int D, bool G53 = false, bool MOVING = false>
+__device__ __forceinline__ int exact_fast(const sfx_solver_params& s,
+                                          const SortedFace<D, MOVING>& w, SFlux<D>& F) {
+    /* of a reflective face's flux only the pressure survives (face_dq) */
+    constexpr bool moving = MOVING;
     double vL = 0., vR = 0.;
 #pragma unroll
     for(int l = 0; l < D; ++l) {
-        vL += (double)w.WL[1 + l] * (double)w.n[l];
-        vR += (double)WRf[1 + l] * (double)w.n[l];
+        vL += (double)w.WL(1 + l) * (double)w.N(l);
+        vR += (double)w.WR(1 + l) * (double)w.N(l);
     }
     if(w.mirror) vR = -vL;
-    const double rL = w.WL[0], pL = w.WL[D + 1], rR = WRf[0], pR = WRf[D + 1];
+    const double rL = w.WL(0), pL = w.WL(D + 1), rR = w.WR(0), pR = w.WR(D + 1);
     const double g = s.gamma;
     const double aL = sqrt(g * pL / rL);
     const double aR = sqrt(g * pR / rR);
@@ -1666,11 +1596,12 @@ __device__ __forceinline__ int exact_fast(const sfx_solver_params& s, const Face
     bool bad = !(srho >= 0.) || !(spr >= 0.);
 #pragma unroll
     for(int l = 0; l < D; ++l) {
-        hv[l] = (double)(right ? WRf[1 + l] : w.WL[1 + l]) + vhalf * (double)w.n[l];
+        const double nl = (double)w.N(l);
+        hv[l] = (double)(right ? w.WR(1 + l) : w.WL(1 + l)) + vhalf * nl;
         bad |= hv[l] != hv[l];
-        un += hv[l] * (double)w.n[l];
-        hv[l] += (double)w.v[l];
-        vn += (double)w.v[l] * (double)w.n[l];
+        un += hv[l] * nl;
+        hv[l] += (double)w.V(l);
+        vn += (double)w.V(l) * nl;
         v2 += hv[l] * hv[l];
     }
     F.m = 0.f;
@@ -1823,7 +1754,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
      * (bit 31: mirror) */
     __shared__ float sW[2 * S][kExactBlock];
     __shared__ float sn[D][kExactBlock];
-    __shared__ float sv[MOVING ? D : 1][MOVING ? kExactBlock : 1];
+    __shared__ float sv[MOVING ? D : 1][kExactBlock]; /* one unused row when static */
     __shared__ float sA[kExactBlock], sLL[kExactBlock], sLR[kExactBlock];
     __shared__ int sf[kExactBlock];
     __shared__ int sbase[kNClass][NW];
@@ -1876,7 +1807,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
 #pragma unroll
         for(int l = 0; l < D; ++l) {
             sn[l][slot] = w.n[l];
-            if(MOVING) sv[MOVING ? l : 0][MOVING ? slot : 0] = w.v[l];
+            if(MOVING) sv[MOVING ? l : 0][slot] = w.v[l];
         }
         sA[slot] = w.A;
         sLL[slot] = w.limL;
@@ -1889,43 +1820,33 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     bool push = false;
     int fq = 0;
     if(t < stotal) {
-        FaceWork<D> v;
-#pragma unroll
-        for(int k = 0; k < S; ++k) {
-            v.WL[k] = sW[k][t];
-            v.WR[k] = sW[S + k][t];
-        }
-#pragma unroll
-        for(int l = 0; l < D; ++l) {
-            v.n[l] = sn[l][t];
-            v.v[l] = MOVING ? sv[MOVING ? l : 0][MOVING ? t : 0] : 0.f;
-        }
-        v.A = sA[t];
-        v.limL = sLL[t];
-        v.limR = sLR[t];
         const int e = sf[t];
-        v.mirror = e < 0;
         fq = e & 0x7fffffff;
+        const SortedFace<D, MOVING> face{sW, sn, sv, t, e < 0};
         SFlux<D> F;
-        const int st = exact_fast<D, G53>(sp, v, MOVING, F);
-        if(st == kDefer)
+        const int st = exact_fast<D, G53, MOVING>(sp, face, F);
+        if(st == kDefer) {
             push = true;
-        else
+        } else {
+            /* what face_dq reads of the face */
+            FaceWork<D> v;
+            v.A = sA[t];
+            v.limL = sLL[t];
+            v.limR = sLR[t];
+            v.mirror = e < 0;
             face_dq<D>(m, dt, fq, v, F, st);
+        }
     }
     queue_faces(m, push, fq);
 }
 
-/* PIPE: the two-stage gather pipeline, with 80 registers (three blocks per
- * SM) for the records in flight */
-template <int D, int LPC, bool PIPE = false>
-__global__ void __launch_bounds__(256, PIPE ? 3 : 4) k_group_sgrad(const sfx_group_entry* tab,
-                                                                  const int* pre, int nm,
-                                                                  float gamma) {
+template <int D, int LPC>
+__global__ void __launch_bounds__(256, 4) k_group_sgrad(const sfx_group_entry* tab, const int* pre,
+                                                     int nm, float gamma) {
     const int mi = group_mesh_of_block(pre, nm);
     if(member_done(tab, mi)) return;
-    sgrad_body<D, LPC, PIPE>(tab[mi].m, gamma,
-                             (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
+    sgrad_body<D, LPC>(tab[mi].m, gamma,
+                       (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x);
 }
 
 template <int D, int SOLVER, int MINB, bool STORED_DW = SOLVER != SFX_SOLVER_HLLC,
@@ -2051,14 +1972,8 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
     const int nm = g->n_meshes;
     if(phase == 0) {
         if(g->blocks[0])
-        {
-            if(g->grad_variant == 1)
-                k_group_sgrad<D, LPC, true><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm,
-                                                                       (float)sp->gamma);
-            else
-                k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm,
-                                                                    (float)sp->gamma);
-        }
+            k_group_sgrad<D, LPC><<<g->blocks[0], 256, 0, s>>>(g->tab, g->pre, nm,
+                                                                (float)sp->gamma);
     } else if(phase == 1) {
         if(g->blocks[1]) {
             const int* pre1 = g->pre + (nm + 1);

@@ -147,7 +147,6 @@ class FluxPass:
         L.check(L.lib().sfx_mesh_upload(ctx.h, C.byref(d), C.byref(h)), "sfx_mesh_upload")
         self.h = h
         self.S = mesh.dim + 2
-        self.grad_variant = 0
 
     def clone(self, ctx: Context | None = None) -> "FluxPass":
         """a new state on this mesh's device geometry (sfx_mesh_clone): the
@@ -305,31 +304,19 @@ class FluxPass:
                 "sfx_mesh_unpack_cells")
 
     def tune(self, dt: float, reps: int = 3) -> int:
-        """split pass: time the lanes-per-cell settings, each with both
-        gradient variants, on this mesh's own gradient+update kernels and keep
-        the fastest pair (advances the state by 10 * (reps + 1) steps: call
-        before loading the initial state); returns the lanes, the variant is
-        in ``grad_variant``"""
-        best, best_ms = (4, 0), 1e30
-        for v in range(L.GRAD_VARIANTS):
-            self.set_grad_variant(v)
-            for lanes in (1, 2, 4, 8, 16):
-                self.set_lanes(lanes)
-                self.step_timed(dt, 1)
-                ms, _ = self.step_timed(dt, reps)
-                t = ms[0] + ms[2]
-                if t < best_ms:
-                    best, best_ms = (lanes, v), t
-        self.set_lanes(best[0])
-        self.set_grad_variant(best[1])
-        return best[0]
-
-    def set_grad_variant(self, variant: int):
-        """split pass: gradient-kernel variant (0: one face's gathers in
-        flight; 1: two-stage pipeline, 80 registers)"""
-        L.check(L.lib().sfx_mesh_set_grad_variant(self.h, variant),
-                "sfx_mesh_set_grad_variant")
-        self.grad_variant = variant
+        """split pass: time the lanes-per-cell variants on this mesh's own
+        gradient+update kernels and keep the fastest (advances the state by
+        5 * (reps + 1) steps: call before loading the initial state)"""
+        best, best_ms = 4, 1e30
+        for lanes in (1, 2, 4, 8, 16):
+            self.set_lanes(lanes)
+            self.step_timed(dt, 1)
+            ms, _ = self.step_timed(dt, reps)
+            t = ms[0] + ms[2]
+            if t < best_ms:
+                best, best_ms = lanes, t
+        self.set_lanes(best)
+        return best
 
     def step_timed(self, dt: float, nsteps: int) -> tuple[np.ndarray, int]:
         """nsteps with per-kernel device times: (ms[gradients, faces, update],
@@ -393,18 +380,6 @@ class Group:
 
     def set_lanes(self, lanes: int):
         L.check(L.lib().sfx_group_set_lanes(self.h, lanes), "sfx_group_set_lanes")
-
-    def set_grad_variant(self, variant: int):
-        L.check(L.lib().sfx_group_set_grad_variant(self.h, variant),
-                "sfx_group_set_grad_variant")
-
-    @property
-    def grad_variant(self) -> int:
-        """the gradient-kernel variant in use (tune() picks it with the lanes)"""
-        v = C.c_int32(0)
-        L.check(L.lib().sfx_group_get_grad_variant(self.h, C.byref(v)),
-                "sfx_group_get_grad_variant")
-        return v.value
 
     def tune_faces(self, reps: int = 3) -> int:
         """time the face-kernel variants on this group's meshes (a gradient

@@ -55,12 +55,10 @@ class Server:
         self.meshes: list[Mesh] = []
         self._mesh_of: dict[int, int] = {}
 
-    def set_tuning(self, dim: int, solver, lanes: int = 0, grad_variant: int = 0,
-                   face_variant: int = 0) -> None:
+    def set_tuning(self, dim: int, solver, lanes: int = 0, face_variant: int = 0) -> None:
         """split servers: kernel settings of one (dim, solver) class's launch
         group (lanes 0: the default), applied before its next round"""
         L.check(L.lib().sfx_server_set_tuning(self.h, dim, SOLVER_CODES[solver], lanes,
-                                              grad_variant,
                                               face_variant), "sfx_server_set_tuning")
 
     def add_mesh(self, mesh: Mesh) -> int:

@@ -78,7 +78,6 @@ def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
     g = Group(ctx, members, [pr.dt for pr in probs])
     lanes = g.tune(2)
     assert lanes in (1, 2, 4, 8, 16)
-    assert g.grad_variant in (0, 1)
     st = g.step(probs[0].nsteps)
     assert np.all(st == 0)
     for pr, fp in zip(probs, members):
@@ -86,42 +85,6 @@ def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
         Qa = _alone(pr)[1]
         err = np.abs(Q - Qa).sum(0) / np.abs(Qa).sum(0)
         assert np.all(err[[0, -1]] <= 1e-6)
-
-
-@pytest.mark.parametrize("dim,solver", [(2, "HLLC"), (3, "Exact")])
-@pytest.mark.parametrize("lanes", [1, 4])
-def test_grad_variants_give_the_same_result(cuda_ok, dim, solver, lanes):
-    """the two-stage gather pipeline of the gradient kernel sums the same
-    faces in the same order: bitwise the same steps, in a group and alone"""
-    from shadowfax_b200.hydro import Context, FluxPass, Group, RiemannSolverFactory
-    sizes = [2500, 900] if dim == 2 else [2000, 700]
-    probs = _problems(dim, solver, sizes)
-    ctx = Context(dim, RiemannSolverFactory.generate(solver), 1)
-    results = {}
-    for v in (0, 1):
-        members = [FluxPass(ctx, pr.mesh) for pr in probs]
-        for fp, pr in zip(members, probs):
-            fp.set_primitive(pr.W0)
-        g = Group(ctx, members, [pr.dt for pr in probs])
-        g.set_lanes(lanes)
-        g.set_grad_variant(v)
-        assert g.grad_variant == v
-        assert np.all(g.step(probs[0].nsteps, graph=True) == 0)
-        results[v] = [fp.state()[1] for fp in members]
-        g.close()
-        for fp in members:
-            fp.close()
-        fp = FluxPass(ctx, probs[0].mesh)
-        fp.set_lanes(lanes)
-        fp.set_grad_variant(v)
-        fp.set_primitive(probs[0].W0)
-        assert fp.step(probs[0].dt, probs[0].nsteps).status == 0
-        results[("alone", v)] = fp.state()[1]
-        fp.close()
-    for a, b in zip(results[1], results[0]):
-        np.testing.assert_array_equal(a, b)
-    np.testing.assert_array_equal(results[("alone", 1)], results[("alone", 0)])
-    np.testing.assert_array_equal(results[("alone", 0)], results[0][0])
 
 
 @pytest.mark.parametrize("dim,solver", [(2, "Exact"), (3, "Exact"), (3, "HLLC")])

@@ -61,25 +61,25 @@ def test_requests_in_a_mix_equal_requests_alone(cuda_ok, precision):
 
 
 def test_tuned_server(cuda_ok):
-    """kernel settings per class: the pipelined gradient kernel and the
-    80-register face kernels change the schedule only (bitwise the same
-    results as alone); the gamma = 5/3 exact forms stay within the split
-    pass's round-off; an FP64 server refuses tuning"""
+    """kernel settings per class: the 80-register face kernels change the
+    schedule only (bitwise the same results as alone); other lanes per cell
+    and the gamma = 5/3 exact forms stay within the split pass's round-off;
+    an FP64 server refuses tuning"""
     from shadowfax_b200._lib import SfxError
     probs = _problems()
     classes = [(d, s) for d in (2, 3) for s in ("Exact", "HLLC")]
-    res, st = _serve(probs, 1, tuning={c: (0, 1, 1) for c in classes})
+    res, st = _serve(probs, 1, tuning={c: (0, 1) for c in classes})
     assert st.completed == len(probs) and st.failed == 0
     for pr, r in zip(probs, res):
         np.testing.assert_array_equal(r.Q, _alone(pr, 1)[1])
-    res, _ = _serve(probs, 1, tuning={c: (2, 1, 3) for c in classes})
+    res, _ = _serve(probs, 1, tuning={c: (2, 3) for c in classes})
     for pr, r in zip(probs, res):
         assert r.status == 0
         Q = _alone(pr, 1)[1]
         err = np.abs(r.Q - Q).sum(0) / np.abs(Q).sum(0)
         assert np.all(err[[0, -1]] <= 1e-6), err
     with pytest.raises(SfxError):
-        _serve(probs[:1], 0, tuning={(2, "HLLC"): (0, 0, 0)})
+        _serve(probs[:1], 0, tuning={(2, "HLLC"): (0, 0)})
 
 
 def test_one_request_alone_and_in_mix(cuda_ok):
