@@ -1065,12 +1065,12 @@ def bench_serve(args, rank, world, local, torch):
     }
 
 
-def flux_error_by_branch(pr, device):
-    """one flux pass from the initial state in FP64 and in split precision:
-    relative L1 error of the per-face dQ (mass, momentum, energy) over all
-    faces and over the faces of each FP64 wave pattern (shock, rarefaction,
-    near-vacuum), and the largest per-face error relative to the largest
-    |dQ| of its field"""
+def flux_error_by_branch(pr, device, face_variant=0):
+    """one flux pass from the initial state in FP64 and in split precision
+    (the benchmarked face-kernel variant): relative L1 error of the per-face
+    dQ (mass, momentum, energy) over all faces and over the faces of each
+    FP64 wave pattern (shock, rarefaction, near-vacuum), and the largest
+    per-face error relative to the largest |dQ| of its field"""
     from shadowfax_b200 import _lib as L
     from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
     out = {}
@@ -1078,6 +1078,8 @@ def flux_error_by_branch(pr, device):
         ctx = Context(pr.mesh.dim, RiemannSolverFactory.generate(pr.solver, pr.gamma), prec,
                       device=device)
         fp = FluxPass(ctx, pr.mesh)
+        if prec == L.PREC_SPLIT:
+            fp.set_face_variant(face_variant or 0)
         fp.set_primitive(pr.W0)
         grad, dQ, br, rc, _ = fp.flux_pass(pr.dt)
         fp.close()
@@ -1212,9 +1214,12 @@ def main():
     fp.set_primitive(pr.W0)
     faces = mesh.n_active_faces
     dt = pr.dt
-    lanes = None
-    if args.precision == "split" and args.workload == "sedov3d":
-        lanes = fp.tune(dt, 3)     # lanes per cell for the gradient/update kernels
+    lanes = face_variant = None
+    if args.precision == "split":
+        # the timing tuners (they step the state; it is loaded again after):
+        # lanes per cell of the gradient/update kernels, face-kernel variant
+        lanes = fp.tune(dt, 3)
+        face_variant = fp.tune_faces(dt, 3)
         fp.set_primitive(pr.W0)
 
     # a mesh whose device data fit in the L2 is timed step by step, with a
@@ -1312,7 +1317,8 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pr)
-    flux_err = flux_error_by_branch(pr, local) if args.precision == "split" and rank == 0 else None
+    flux_err = (flux_error_by_branch(pr, local, face_variant)
+                if args.precision == "split" and rank == 0 else None)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -1322,7 +1328,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": problem_text(args, pr),
                        "solver": pr.solver, "precision": args.precision,
-                       "lanes_per_cell": lanes,
+                       "lanes_per_cell": lanes, "face_variant": face_variant,
                        "l2": ("working set > L2 (no flush)" if flush is None else
                               "L2 flushed between steps (256 MB write outside the timed "
                               "events; step times summed)"),

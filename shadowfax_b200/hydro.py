@@ -278,9 +278,24 @@ class FluxPass:
         return pos
 
     def set_face_variant(self, variant: int):
-        """split pass: register cap of the face kernel (0: 64 registers, four
-        blocks per SM; 1: 80 registers, three)"""
+        """split pass: face-kernel variant (SFX_FACE_VARIANTS: 0 and 1 the
+        64- and 80-register kernels; 2 and 3 the exact solver's gamma = 5/3
+        forms, HLLC's stored dW/dt; include/sfxflux.h)"""
         L.check(L.lib().sfx_mesh_set_face_variant(self.h, variant), "sfx_mesh_set_face_variant")
+
+    def tune_faces(self, dt: float, reps: int = 3) -> int:
+        """split pass: time the face-kernel variants on this mesh and keep the
+        fastest (advances the state by FACE_VARIANTS * (reps + 1) steps: call
+        before loading the initial state); returns it"""
+        best, best_ms = 0, 1e30
+        for v in range(L.FACE_VARIANTS):
+            self.set_face_variant(v)
+            self.step_timed(dt, 1)
+            ms, _ = self.step_timed(dt, reps)
+            if ms[1] < best_ms:
+                best, best_ms = v, ms[1]
+        self.set_face_variant(best)
+        return best
 
     def set_ranges(self, grad_cells: int, flux_faces: int, update_cells: int):
         """one part of a mesh split over several devices (plain FP64):
