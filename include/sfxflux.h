@@ -207,7 +207,7 @@ int sfx_step(sfx_mesh* mesh, double dt, int32_t nsteps, sfx_stats* stats);
 int sfx_step_moving(sfx_mesh* mesh, double dt, int32_t periodic, double* positions,
                     sfx_stats* stats);
 
-/* ---- local (hierarchical) time steps, plain FP64 ----
+/* ---- local (hierarchical) time steps, plain FP64 and split ----
  * Every cell advances on its own step of the integer timeline: 2^60 ticks
  * from time 0 to t_total (TimeLine, src/TimeLine.hpp:145-178).  A cell is
  * active at tick t_now when its step starts there.
@@ -229,7 +229,10 @@ int sfx_step_moving(sfx_mesh* mesh, double dt, int32_t periodic, double* positio
  * cell's end and clamped to [min_step, max_step] ticks; the cell's next step
  * starts at its end; *system_step receives the smallest new step (the next
  * system step).  Start a run with t_next = 0 (every cell's end is 0).
- * SFX_ERR_UNSUPPORTED for split-precision meshes and parts. */
+ * Split-precision meshes (not clones) run the same window with their
+ * kernels (per-face step and timefac in FP32 beside the FP64 accumulation;
+ * the CFL steps from their FP32 states); sfx_mesh_set/get_gradients are
+ * plain FP64 only.  SFX_ERR_UNSUPPORTED for parts and split clones. */
 int sfx_mesh_set_timesteps(sfx_mesh* mesh, const uint64_t* start, const uint64_t* end);
 int sfx_mesh_get_timesteps(sfx_mesh* mesh, uint64_t* start, uint64_t* end);
 int sfx_mesh_set_gradients(sfx_mesh* mesh, const double* grad);
@@ -282,9 +285,10 @@ int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
  * formed per face; exact solver with gamma = 5/3: the p* step's powers as a
  * fifth root by Newton's method and the sampling's powers as integer powers;
  * other gamma: as 0), 3 (exact solver with gamma = 5/3: 2 with 80
- * registers; other gamma and HLLC: as 1).  Variants 0 and 1 change the
- * schedule only, not the results; 2 and 3 change round-off within the split
- * pass's tolerance. */
+ * registers; other gamma: as 1; HLLC: 48 registers, five blocks).  Variants
+ * 0 and 1, and 3 for HLLC, change the schedule only, not the results; 2, and
+ * 3 for the exact solver, change round-off within the split pass's
+ * tolerance. */
 #define SFX_FACE_VARIANTS 4
 int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
 

@@ -745,8 +745,11 @@ static int ensure_local(sfx_mesh* m) {
     return SFX_OK;
 }
 
+/* local time steps: plain FP64 meshes, and split meshes that are not
+ * clones (a clone is a request instance of the server) */
 static bool local_ok(const sfx_mesh* m) {
-    return m->ctx->cfg.precision == SFX_PREC_FP64 && !m->d.ranged;
+    if(m->d.ranged) return false;
+    return m->ctx->cfg.precision == SFX_PREC_FP64 || !m->clone;
 }
 
 int sfx_mesh_set_timesteps(sfx_mesh* m, const uint64_t* start, const uint64_t* end) {
@@ -810,15 +813,24 @@ int sfx_step_window(sfx_mesh* m, double t_total, uint64_t t_now, uint64_t t_next
     sfx_ctx* c = m->ctx;
     cudaStream_t s = c->stream;
     sfx_dmesh& d = m->d;
+    const bool split = c->cfg.precision == SFX_PREC_SPLIT;
     d.local = 1;
     d.t_now = t_now;
     d.t_next = t_next;
     d.t_total = t_total;
     int rc = reset_err(m);
-    /* the cells starting a step set their generator velocity (the mesh stays) */
+    /* the cells starting a step set their generator velocity (the mesh
+     * stays); a split mesh's FP32 states are exported to its FP64 W first */
+    if(!rc && split) rc = sfx_split_export_W(&d, s);
     if(!rc) rc = sfx_fp64_move_velocities(&d, c->cfg.gamma, 0., periodic ? 1 : 0, 0, s);
+    /* a split mesh's kernels read the window from its device table */
+    if(!rc && split) rc = setup_self(m, s);
     for(int ph = 0; ph < 3 && !rc; ++ph) rc = run_phase(m, ph, 1., 0, s);
     d.local = 0;
+    if(split) {
+        const int r2 = setup_self(m, s);
+        if(!rc) rc = r2;
+    }
     if(rc) return rc;
     sfx_stats local;
     sfx_stats* out = st ? st : &local;
@@ -844,6 +856,8 @@ int sfx_timestep_bins(sfx_mesh* m, double t_total, double cfl, uint64_t max_step
     SFX_TRY(reset_err(m));
     const unsigned long long smax = max_step;
     SFX_TRY(h2d(m->d_smin, &smax, 1, s));
+    /* a split mesh: the CFL steps from its FP32 states, exported to FP64 */
+    if(c->cfg.precision == SFX_PREC_SPLIT) SFX_TRY(sfx_split_export_W(&d, s));
     SFX_TRY(sfx_fp64_timestep_bins(&d, c->cfg.gamma, cfl, max_step, min_step, m->d_smin, s));
     unsigned long long out = 0;
     SFX_TRY(cuda_ok(cudaMemcpyAsync(&out, m->d_smin, sizeof out, cudaMemcpyDeviceToHost, s)));

@@ -315,8 +315,11 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
     constexpr int S = D + 2, G = GradVec4<D>::value;
     const int i = t / LPC, lane = t % LPC;
     if(t == 0) *m.slowq_n = 0; /* a new step: empty the queued-face list */
-    /* whole warps stay alive for the shuffles; lanes past the end idle */
-    const bool live = i < m.n_cells && !failed(m.err);
+    /* whole warps stay alive for the shuffles; lanes past the end idle, and so
+     * do the lanes of a cell that is not active (local time steps: it keeps
+     * its gradients, src/Simulation.cpp:414-420) */
+    const bool live = i < m.n_cells && !failed(m.err) &&
+                      !(m.local && i < m.n_cells && m.tstart[i] != m.t_now);
     const int ic = live ? i : 0;
     const Cell<D> own = load_cell<D>(m.cw, ic);
     const float4 xv = __ldg(m.cx + ic);
@@ -1208,6 +1211,7 @@ template <int D>
 struct FaceWork {
     float WL[D + 2], WR[D + 2], n[D];
     float A, limL, limR;
+    float dt; /* the face's time step (the step's dt; the shorter cell step with local steps) */
     float v[D]; /* face velocity (moving mesh; 0 on a static one) */
     bool mirror;
 };
@@ -1215,21 +1219,43 @@ struct FaceWork {
 /* false: nothing to solve (a face past the end, or of zero area, whose dQ is
  * written as zero here) */
 template <int D, bool STORED, bool MOVING = false>
-__device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma, const float hdt,
+__device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma, const float dt,
                                           const int f, FaceWork<D>& w) {
     constexpr int S = D + 2;
     float c[D], r[D], rn;
     geom<D>(m.fg, f, w.A, c, r, rn);
-    if(w.A == 0.f) {
+    const int2 fi = __ldg(m.fi + f);
+    const int iL = fi.x;
+    w.mirror = fi.y < 0;
+    const int iR = w.mirror ? 0 : (fi.y & kIndexMask);
+    /* local time steps (VorFace.cpp:672-697): a face is computed when either
+     * of its cells is active, with the shorter of the two cells' steps;
+     * timefac = that step / the longer one scales the over-flux limits */
+    w.dt = dt;
+    float timefac = 1.f;
+    bool active = true;
+    if(m.local) {
+        const bool aL = m.tstart[iL] == m.t_now;
+        const bool aR = !w.mirror && m.tstart[iR] == m.t_now;
+        active = aL || aR;
+        if(active) {
+            double dtf = sfx_realtime(m.t_total, m.tend[iL] - m.tstart[iL]), dtmax = dtf;
+            if(!w.mirror) {
+                const double dtR = sfx_realtime(m.t_total, m.tend[iR] - m.tstart[iR]);
+                dtf = fmin(dtf, dtR);
+                dtmax = fmax(dtmax, dtR);
+                timefac = (float)(dtf / dtmax);
+            }
+            w.dt = (float)dtf;
+        }
+    }
+    if(w.A == 0.f || !active) {
         m.dqm[f] = make_float2(0.f, 0.f);
 #pragma unroll
         for(int l = 0; l < D; ++l) m.dqv[(size_t)l * m.n_faces + f] = 0.;
         return false;
     }
-    const int2 fi = __ldg(m.fi + f);
-    const int iL = fi.x;
-    w.mirror = fi.y < 0;
-    const int iR = w.mirror ? 0 : (fi.y & kIndexMask);
+    const float hdt = 0.5f * w.dt;
     const float irn = 1.f / rn;
 #pragma unroll
     for(int l = 0; l < D; ++l) w.n[l] = -r[l] * irn;
@@ -1251,7 +1277,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         w.v[l] = MOVING ? (float)__ldg(m.vel + (size_t)l * m.n_faces + f) : 0.f;
         if(MOVING) w.WL[1 + l] -= w.v[l];
     }
-    w.limL = w.A / cL.tarea * cL.Qm;
+    w.limL = w.A / cL.tarea * timefac * cL.Qm;
     w.limR = 0.f;
     float rr = 1.f;
     if(!w.mirror) {
@@ -1264,7 +1290,7 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
 #pragma unroll
             for(int l = 0; l < D; ++l) w.WR[1 + l] -= w.v[l];
         }
-        w.limR = w.A / cR.tarea * cR.Qm;
+        w.limR = w.A / cR.tarea * timefac * cR.Qm;
         /* centroid difference (unshifted centroids, as the reference) */
         float sh[D];
 #pragma unroll
@@ -1364,8 +1390,9 @@ __device__ __forceinline__ void hllc_deboost_split(const float* v, const float* 
 /* Last phase of every face kernel: dt A flux with the over-flux limiter, the
  * face's dQ records and its status. */
 template <int D>
-__device__ __forceinline__ void face_dq(const sfx_dmesh& m, const float dt, const int f,
-                                        const FaceWork<D>& w, SFlux<D> F, int status) {
+__device__ __forceinline__ void face_dq(const sfx_dmesh& m, const int f, const FaceWork<D>& w,
+                                        SFlux<D> F, int status) {
+    const float dt = w.dt;
     if(w.mirror) {
         /* the reflective Riemann problem has zero normal velocity at the wall:
          * no mass, energy or advected momentum crosses it, only the pressure
@@ -1419,7 +1446,7 @@ __device__ __forceinline__ bool sfaces_body(const sfx_dmesh& m, const sfx_solver
     FaceWork<D> w;
     /* by default HLLC forms dW/dt itself and the exact solver's kernels read
      * it (STORED_DW: from the per-cell record) */
-    if(!face_work<D, STORED_DW, MOVING>(m, (float)sp.gamma, 0.5f * dt, f, w)) return false;
+    if(!face_work<D, STORED_DW, MOVING>(m, (float)sp.gamma, dt, f, w)) return false;
     SFlux<D> F;
     int status = SFX_OK;
     if constexpr(SOLVER == SFX_SOLVER_HLLC) {
@@ -1438,7 +1465,7 @@ __device__ __forceinline__ bool sfaces_body(const sfx_dmesh& m, const sfx_solver
         status = sexact<D, MODE>(sp, dWL, dWR, dn, w.mirror, h);
         exact_flux<D>(sp.gamma, h, dn, w.v, MOVING, F);
     }
-    face_dq<D>(m, dt, f, w, F, status);
+    face_dq<D>(m, f, w, F, status);
     return false;
 }
 
@@ -1684,6 +1711,17 @@ __device__ __forceinline__ void sapply_body(const sfx_dmesh& m, const double gam
         report_cell(m.err, i, SFX_ERR_NEG_STATE);
         return;
     }
+    if(m.local && m.tend[i] != m.t_next) {
+        /* local time steps: a cell in the middle of its step takes its
+         * active neighbours' flux into Q; its W waits for the end of its
+         * step (src/Simulation.cpp:791-836); the record's mass (the
+         * over-flux limit) follows Q */
+#pragma unroll
+        for(int k = 0; k < S; ++k) m.Q[(size_t)k * n + i] = Q[k];
+        const Cell<D> c = load_cell<D>(m.cw, i);
+        store_cell<D>(m.cw, i, c.W, (float)Q[0], c.tarea);
+        return;
+    }
     /* get_W (ExactRiemannSolver.cpp:716-766 / HLLCRiemannSolver.cpp:495-535) */
     const double V = m.vol[i];
     double W[S];
@@ -1755,7 +1793,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     __shared__ float sW[2 * S][kExactBlock];
     __shared__ float sn[D][kExactBlock];
     __shared__ float sv[MOVING ? D : 1][kExactBlock]; /* one unused row when static */
-    __shared__ float sA[kExactBlock], sLL[kExactBlock], sLR[kExactBlock];
+    __shared__ float sA[kExactBlock], sLL[kExactBlock], sLR[kExactBlock], sdt[kExactBlock];
     __shared__ int sf[kExactBlock];
     __shared__ int sbase[kNClass][NW];
     __shared__ int stotal;
@@ -1769,7 +1807,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     FaceWork<D> w;
     int cls = kClassNone;
     if(f < m.n_faces && !failed(m.err) &&
-       face_work<D, true, MOVING>(m, (float)sp.gamma, 0.5f * dt, f, w))
+       face_work<D, true, MOVING>(m, (float)sp.gamma, dt, f, w))
         cls = wave_class<D>(sp, w);
     queue_faces(m, cls == kClassQueue, f);
     /* phase 2: counting sort by class */
@@ -1810,6 +1848,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
             if(MOVING) sv[MOVING ? l : 0][slot] = w.v[l];
         }
         sA[slot] = w.A;
+        sdt[slot] = w.dt;
         sLL[slot] = w.limL;
         sLR[slot] = w.limR;
         sf[slot] = f | (w.mirror ? (int)kRightBit : 0);
@@ -1831,10 +1870,11 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
             /* what face_dq reads of the face */
             FaceWork<D> v;
             v.A = sA[t];
+            v.dt = sdt[t];
             v.limL = sLL[t];
             v.limR = sLR[t];
             v.mirror = e < 0;
-            face_dq<D>(m, dt, fq, v, F, st);
+            face_dq<D>(m, fq, v, F, st);
         }
     }
     queue_faces(m, push, fq);
@@ -2016,7 +2056,10 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                     k_group_sfaces_slow<D, false, SFX_SOLVER_HLLC, true>
                             <<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
                 } else {
-                    if(v == 1)
+                    if(v == 3)
+                        k_group_sfaces<D, SFX_SOLVER_HLLC, 5><<<g->blocks[1], 256, 0, s>>>(
+                                g->tab, pre1, nm, *sp);
+                    else if(v == 1)
                         k_group_sfaces<D, SFX_SOLVER_HLLC, 3><<<g->blocks[1], 256, 0, s>>>(
                                 g->tab, pre1, nm, *sp);
                     else
@@ -2098,7 +2141,7 @@ int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant) {
         if(sp->gamma != 5. / 3. && variant >= 2) return variant - 2;
         return variant;
     }
-    return variant == 3 ? 1 : variant; /* HLLC: 3 is 1 */
+    return variant; /* HLLC: 3 is the 48-register kernel */
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {
