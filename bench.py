@@ -790,7 +790,7 @@ def run_resident(pool, reqs, nseg, warmup, chunk, torch, local):
 # (2,396,113 faces) and a 700,000-cell one in 2D; the gathers and the per-face
 # records scale with the faces, so a launch over F faces moves about F times
 # these
-TRAFFIC_B_PER_FACE = {("faces", 3, "Exact"): 110.1, ("faces", 3, "HLLC"): 105.5,
+TRAFFIC_B_PER_FACE = {("faces", 3, "Exact"): 106.8, ("faces", 3, "HLLC"): 102.0,
                       ("gradients", 3): 61.4, ("update", 3): 52.8,
                       ("faces", 2, "Exact"): 104.8, ("faces", 2, "HLLC"): 98.6,
                       ("gradients", 2): 73.3, ("update", 2): 54.2}
