@@ -112,18 +112,16 @@ __device__ __forceinline__ double limit1(double phimid0, double phiL, double phi
     double phimin = fmin(phiL, phiR);
     double phimax = fmax(phiL, phiR);
     double phibar = phiL + dnrm / r * (phiR - phiL);
-    double phiplus, phiminus;
-    if((phimax + delta1) * phimax > 0.)
-        phiplus = phimax + delta1;
-    else
-        phiplus = phimax / (1. + delta1 / fabs(phimax));
-    if((phimin - delta1) * phimin > 0.)
-        phiminus = phimin - delta1;
-    else
-        phiminus = phimin / (1. + delta1 / fabs(phimin));
     if(phiL == phiR) return phiL;
-    if(phiL < phiR) return fmax(phiminus, fmin(phibar + delta2, phimid0));
-    return fmin(phiplus, fmax(phibar - delta2, phimid0));
+    /* only the bound the result uses (phi- when phiL < phiR, else phi+), with
+     * the sign-preserving fallback where the shifted extreme changes sign:
+     * the reference's values, without the other bound's divisions */
+    const bool up = phiL < phiR;
+    const double ext = up ? phimin : phimax;
+    double bound = up ? ext - delta1 : ext + delta1;
+    if(!(bound * ext > 0.)) bound = ext / (1. + delta1 / fabs(ext));
+    if(up) return fmax(bound, fmin(phibar + delta2, phimid0));
+    return fmin(bound, fmax(phibar - delta2, phimid0));
 }
 
 /* mirror a state across a reflective face: transform, flip the normal
