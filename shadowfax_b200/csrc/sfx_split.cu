@@ -435,11 +435,10 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
             float dp = 0.f;
 #pragma unroll
             for(int l = 0; l < D; ++l) dp += delta[l][k] * d[l];
+            /* max((Wmax - W) / dp, (Wmin - W) / dp): the sign of dp picks
+             * the operand (Wmax - W >= 0 >= Wmin - W) */
             float mx = 1.f;
-            if(dp != 0.f) {
-                const float id = 1.f / dp;
-                mx = fmaxf((Wmax[k] - W[k]) * id, (Wmin[k] - W[k]) * id);
-            }
+            if(dp != 0.f) mx = (dp > 0.f ? Wmax[k] - W[k] : Wmin[k] - W[k]) * (1.f / dp);
             alpha[k] = fminf(alpha[k], mx);
         }
     }
