@@ -285,11 +285,13 @@ int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
  * formed per face; exact solver with gamma = 5/3: the p* step's powers as a
  * fifth root by Newton's method and the sampling's powers as integer powers;
  * other gamma: as 0), 3 (exact solver with gamma = 5/3: 2 with 80
- * registers; other gamma: as 1; HLLC: 48 registers, five blocks).  Variants
- * 0 and 1, and 3 for HLLC, change the schedule only, not the results; 2, and
- * 3 for the exact solver, change round-off within the split pass's
- * tolerance. */
-#define SFX_FACE_VARIANTS 4
+ * registers; other gamma: as 1; HLLC: 48 registers, five blocks), 4 (the
+ * left cells of each 256-face block staged in shared memory by bulk copies:
+ * exact solver as 2 at gamma = 5/3, as 0 otherwise; HLLC as 3).  Variants 0
+ * and 1, 3 for HLLC and 4 change the schedule only, not the results of the
+ * variant they stage for; 2, and 3 for the exact solver, change round-off
+ * within the split pass's tolerance. */
+#define SFX_FACE_VARIANTS 5
 int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
 
 /* ---- one mesh over several devices (plain FP64) ----

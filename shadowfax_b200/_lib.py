@@ -29,7 +29,7 @@ SFX_ERR_TOO_LARGE, SFX_ERR_IO, SFX_ERR_TIMESTEP = 13, 14, 15
 
 SOLVER_EXACT, SOLVER_HLLC = 0, 1
 PREC_FP64, PREC_SPLIT = 0, 1
-FACE_VARIANTS = 4  # SFX_FACE_VARIANTS
+FACE_VARIANTS = 5  # SFX_FACE_VARIANTS
 FACE_REAL, FACE_PERIODIC, FACE_MIRROR = 0, 1, 2
 
 

@@ -69,10 +69,20 @@ struct Cell {
     float Qm, tarea;
 };
 
-template <int D>
+/* GL: global memory through the read-only path; otherwise plain loads (a
+ * copy in shared memory) */
+template <bool GL>
+__device__ __forceinline__ float4 ld4(const float4* p) {
+    if constexpr(GL)
+        return __ldg(p);
+    else
+        return *p;
+}
+
+template <int D, bool GL = true>
 __device__ __forceinline__ Cell<D> load_cell(const float4* __restrict__ cw, int i) {
-    const float4 a = __ldg(cw + 2 * i);
-    const float4 b = __ldg(cw + 2 * i + 1);
+    const float4 a = ld4<GL>(cw + 2 * i);
+    const float4 b = ld4<GL>(cw + 2 * i + 1);
     Cell<D> c;
     c.W[0] = a.x;
     c.W[1] = a.y;
@@ -120,7 +130,7 @@ __device__ __forceinline__ void sdwdt(float gamma, const float* W, const float (
 /* a cell's gradients and dW/dt: with STORED dW/dt from its record (the
  * exact solver's kernels, bound by instruction issue), otherwise formed here
  * (the HLLC face kernel, closer to the memory bound) */
-template <int D, bool STORED>
+template <int D, bool STORED, bool GL = true>
 __device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
                                           const float4* __restrict__ cdw, int i, float gamma,
                                           const float* W, float (*g)[D + 2], float* dWdt,
@@ -129,7 +139,7 @@ __device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
     float t[4 * G];
 #pragma unroll
     for(int q = 0; q < G; ++q) {
-        const float4 v = __ldg(cg + (size_t)G * i + q);
+        const float4 v = ld4<GL>(cg + (size_t)G * i + q);
         t[4 * q] = v.x;
         t[4 * q + 1] = v.y;
         t[4 * q + 2] = v.z;
@@ -143,7 +153,7 @@ __device__ __forceinline__ void load_grad(const float4* __restrict__ cg,
         float u[4 * H];
 #pragma unroll
         for(int q = 0; q < H; ++q) {
-            const float4 v = __ldg(cdw + (size_t)H * i + q);
+            const float4 v = ld4<GL>(cdw + (size_t)H * i + q);
             u[4 * q] = v.x;
             u[4 * q + 1] = v.y;
             u[4 * q + 2] = v.z;
@@ -1207,6 +1217,65 @@ __device__ int sexact(const sfx_solver_params& s, double* WL, double* WR, const 
  * Hancock half step with the pairwise limiter, VorFace.cpp:670-838), its unit
  * normal and what its dQ needs.  The over-flux limits lim_K = A / total_area_K
  * * Q.m_K (VorFace.cpp:837-866) are formed here once. */
+/* ------------------- left-cell tiles staged by bulk copies -------------------
+ * A 256-face block of the face list references a short range of left cells:
+ * the builder emits each cell's faces together, in ascending cell order, and
+ * cells are in spatial (Morton) order, so a block's left cells are about 33
+ * consecutive cells in 3D and 85 in 2D on the random-field meshes.  The
+ * staged face kernels (variant 4) copy the records of the block's left-cell
+ * range -- state, position - centroid, gradients, and dW/dt where the kernel
+ * reads it -- into shared memory with one 1D bulk copy per array
+ * (cp.async.bulk, completion counted on an mbarrier, no multicast), and
+ * face_work reads a left cell from there.  Any face order is valid: the range
+ * is the block's lowest to highest left cell, capped at kTileCells cells, and
+ * a left cell outside it is read from global memory.  Every array is 256-byte
+ * aligned and a record is a whole number of 16-byte units, so each copy
+ * starts and ends on a 16-byte boundary. */
+constexpr int kTileCells = 128;
+
+template <int D>
+struct LeftTile {
+    int c0 = 0, n = 0;          /* staged cells [c0, c0 + n); n = 0: none */
+    const float4* cw = nullptr; /* [2 n] */
+    const float4* cx = nullptr; /* [n] */
+    const float4* cg = nullptr; /* [GradVec4 n] */
+    const float4* cdw = nullptr; /* [DwdtVec4 n] (when staged) */
+    __device__ bool has(int i) const { return (unsigned)(i - c0) < (unsigned)n; }
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+/* one 1D bulk copy global -> shared, completion on mbar (16-byte aligned
+ * addresses, size a multiple of 16) */
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* mbar) {
+    asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(smem_addr(dst)),
+            "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+            : "memory");
+}
+
+/* wait for phase 0 of mbar with an iteration limit; false: gave up */
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, int limit) {
+    const uint32_t a = smem_addr(mbar);
+    for(int it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; "
+                "selp.u32 %0, 1, 0, p; }"
+                : "=r"(done)
+                : "r"(a)
+                : "memory");
+        if(done) return true;
+    }
+    return false;
+}
+
+constexpr int kTileWaitLimit = 1 << 16;
+
 template <int D>
 struct FaceWork {
     float WL[D + 2], WR[D + 2], n[D];
@@ -1218,9 +1287,10 @@ struct FaceWork {
 
 /* false: nothing to solve (a face past the end, or of zero area, whose dQ is
  * written as zero here) */
-template <int D, bool STORED, bool MOVING = false>
+template <int D, bool STORED, bool MOVING = false, bool TILE = false>
 __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma, const float dt,
-                                          const int f, FaceWork<D>& w) {
+                                          const int f, FaceWork<D>& w,
+                                          const LeftTile<D>& tile = LeftTile<D>{}) {
     constexpr int S = D + 2;
     float c[D], r[D], rn;
     geom<D>(m.fg, f, w.A, c, r, rn);
@@ -1259,8 +1329,11 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
     const float irn = 1.f / rn;
 #pragma unroll
     for(int l = 0; l < D; ++l) w.n[l] = -r[l] * irn;
-    const Cell<D> cL = load_cell<D>(m.cw, iL);
-    const float4 xL = __ldg(m.cx + iL);
+    /* the left cell from the block's staged tile when it holds it */
+    const bool tL = TILE && tile.has(iL);
+    const int jL = tL ? iL - tile.c0 : iL;
+    const Cell<D> cL = tL ? load_cell<D, false>(tile.cw, jL) : load_cell<D>(m.cw, iL);
+    const float4 xL = tL ? tile.cx[jL] : __ldg(m.cx + iL);
     const float xmcL[3] = {xL.x, xL.y, xL.z};
     float WLr[S], WRr[S];
 #pragma unroll
@@ -1321,7 +1394,10 @@ __device__ __forceinline__ bool face_work(const sfx_dmesh& m, const float gamma,
         float dL[D], gL[D][S], dWL[S];
 #pragma unroll
         for(int l = 0; l < D; ++l) dL[l] = c[l] + xmcL[l] - 0.5f * r[l];
-        load_grad<D, STORED>(m.cg, m.cdw, iL, gamma, w.WL, gL, dWL, moving);
+        if(tL)
+            load_grad<D, STORED, false>(tile.cg, tile.cdw, jL, gamma, w.WL, gL, dWL, moving);
+        else
+            load_grad<D, STORED>(m.cg, m.cdw, iL, gamma, w.WL, gL, dWL, moving);
 #pragma unroll
         for(int k = 0; k < S; ++k) WLr[k] = w.WL[k];
         spredict<D>(hdt, WLr, w.WL, w.WR, gL, dWL, dL, !w.mirror, rr);
@@ -1435,18 +1511,92 @@ __device__ __forceinline__ void face_dq(const sfx_dmesh& m, const int f, const F
     if(status != SFX_OK) report_face(m.err, f, status);
 }
 
+/* shared-memory copy of a block's left-cell records (DW: with dW/dt) */
+template <int D, bool DW>
+struct TileStore {
+    float4 cw[2 * kTileCells];
+    float4 cx[kTileCells];
+    float4 cg[GradVec4<D>::value * kTileCells];
+    float4 cdw[DW ? DwdtVec4<D>::value * kTileCells : 1];
+    uint64_t mbar;
+    int lo[32], hi[32];
+    int c0, n;
+};
+
+/* stage the left cells of the block's faces (face f for this thread; every
+ * thread of the block calls this): the block's lowest and highest left cell
+ * by warp reductions, then thread 0 starts one bulk copy per array and
+ * every thread waits for them, up to kTileWaitLimit tries.  ok = false: the
+ * copies did not complete in time; the tile is then empty (every cell read
+ * from global memory) and the caller reports the error and waits for the
+ * copies again before it exits. */
+template <int D, bool DW>
+__device__ __forceinline__ LeftTile<D> stage_left_cells(const sfx_dmesh& m, int f,
+                                                        TileStore<D, DW>& ts, bool& ok) {
+    constexpr int G = GradVec4<D>::value, H = DwdtVec4<D>::value;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int lo = 0x7fffffff, hi = -1;
+    if(f < m.n_faces) lo = hi = __ldg(m.fi + f).x;
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if(lane == 0) {
+        ts.lo[warp] = lo;
+        ts.hi[warp] = hi;
+    }
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        int a = 0x7fffffff, b = -1;
+        for(int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a = min(a, ts.lo[w]);
+            b = max(b, ts.hi[w]);
+        }
+        const int n = b >= a ? min(b - a + 1, kTileCells) : 0;
+        ts.c0 = a;
+        ts.n = n;
+        if(n) {
+            const uint32_t bar = smem_addr(&ts.mbar);
+            const uint32_t bytes = (uint32_t)n * (32u + 16u + 16u * G + (DW ? 16u * H : 0u));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"(bytes)
+                         : "memory");
+            bulk_copy(ts.cw, m.cw + 2 * (size_t)a, 32u * n, &ts.mbar);
+            bulk_copy(ts.cx, m.cx + a, 16u * n, &ts.mbar);
+            bulk_copy(ts.cg, m.cg + (size_t)G * a, 16u * G * n, &ts.mbar);
+            if(DW) bulk_copy(ts.cdw, m.cdw + (size_t)H * a, 16u * H * n, &ts.mbar);
+        }
+    }
+    __syncthreads();
+    LeftTile<D> t;
+    ok = true;
+    if(ts.n) {
+        ok = mbar_wait(&ts.mbar, kTileWaitLimit);
+        if(ok) {
+            t.c0 = ts.c0;
+            t.n = ts.n;
+            t.cw = ts.cw;
+            t.cx = ts.cx;
+            t.cg = ts.cg;
+            t.cdw = ts.cdw;
+        }
+    }
+    return t;
+}
+
 /* one face; true when the face is left for the queued-face kernel (HLLC in
  * kSolveDefer mode whose FP32 flux is not finite) */
 template <int D, int SOLVER, int MODE, bool STORED_DW = SOLVER != SFX_SOLVER_HLLC,
-          bool MOVING = false>
+          bool MOVING = false, bool TILE = false>
 __device__ __forceinline__ bool sfaces_body(const sfx_dmesh& m, const sfx_solver_params& sp,
-                                            const float dt, const int f) {
+                                            const float dt, const int f,
+                                            const LeftTile<D>& tile = LeftTile<D>{}) {
     constexpr int S = D + 2;
     if(f >= m.n_faces || failed(m.err)) return false;
     FaceWork<D> w;
     /* by default HLLC forms dW/dt itself and the exact solver's kernels read
      * it (STORED_DW: from the per-cell record) */
-    if(!face_work<D, STORED_DW, MOVING>(m, (float)sp.gamma, dt, f, w)) return false;
+    if(!face_work<D, STORED_DW, MOVING, TILE>(m, (float)sp.gamma, dt, f, w, tile)) return false;
     SFlux<D> F;
     int status = SFX_OK;
     if constexpr(SOLVER == SFX_SOLVER_HLLC) {
@@ -1782,7 +1932,7 @@ __device__ __forceinline__ bool member_done(const sfx_group_entry* tab, int mi) 
     return sl && *(volatile const int32_t*)sl <= 0;
 }
 
-template <int D, int MINB, bool MOVING = false, bool G53 = false>
+template <int D, int MINB, bool MOVING = false, bool G53 = false, bool TILE = false>
 __global__ void __launch_bounds__(kExactBlock, MINB)
         k_group_sfaces_exact(const sfx_group_entry* tab, const int* pre, int nm,
                              sfx_solver_params sp) {
@@ -1803,13 +1953,24 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     const float dt = tab[mi].dt;
     const int f = (blockIdx.x - __ldg(pre + mi)) * kExactBlock + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    /* phase 1 (no thread leaves before the block's barriers) */
+    /* phase 1 (no thread leaves before the block's barriers); TILE: the
+     * block's left cells staged in shared memory first */
+    LeftTile<D> tile;
+    bool tile_ok = true;
+    uint64_t* tile_bar = nullptr;
+    if constexpr(TILE) {
+        __shared__ __align__(16) TileStore<D, true> ts;
+        tile = stage_left_cells<D, true>(m, f, ts, tile_ok);
+        tile_bar = &ts.mbar;
+        if(!tile_ok && threadIdx.x == 0) report_face(m.err, f, SFX_ERR_CUDA);
+    }
     FaceWork<D> w;
     int cls = kClassNone;
     if(f < m.n_faces && !failed(m.err) &&
-       face_work<D, true, MOVING>(m, (float)sp.gamma, dt, f, w))
+       face_work<D, true, MOVING, TILE>(m, (float)sp.gamma, dt, f, w, tile))
         cls = wave_class<D>(sp, w);
     queue_faces(m, cls == kClassQueue, f);
+    if(TILE && !tile_ok) mbar_wait(tile_bar, kTileWaitLimit); /* copies still in flight */
     /* phase 2: counting sort by class */
     unsigned mine = 0; /* the ballot of this thread's class */
 #pragma unroll
@@ -1890,7 +2051,7 @@ __global__ void __launch_bounds__(256, 4) k_group_sgrad(const sfx_group_entry* t
 }
 
 template <int D, int SOLVER, int MINB, bool STORED_DW = SOLVER != SFX_SOLVER_HLLC,
-          bool MOVING = false>
+          bool MOVING = false, bool TILE = false>
 __global__ void __launch_bounds__(256, MINB)
         k_group_sfaces(const sfx_group_entry* tab, const int* pre, int nm,
                        sfx_solver_params sp) {
@@ -1899,9 +2060,21 @@ __global__ void __launch_bounds__(256, MINB)
     if(member_done(tab, mi)) return; /* the same for every thread of the block */
     const sfx_dmesh& m = tab[mi].m;
     const int f = (blockIdx.x - __ldg(pre + mi)) * blockDim.x + threadIdx.x;
-    const bool push =
-            sfaces_body<D, SOLVER, kSolveDefer, STORED_DW, MOVING>(m, sp, tab[mi].dt, f);
-    queue_faces(m, push, f);
+    if constexpr(TILE) {
+        /* the block's left cells staged in shared memory first */
+        __shared__ __align__(16) TileStore<D, STORED_DW> ts;
+        bool ok;
+        const LeftTile<D> tile = stage_left_cells<D, STORED_DW>(m, f, ts, ok);
+        if(!ok && threadIdx.x == 0) report_face(m.err, f, SFX_ERR_CUDA);
+        const bool push = sfaces_body<D, SOLVER, kSolveDefer, STORED_DW, MOVING, true>(
+                m, sp, tab[mi].dt, f, tile);
+        queue_faces(m, push, f);
+        if(!ok) mbar_wait(&ts.mbar, kTileWaitLimit); /* copies still in flight */
+    } else {
+        const bool push =
+                sfaces_body<D, SOLVER, kSolveDefer, STORED_DW, MOVING>(m, sp, tab[mi].dt, f);
+        queue_faces(m, push, f);
+    }
 }
 
 /* The queued faces of every member, one per thread.  Exact solver: the
@@ -2033,7 +2206,13 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                 sfx_count_launches(1);
             } else if(sp->kind == SFX_SOLVER_EXACT) {
                 const int v = sfx_split_face_variant_kernel(sp, g->face_variant);
-                if(v == 3)
+                if(v == 4 && sp->gamma == 5. / 3.)
+                    k_group_sfaces_exact<D, 4, false, true, true>
+                            <<<g->blocks[1], kExactBlock, 0, s>>>(g->tab, pre1, nm, *sp);
+                else if(v == 4)
+                    k_group_sfaces_exact<D, 4, false, false, true>
+                            <<<g->blocks[1], kExactBlock, 0, s>>>(g->tab, pre1, nm, *sp);
+                else if(v == 3)
                     k_group_sfaces_exact<D, 3, false, true><<<g->blocks[1], kExactBlock, 0, s>>>(
                             g->tab, pre1, nm, *sp);
                 else if(v == 2)
@@ -2056,7 +2235,10 @@ int group_phase(const sfx_group_dev* g, int phase, const sfx_solver_params* sp,
                     k_group_sfaces_slow<D, false, SFX_SOLVER_HLLC, true>
                             <<<kSlowGroupBlocks, kSlowBlock, 0, s>>>(g->tab, nm, *sp);
                 } else {
-                    if(v == 3)
+                    if(v == 4)
+                        k_group_sfaces<D, SFX_SOLVER_HLLC, 5, false, false, true>
+                                <<<g->blocks[1], 256, 0, s>>>(g->tab, pre1, nm, *sp);
+                    else if(v == 3)
                         k_group_sfaces<D, SFX_SOLVER_HLLC, 5><<<g->blocks[1], 256, 0, s>>>(
                                 g->tab, pre1, nm, *sp);
                     else if(v == 1)
@@ -2137,11 +2319,13 @@ int sfx_split_export_dQ(const sfx_dmesh* m, void* stream) {
 int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant) {
     if(variant < 0 || variant >= SFX_FACE_VARIANTS) return 0;
     if(sp->kind == SFX_SOLVER_EXACT) {
-        /* the gamma = 5/3 forms (2: 64 registers, 3: 80) exist for that gamma only */
-        if(sp->gamma != 5. / 3. && variant >= 2) return variant - 2;
+        /* the gamma = 5/3 forms (2: 64 registers, 3: 80) exist for that gamma
+         * only; 4 (left cells staged) is the gamma = 5/3 form at that gamma
+         * and the generic one at others */
+        if(sp->gamma != 5. / 3. && (variant == 2 || variant == 3)) return variant - 2;
         return variant;
     }
-    return variant; /* HLLC: 3 is the 48-register kernel */
+    return variant; /* HLLC: 3 is the 48-register kernel, 4 that with staged left cells */
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {

@@ -90,8 +90,9 @@ def test_tune_picks_a_variant_and_stays_within_tolerance(cuda_ok):
 @pytest.mark.parametrize("dim,solver", [(2, "Exact"), (3, "Exact"), (3, "HLLC")])
 def test_face_variants_give_the_same_result(cuda_ok, dim, solver):
     """variants 0 and 1 of the face kernel differ only in their register cap:
-    the same result bit for bit, and so do 2 and 3 for the exact solver
-    (HLLC: 3 is the 48-register kernel, bitwise 0 too); variant 2 (HLLC: the prediction's dW/dt from the
+    the same result bit for bit, and so do 2, 3 and 4 (left cells staged in
+    shared memory by bulk copies) for the exact solver (HLLC: 3 is the
+    48-register kernel and 4 that with staged cells, bitwise 0 too); variant 2 (HLLC: the prediction's dW/dt from the
     per-cell record; exact solver at gamma 5/3: fifth roots and integer
     powers) and the variant the face tuner keeps are within the split pass's
     round-off of 0"""
@@ -101,14 +102,14 @@ def test_face_variants_give_the_same_result(cuda_ok, dim, solver):
     probs = _problems(dim, solver, sizes)
     ctx = Context(dim, RiemannSolverFactory.generate(solver), 1)
     results = {}
-    for v in (0, 1, 2, 3, "tuned"):
+    for v in (0, 1, 2, 3, 4, "tuned"):
         members = [FluxPass(ctx, pr.mesh) for pr in probs]
         for fp, pr in zip(members, probs):
             fp.set_primitive(pr.W0)
         g = Group(ctx, members, [pr.dt for pr in probs])
         if v == "tuned":
             Q0 = [fp.state()[1] for fp in members]
-            assert g.tune_faces(2) in (0, 1, 2, 3)
+            assert g.tune_faces(2) in (0, 1, 2, 3, 4)
             for fp, q in zip(members, Q0):          # tuning reads the states only
                 assert np.array_equal(fp.state()[1], q)
         else:
@@ -120,11 +121,12 @@ def test_face_variants_give_the_same_result(cuda_ok, dim, solver):
             fp.close()
     for a, b in zip(results[1], results[0]):
         np.testing.assert_array_equal(a, b)
-    for a, b in zip(results[3], results[2 if solver == "Exact" else 0]):
-        np.testing.assert_array_equal(a, b)
+    for v in (3, 4):       # the same arithmetic as 2 (exact) or 0 (HLLC)
+        for a, b in zip(results[v], results[2 if solver == "Exact" else 0]):
+            np.testing.assert_array_equal(a, b)
     for v in (2, "tuned"):
         for a, b in zip(results[v], results[0]):
             err = np.abs(a - b).sum(0) / np.abs(b).sum(0)
             assert np.all(err[[0, -1]] <= 1e-6), err
     with pytest.raises(SfxError):
-        Group(ctx, [FluxPass(ctx, probs[0].mesh)], [probs[0].dt]).set_face_variant(4)
+        Group(ctx, [FluxPass(ctx, probs[0].mesh)], [probs[0].dt]).set_face_variant(5)
