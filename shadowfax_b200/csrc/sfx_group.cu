@@ -198,9 +198,9 @@ extern "C" int sfx_group_step(sfx_group* g, int32_t nsteps, int32_t use_graph,
         if(!rc) {
             int per_step = g->d_steps ? 1 : 0;
             for(int p = 0; p < 3; ++p) per_step += g->dev.blocks[p] > 0;
-            /* the queued exact-solver faces */
-            if(sfx_ctx_params(g->ctx)->kind == SFX_SOLVER_EXACT && g->dev.blocks[1] > 0)
-                per_step += 1;
+            /* the queued faces (both solvers: the exact solver's refused
+             * faces, HLLC's non-finite FP32 fluxes) */
+            if(g->dev.blocks[1] > 0) per_step += 1;
             sfx_count_launches(per_step * nsteps);
         }
     } else {
