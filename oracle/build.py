@@ -13,6 +13,11 @@
   (refharness/pow_interpose.c).
 * ``oracle/_ref/refharness_{2,3}d_moving_{libm,sfxpow}`` - the same sources
   built without -DSTATIC (moving generators: VorFace::set_v and the drift).
+* ``oracle/_ref/tessharness_{2,3}d_{libm,sfxpow}`` - the reference's own
+  tessellation (DelTess, VorTess, the exact predicates of ExArith with the
+  fixed-width integer stand-in in refharness/shim/boost, the particle tree)
+  and the same hot path, with oracle/refharness/tessharness.cpp: tessellate,
+  export the face list, run the step loop on that tessellation.
 
 Nothing here is linked into or called by the product library.
 """
@@ -36,6 +41,12 @@ REF_UNITS = [
     "riemann/HLLCRiemannSolver.cpp", "VorFace.cpp", "VorCell.cpp", "VorGen.cpp",
     "utilities/GasParticle.cpp", "utilities/Particle.cpp", "utilities/Timer.cpp",
     "utilities/HelperFunctions.cpp", "utilities/Hilbert.cpp", "ColorMap.cpp", "MPIGlobal.cpp", "ProgramLog.cpp", "RestartFile.cpp",
+]
+# the reference's tessellation and what it links (the static build only)
+TESS_UNITS = [
+    "DelTess.cpp", "DelTess_mpi.cpp", "ExArith.cpp", "VorTess.cpp", "Simplex.cpp",
+    "NgbSearch.cpp", "Line.cpp", "Plane.cpp", "RectangularBox.cpp", "utilities/Tree.cpp",
+    "utilities/EwaldTable.cpp", "utilities/DMParticle.cpp", "utilities/StarParticle.cpp",
 ]
 # the reference's release flags plus: no FMA contraction (matches x86-64 default
 # code generation on every host), no builtin pow folding (so the sfxpow build
@@ -66,6 +77,10 @@ def ref_binary(dim: int, pow_kind: str, moving: bool = False) -> Path:
     return OUT / f"refharness_{dim}d{'_moving' if moving else ''}_{pow_kind}"
 
 
+def tess_binary(dim: int, pow_kind: str) -> Path:
+    return OUT / f"tessharness_{dim}d_{pow_kind}"
+
+
 def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
     """Compile the reference harness binaries; returns [] if the reference
     tree is absent (the prebuilt binaries are used instead)."""
@@ -77,11 +92,15 @@ def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
     inc = ["-I", str(HERE / "refharness" / "shim"), "-I", str(HERE / "refharness"),
            "-I", str(REF_SRC), "-I", str(REF_SRC / "utilities")]
     harness = HERE / "refharness" / "harness.cpp"
+    tessh = HERE / "refharness" / "tessharness.cpp"
     interpose = HERE / "refharness" / "pow_interpose.c"
     outs = [ref_binary(d, k, mv) for d in (2, 3) for k in ("libm", "sfxpow")
             for mv in (False, True)]
-    deps = [harness, interpose, HERE / "refharness" / "shim" / "mpi.h", Path(__file__),
-            HERE.parent / "shadowfax_b200" / "csrc" / "sfx_pow.h"]
+    outs += [tess_binary(d, k) for d in (2, 3) for k in ("libm", "sfxpow")]
+    deps = [harness, tessh, interpose, HERE / "refharness" / "timeline_stub.hpp",
+            HERE / "refharness" / "shim" / "mpi.h",
+            HERE / "refharness" / "shim" / "boost" / "multiprecision" / "cpp_int.hpp",
+            Path(__file__), HERE.parent / "shadowfax_b200" / "csrc" / "sfx_pow.h"]
     if not force and all(_newer(o, deps) for o in outs):
         return outs
     tasks = []
@@ -93,6 +112,11 @@ def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
                               str(REF_SRC / u), "-o", str(o)])
             tasks.append(["g++", *REF_FLAGS, *vflags, f"-Dndim_={d}", *inc, "-c", str(harness),
                           "-o", str(obj / f"harness.{d}d{var}.o")])
+        for u in TESS_UNITS:
+            tasks.append(["g++", *REF_FLAGS, "-DSTATIC", f"-Dndim_={d}", *inc, "-c",
+                          str(REF_SRC / u), "-o", str(obj / (u.replace("/", "_") + f".{d}d.o"))])
+        tasks.append(["g++", *REF_FLAGS, "-DSTATIC", f"-Dndim_={d}", *inc, "-c", str(tessh),
+                      "-o", str(obj / f"tessharness.{d}d.o")])
     tasks.append(["gcc", "-O2", "-ffp-contract=off", "-std=c99", "-c", str(interpose), "-o",
                   str(obj / "pow_interpose.o")])
     with ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -107,6 +131,12 @@ def build_reference(force: bool = False, jobs: int = 8) -> list[Path]:
                 extra = [str(obj / "pow_interpose.o")] if k == "sfxpow" else []
                 subprocess.run(["g++", "-o", str(ref_binary(d, k, var == "_moving")), *objs,
                                 *extra, "-lm"], check=True)
+        tobjs = [str(obj / (u.replace("/", "_") + f".{d}d.o")) for u in REF_UNITS + TESS_UNITS]
+        tobjs.append(str(obj / f"tessharness.{d}d.o"))
+        for k in ("libm", "sfxpow"):
+            extra = [str(obj / "pow_interpose.o")] if k == "sfxpow" else []
+            subprocess.run(["g++", "-o", str(tess_binary(d, k)), *tobjs, *extra, "-lm"],
+                           check=True)
     return outs
 
 

@@ -9,7 +9,9 @@ shipped).
 * :func:`run_reference` runs the reference's own CPU flux pass (the unmodified
   Shadowfax sources, oracle/_ref/refharness_*) on a mesh and returns its
   final state; :func:`riemann_reference` evaluates the reference Riemann
-  solvers on state pairs.
+  solvers on state pairs; :func:`reference_tessellation` tessellates with the
+  reference's own DelTess/VorTess (oracle/_ref/tessharness_*), exports the
+  face list and can run the reference's step loop on that tessellation.
 """
 from __future__ import annotations
 
@@ -280,6 +282,71 @@ def run_reference(mesh, p: Params, dt: float, nsteps: int, W0: np.ndarray,
         out["vel"] = body[o:o + n * mesh.dim].reshape(n, mesh.dim).copy(); o += n * mesh.dim
     if moving:
         out["pos"] = body[o:o + n * mesh.dim].reshape(n, mesh.dim).copy()
+    return out
+
+
+def tess_binary(dim: int, pow_kind: str = "libm") -> Path:
+    return REF_DIR / f"tessharness_{dim}d_{pow_kind}"
+
+
+def reference_tessellation(pos: np.ndarray, periodic: bool, p: Params | None = None,
+                           dt: float = 0., nsteps: int = 0, W0: np.ndarray | None = None,
+                           pow_kind: str = "libm", tess_tolerance: float = 1e-9,
+                           timeout: float | None = None) -> dict:
+    """Tessellate generator positions in the unit box with the reference's own
+    DelTess/VorTess (oracle/refharness/tessharness.cpp) and export its face
+    list; cells come back in the reference's Hilbert order ("order": the
+    input index of each cell).  With W0 (input order) the reference's step
+    loop also runs nsteps on the objects VorTess built ("W", "Q", sorted
+    order).  Returns {"mesh": Mesh, "order", "status", "steps", "W", "Q"}."""
+    from shadowfax_b200.mesh import Mesh
+    pos = np.ascontiguousarray(pos, np.float64)
+    n, dim = pos.shape
+    exe = tess_binary(dim, pow_kind)
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} not built (oracle/build.py needs the reference tree)")
+    p = p or Params()
+    S = dim + 2
+    has_w = W0 is not None
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            np.array([dim, n, int(periodic), SOLVERS[p.solver], nsteps, int(has_w)],
+                     np.int32).tofile(f)
+            np.array([p.gamma, p.tolerance, p.cutoff, dt, tess_tolerance], np.float64).tofile(f)
+            pos.tofile(f)
+            if has_w:
+                np.ascontiguousarray(W0, np.float64).tofile(f)
+        subprocess.run([str(exe), fin, fout], check=True, timeout=timeout,
+                       stdout=subprocess.DEVNULL)
+        raw = open(fout, "rb").read()
+    status, steps, nn, F, nnz = np.frombuffer(raw, np.int32, 5)
+    o = 20
+
+    def take(dtype, count, shape=None):
+        nonlocal o
+        a = np.frombuffer(raw, dtype, count, o).copy()
+        o += a.nbytes
+        return a.reshape(shape) if shape else a
+
+    order = take(np.int32, n)
+    mesh = Mesh(dim=dim, periodic=bool(periodic),
+                cell_pos=take(np.float64, n * dim, (n, dim)),
+                cell_centroid=take(np.float64, n * dim, (n, dim)),
+                cell_volume=take(np.float64, n),
+                cell_total_area=take(np.float64, n),
+                cell_face_offset=take(np.int32, n + 1),
+                cell_face_index=take(np.int32, int(nnz)),
+                face_area=take(np.float64, int(F)),
+                face_midpoint=take(np.float64, int(F) * dim, (int(F), dim)),
+                face_left=take(np.int32, int(F)),
+                face_right=take(np.int32, int(F)),
+                face_kind=take(np.int32, int(F)),
+                face_right_pos=take(np.float64, int(F) * dim, (int(F), dim)))
+    out = dict(mesh=mesh, order=order, status=int(status), steps=int(steps))
+    if has_w:
+        out["W"] = take(np.float64, n * S, (n, S))
+        out["Q"] = take(np.float64, n * S, (n, S))
     return out
 
 

@@ -12,6 +12,9 @@ MOVING_CASES = [f"moving_{d}d_{b}_{s}" for d in (2, 3) for b in ("reflective", "
                 for s in ("exact", "hllc")]
 MOVING_FAILS = "moving_2d_periodic_hllc_fails"
 LOCAL_CASES = [f"local_{d}d_{s}" for d in (2, 3) for s in ("exact", "hllc")]
+# meshes the reference's own DelTess/VorTess built (tests/golden/make_reftess.py)
+REFTESS_CASES = ["reftess_sod2d_reflective_exact", "reftess_random2d_periodic_hllc",
+                 "reftess_sedov3d_reflective_hllc", "reftess_random3d_periodic_exact"]
 MESH_CASES = ["sod2d_exact", "sod2d_hllc", "sedov3d_hllc", "random3d_exact",
               "random2d_periodic_exact"]
 

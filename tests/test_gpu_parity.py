@@ -3,8 +3,8 @@ reference's own results: bit-identical in plain FP64."""
 import numpy as np
 import pytest
 
-from golden_util import MESH_CASES, TORO_HALF_STATES, assert_values_equal, load_case, \
-    load_riemann, toro_pairs
+from golden_util import MESH_CASES, REFTESS_CASES, TORO_HALF_STATES, assert_values_equal, \
+    load_case, load_riemann, toro_pairs
 from oracle.oracle import Params
 
 pytestmark = pytest.mark.gpu
@@ -75,10 +75,12 @@ def test_face_off_its_right_cell_bitwise_vs_oracle(cuda_ok, oracle, name):
     np.testing.assert_array_equal(br, ocode)
 
 
-@pytest.mark.parametrize("name", MESH_CASES)
+@pytest.mark.parametrize("name", MESH_CASES + REFTESS_CASES)
 def test_steps_bitwise_vs_reference(cuda_ok, name):
     """n steps on the GPU == the reference's CPU pass (sfx_pow build), bit for
-    bit; and within 1e-12 relative of the reference with glibc pow"""
+    bit; and within 1e-12 relative of the reference with glibc pow.  The
+    reftess cases are meshes the reference's own DelTess/VorTess built, and
+    their reference results come from its step loop on that tessellation"""
     mesh, meta, ref = load_case(name)
     ctx, fp = _pass(mesh, meta)
     st = fp.step(meta["dt"], meta["nsteps"])
