@@ -7,6 +7,7 @@
 
 #include <cstdio>
 #include <atomic>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <unordered_map>
@@ -366,8 +367,10 @@ int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
     int64_t cells = n * (8 * (2 * dim + 2 + 2 * S + dim * S) + 4) + 4;
     int64_t faces = F * (8 * (1 + 3 * dim + S) + 4 * 4);
     int64_t bytes = cells + faces + nnz * 4 + 8 * 8 * 1024 + 4096;
-    if(precision != SFX_PREC_SPLIT) /* the gradient terms, dQf inside them */
-        bytes += F * 8 * (sfx_grad_term_stride(dim) - S);
+    if(precision != SFX_PREC_SPLIT) /* the gradient terms, dQf inside them; the
+                                       update's CSR copy (cells not in ascending
+                                       face order) */
+        bytes += F * 8 * (sfx_grad_term_stride(dim) - S) + nnz * 4;
     if(precision == SFX_PREC_SPLIT) {
         /* fg, fi, fsh, an, dqm, dqv, queue; cw, cg, cx, self table; nbe */
         bytes += F * (32 + 8 + 1 + 8 * dim + 8 + 8 * dim) + 4 * slowq_capacity(F) + 4;
@@ -426,6 +429,28 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
      * its owner takes the negated flux of the twin, so mass and energy leave
      * one cell exactly as they enter the other. */
     std::vector<uint8_t> skip;
+    /* The reference adds each face's dQ to its cells in its face loop, in
+     * ascending face order (src/VorTessManager.cpp:198-212), while a cell's
+     * gradient walks the cell's own face list (src/VorCell.cpp:464-530).  A
+     * face list whose cells list their faces in ascending order (the
+     * builder's) serves both; otherwise the plain-FP64 update gets a copy of
+     * the CSR sorted per cell, so that its sums round as the reference's. */
+    std::vector<int32_t> aidx;
+    if(ctx->cfg.precision == SFX_PREC_FP64) {
+        bool ascending = true;
+        for(int64_t i = 0; i < n && ascending; ++i)
+            for(int64_t j = off[i] + 1; j < off[i + 1]; ++j)
+                if((idx[j] & 0x7fffffff) < (idx[j - 1] & 0x7fffffff)) {
+                    ascending = false;
+                    break;
+                }
+        if(!ascending) {
+            aidx = idx;
+            for(int64_t i = 0; i < n; ++i)
+                std::sort(aidx.begin() + off[i], aidx.begin() + off[i + 1],
+                          [](int32_t a, int32_t b) { return (a & 0x7fffffff) < (b & 0x7fffffff); });
+        }
+    }
     std::vector<int32_t> idx_split;
     if(ctx->cfg.precision == SFX_PREC_SPLIT) {
         skip.assign(F, 0);
@@ -516,6 +541,7 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     A(&d.tarea, n);
     A(&d.off, n + 1);
     A(&d.idx, nnz);
+    if(!aidx.empty()) A(&d.aidx, nnz);
     A(&d.W, n * S);
     A(&d.Q, n * S);
     A(&d.grad, n * dim * S);
@@ -573,6 +599,8 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     if(!rc) rc = h2d(d.tarea, desc->cell_total_area, n, s);
     if(!rc) rc = h2d(d.off, off, n + 1, s);
     if(!rc) rc = h2d(d.idx, split ? idx_split.data() : idx.data(), nnz, s);
+    if(!rc && !aidx.empty()) rc = h2d(d.aidx, aidx.data(), nnz, s);
+    if(aidx.empty()) d.aidx = d.idx;
     std::vector<int32_t> nbe;
     if(split) {
         /* the neighbour of each CSR entry, so the gradient kernel loads it

@@ -1277,8 +1277,10 @@ __global__ void __launch_bounds__(128) k_apply(sfx_dmesh m, double gamma) {
 #pragma unroll
     for(int k = 0; k < S; ++k) dQ[k] = 0.;
     const int beg = m.off[i], end = m.off[i + 1];
+    /* the cell's faces in ascending face order (aidx), the order in which
+     * the reference's face loop adds them */
     for(int j = beg; j < end; ++j) {
-        const unsigned e = (unsigned)m.idx[j];
+        const unsigned e = (unsigned)m.aidx[j];
         const int f = (int)(e & ~kRightBit);
         if(m.area[f] == 0.) continue;
         if(e & kRightBit) {

@@ -37,6 +37,9 @@ struct sfx_dmesh {
     double* tarea;  /* [n]       */
     int32_t* off;   /* [n+1]     */
     int32_t* idx;   /* [nnz] face id | (1u << 31 if the cell is the right) */
+    int32_t* aidx;  /* [nnz] the same entries in ascending face order per cell, the
+                       order the plain-FP64 update sums them in; == idx when every
+                       cell lists its faces that way */
     double* W;      /* [S][n]    */
     double* Q;      /* [S][n]    */
     double* grad;   /* [dim*S][n]: grad[(l*S + k)*n + i] = dW_k/dx_l       */
