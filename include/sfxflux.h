@@ -294,7 +294,7 @@ int sfx_mesh_set_lanes(sfx_mesh* mesh, int32_t lanes);
 #define SFX_FACE_VARIANTS 5
 int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
 
-/* ---- one mesh over several devices (plain FP64) ----
+/* ---- one mesh over several devices (plain FP64 and split) ----
  * Replaces the reference's MPI halo updates for the flux pass
  * (DelTess::update_Ws / update_gradients / update_dQs, src/DelTess_mpi.cpp:1614,
  * 1781, 2024): each device holds its owned cells, numbered first, then the
@@ -310,8 +310,10 @@ int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
  * records into the listed cells.  idx, out and in are device pointers;
  * stream NULL is the context's stream.  The lists are made once per
  * partition and are not checked on every call: an index outside the mesh
- * is skipped (never dereferenced).  SFX_ERR_UNSUPPORTED on a
- * split-precision mesh. */
+ * is skipped (never dereferenced).  A split-precision mesh packs its FP32
+ * states (exact in the doubles) and its FP64 mass, and its owned cells also
+ * receive exactly the values of a split pass over the whole mesh;
+ * SFX_ERR_UNSUPPORTED for a split clone. */
 int sfx_mesh_set_ranges(sfx_mesh* mesh, int32_t grad_cells, int32_t flux_faces,
                         int32_t update_cells);
 int sfx_mesh_pack_cells(sfx_mesh* mesh, const int32_t* idx, int32_t count, double* out,

@@ -146,6 +146,15 @@ int run_phase(sfx_mesh* m, int phase, double dt, int write_branch, cudaStream_t 
         g.moving = m->d.vel != nullptr ? 1 : 0; /* split meshes get face velocities
                                                    only from sfx_step_moving */
         sfx_split_blocks(m->d.dim, m->d.lanes, m->d.n_cells, m->d.n_faces, g.blocks);
+        if(m->d.ranged) {
+            /* one part of a mesh: the phases' own ranges */
+            int32_t b[3];
+            sfx_split_blocks(m->d.dim, m->d.lanes, sfx_grad_cells(m->d), sfx_flux_faces(m->d), b);
+            g.blocks[0] = b[0];
+            g.blocks[1] = b[1];
+            sfx_split_blocks(m->d.dim, m->d.lanes, sfx_update_cells(m->d), 0, b);
+            g.blocks[2] = b[0];
+        }
         return sfx_split_group_phase(&g, phase, &c->sp, s);
     }
     switch(phase) {
@@ -1044,7 +1053,8 @@ int sfx_mesh_set_face_variant(sfx_mesh* m, int32_t variant) {
 int sfx_mesh_set_ranges(sfx_mesh* m, int32_t grad_cells, int32_t flux_faces,
                         int32_t update_cells) {
     if(!m) return SFX_ERR_INVALID;
-    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    const bool split = m->ctx->cfg.precision == SFX_PREC_SPLIT;
+    if(split && m->clone) return SFX_ERR_UNSUPPORTED;
     sfx_dmesh& d = m->d;
     if(update_cells < 0 || update_cells > grad_cells || grad_cells > d.n_cells ||
        flux_faces < 0 || flux_faces > d.n_faces)
@@ -1053,13 +1063,17 @@ int sfx_mesh_set_ranges(sfx_mesh* m, int32_t grad_cells, int32_t flux_faces,
     d.r_grad = grad_cells;
     d.r_flux = flux_faces;
     d.r_upd = update_cells;
+    /* a split mesh's kernels read the ranges from its device table */
+    if(split) return setup_self(m, m->ctx->stream);
     return SFX_OK;
 }
 
 int sfx_mesh_pack_cells(sfx_mesh* m, const int32_t* idx, int32_t count, double* out,
                         void* stream) {
     if(!m || count < 0 || (count > 0 && (!idx || !out))) return SFX_ERR_INVALID;
-    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT)
+        return sfx_split_pack_cells(&m->d, idx, count, out,
+                                    stream ? stream : (void*)m->ctx->stream);
     return sfx_fp64_pack_cells(&m->d, idx, count, out,
                                stream ? stream : (void*)m->ctx->stream);
 }
@@ -1067,7 +1081,9 @@ int sfx_mesh_pack_cells(sfx_mesh* m, const int32_t* idx, int32_t count, double* 
 int sfx_mesh_unpack_cells(sfx_mesh* m, const int32_t* idx, int32_t count, const double* in,
                           void* stream) {
     if(!m || count < 0 || (count > 0 && (!idx || !in))) return SFX_ERR_INVALID;
-    if(m->ctx->cfg.precision == SFX_PREC_SPLIT) return SFX_ERR_UNSUPPORTED;
+    if(m->ctx->cfg.precision == SFX_PREC_SPLIT)
+        return sfx_split_unpack_cells(&m->d, idx, count, in,
+                                      stream ? stream : (void*)m->ctx->stream);
     return sfx_fp64_unpack_cells(&m->d, idx, count, in,
                                  stream ? stream : (void*)m->ctx->stream);
 }

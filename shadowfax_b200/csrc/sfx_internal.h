@@ -268,6 +268,12 @@ inline int sfx_default_lanes(int dim) {
 
 /* grouped launches (sfx_split.cu) */
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out);
+/* a part's ring exchange in the split pass (the plain-FP64 record layout:
+ * W, then the mass, per listed cell) */
+int sfx_split_pack_cells(const sfx_dmesh* m, const int32_t* idx, int count, double* out,
+                         void* stream);
+int sfx_split_unpack_cells(const sfx_dmesh* m, const int32_t* idx, int count, const double* in,
+                           void* stream);
 /* the face-kernel variant that variant `variant` runs for this solver (the
  * variants that do not apply to it run another one's kernel) */
 int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant);

@@ -267,6 +267,43 @@ __global__ void k_export_W(sfx_dmesh m) {
     for(int k = 0; k < S; ++k) m.W[(size_t)k * n + i] = c.W[k];
 }
 
+/* a part's ring exchange (split pass): per listed cell its FP32 state W (S
+ * values) and its FP64 mass Q[0], as S + 1 doubles, the record layout of the
+ * plain-FP64 pass; W goes through double and back exactly */
+template <int D>
+__global__ void k_pack_cells_split(sfx_dmesh m, const int32_t* idx, int count, double* out) {
+    constexpr int S = D + 2, R = S + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= (long long)count * R) return;
+    const int j = (int)(t / R), q = (int)(t % R);
+    const int c = idx[j];
+    if(c < 0 || c >= m.n_cells) return;
+    if(q < S) {
+        const Cell<D> cell = load_cell<D>(m.cw, c);
+        out[t] = cell.W[q];
+    } else {
+        out[t] = m.Q[c];
+    }
+}
+
+/* one thread per listed cell: the received W and mass into the cell's FP32
+ * record (total area kept) and its FP64 mass */
+template <int D>
+__global__ void k_unpack_cells_split(sfx_dmesh m, const int32_t* idx, int count,
+                                     const double* in) {
+    constexpr int S = D + 2, R = S + 1;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if(j >= count) return;
+    const int c = idx[j];
+    if(c < 0 || c >= m.n_cells) return;
+    float W[S];
+    for(int k = 0; k < S; ++k) W[k] = (float)in[(size_t)j * R + k];
+    const double mass = in[(size_t)j * R + S];
+    const Cell<D> cell = load_cell<D>(m.cw, c);
+    store_cell<D>(m.cw, c, W, (float)mass, cell.tarea);
+    m.Q[c] = mass;
+}
+
 template <int D>
 __global__ void k_export_dQ(sfx_dmesh m) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -328,7 +365,7 @@ __device__ __forceinline__ void sgrad_body(const sfx_dmesh& m, const float gamma
     /* whole warps stay alive for the shuffles; lanes past the end idle, and so
      * do the lanes of a cell that is not active (local time steps: it keeps
      * its gradients, src/Simulation.cpp:414-420) */
-    const bool live = i < m.n_cells && !failed(m.err) &&
+    const bool live = i < sfx_grad_cells(m) && !failed(m.err) &&
                       !(m.local && i < m.n_cells && m.tstart[i] != m.t_now);
     const int ic = live ? i : 0;
     const Cell<D> own = load_cell<D>(m.cw, ic);
@@ -1536,7 +1573,7 @@ __device__ __forceinline__ LeftTile<D> stage_left_cells(const sfx_dmesh& m, int 
     constexpr int G = GradVec4<D>::value, H = DwdtVec4<D>::value;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int lo = 0x7fffffff, hi = -1;
-    if(f < m.n_faces) lo = hi = __ldg(m.fi + f).x;
+    if(f < sfx_flux_faces(m)) lo = hi = __ldg(m.fi + f).x;
     lo = __reduce_min_sync(0xffffffffu, lo);
     hi = __reduce_max_sync(0xffffffffu, hi);
     if(lane == 0) {
@@ -1592,7 +1629,7 @@ __device__ __forceinline__ bool sfaces_body(const sfx_dmesh& m, const sfx_solver
                                             const float dt, const int f,
                                             const LeftTile<D>& tile = LeftTile<D>{}) {
     constexpr int S = D + 2;
-    if(f >= m.n_faces || failed(m.err)) return false;
+    if(f >= sfx_flux_faces(m) || failed(m.err)) return false;
     FaceWork<D> w;
     /* by default HLLC forms dW/dt itself and the exact solver's kernels read
      * it (STORED_DW: from the per-cell record) */
@@ -1825,7 +1862,7 @@ __device__ __forceinline__ void sapply_body(const sfx_dmesh& m, const double gam
                                             const int t) {
     constexpr int S = D + 2;
     const int i = t / LPC, lane = t % LPC;
-    const bool live = i < m.n_cells && !failed(m.err);
+    const bool live = i < sfx_update_cells(m) && !failed(m.err);
     const int n = m.n_cells, F = m.n_faces;
     double dQ[S];
 #pragma unroll
@@ -1966,7 +2003,7 @@ __global__ void __launch_bounds__(kExactBlock, MINB)
     }
     FaceWork<D> w;
     int cls = kClassNone;
-    if(f < m.n_faces && !failed(m.err) &&
+    if(f < sfx_flux_faces(m) && !failed(m.err) &&
        face_work<D, true, MOVING, TILE>(m, (float)sp.gamma, dt, f, w, tile))
         cls = wave_class<D>(sp, w);
     queue_faces(m, cls == kClassQueue, f);
@@ -2326,6 +2363,29 @@ int sfx_split_face_variant_kernel(const sfx_solver_params* sp, int variant) {
         return variant;
     }
     return variant; /* HLLC: 3 is the 48-register kernel, 4 that with staged left cells */
+}
+
+int sfx_split_pack_cells(const sfx_dmesh* m, const int32_t* idx, int count, double* out,
+                         void* stream) {
+    if(count <= 0) return SFX_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long t = (long long)count * (m->S + 1);
+    if(m->dim == 3)
+        k_pack_cells_split<3><<<grid_for(t, 256), 256, 0, s>>>(*m, idx, count, out);
+    else
+        k_pack_cells_split<2><<<grid_for(t, 256), 256, 0, s>>>(*m, idx, count, out);
+    return launched(1);
+}
+
+int sfx_split_unpack_cells(const sfx_dmesh* m, const int32_t* idx, int count, const double* in,
+                           void* stream) {
+    if(count <= 0) return SFX_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    if(m->dim == 3)
+        k_unpack_cells_split<3><<<grid_for(count, 256), 256, 0, s>>>(*m, idx, count, in);
+    else
+        k_unpack_cells_split<2><<<grid_for(count, 256), 256, 0, s>>>(*m, idx, count, in);
+    return launched(1);
 }
 
 int sfx_split_blocks(int dim, int lanes, int n_cells, int n_faces, int32_t* out) {

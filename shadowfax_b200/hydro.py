@@ -298,9 +298,10 @@ class FluxPass:
         return best
 
     def set_ranges(self, grad_cells: int, flux_faces: int, update_cells: int):
-        """one part of a mesh split over several devices (plain FP64):
-        gradients of cells [0, grad_cells), fluxes of faces [0, flux_faces),
-        update of cells [0, update_cells) (sfx_mesh_set_ranges)"""
+        """one part of a mesh split over several devices (plain FP64 or
+        split): gradients of cells [0, grad_cells), fluxes of faces
+        [0, flux_faces), update of cells [0, update_cells)
+        (sfx_mesh_set_ranges)"""
         L.check(L.lib().sfx_mesh_set_ranges(self.h, grad_cells, flux_faces, update_cells),
                 "sfx_mesh_set_ranges")
 

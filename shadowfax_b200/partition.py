@@ -214,7 +214,7 @@ def exchange_records(send: dict, recv: dict, group=None) -> None:
 
 class PartitionedPass:
     """This rank's part of one mesh split over the ranks of a process group
-    (plain FP64, one GPU per rank): the local mesh with its two rings on the
+    (plain FP64 or split, one GPU per rank): the local mesh with its two rings on the
     device, the pass restricted to it, and the ring exchange after every
     step.  The owned cells' W and Q equal those of a pass over the whole
     mesh, bit for bit.

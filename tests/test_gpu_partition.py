@@ -1,5 +1,6 @@
 """One mesh split into parts, all parts on one GPU in one process (plain
-FP64): each part's pass restricted to its ranges (sfx_mesh_set_ranges) and
+FP64 and the FP32/FP64 split): each part's pass restricted to its ranges
+(sfx_mesh_set_ranges) and
 the ring records moved between parts through device buffers
 (sfx_mesh_pack_cells / sfx_mesh_unpack_cells) give the owned cells the
 values of the pass over the whole mesh, bit for bit.  On several GPUs the
@@ -19,16 +20,17 @@ def _ctx(mesh, meta, precision=0):
                    precision)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name,nparts", [("sod2d_exact", 2), ("random2d_periodic_exact", 3),
                                          ("sedov3d_hllc", 2), ("random3d_exact", 3)])
-def test_parts_on_one_gpu_equal_the_whole_mesh(cuda_ok, name, nparts):
+def test_parts_on_one_gpu_equal_the_whole_mesh(cuda_ok, name, nparts, precision):
     import torch
 
     from shadowfax_b200 import partition as P
     from shadowfax_b200.hydro import FluxPass
     mesh, meta, _ = load_case(name)
     dt, nsteps = meta["dt"], 5
-    ctx = _ctx(mesh, meta)
+    ctx = _ctx(mesh, meta, precision)
     whole = FluxPass(ctx, mesh)
     whole.set_primitive(meta["W0"])
     whole.step(dt, nsteps)
