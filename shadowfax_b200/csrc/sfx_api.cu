@@ -431,13 +431,6 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
             }
         }
     }
-    /* Split pass only: a face across a periodic boundary is listed twice, once
-     * owned by each cell (the reference computes it twice and lets each copy
-     * update only its owner, src/VorFace.cpp:913-955).  The split pass
-     * computes such a pair once: the copy with the higher index is dropped and
-     * its owner takes the negated flux of the twin, so mass and energy leave
-     * one cell exactly as they enter the other. */
-    std::vector<uint8_t> skip;
     /* The reference adds each face's dQ to its cells in its face loop, in
      * ascending face order (src/VorTessManager.cpp:198-212), while a cell's
      * gradient walks the cell's own face list (src/VorCell.cpp:464-530).  A
@@ -460,6 +453,16 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
                           [](int32_t a, int32_t b) { return (a & 0x7fffffff) < (b & 0x7fffffff); });
         }
     }
+    /* Split pass only: a face across a periodic boundary is listed twice, once
+     * owned by each cell (the reference computes it twice and lets each copy
+     * update only its owner, src/VorFace.cpp:913-955).  The split pass
+     * computes such a pair once and the other copy's owner takes the negated
+     * flux, so mass and energy leave one cell exactly as they enter the other.
+     * The copy kept is chosen by geometry, not by face number: the one whose
+     * image shift has the smaller code.  Any numbering of the same faces --
+     * a part of the mesh (shadowfax_b200/partition.py) renumbers them -- then
+     * computes the same copy with the same rounding. */
+    std::vector<uint8_t> skip;
     std::vector<int32_t> idx_split;
     if(ctx->cfg.precision == SFX_PREC_SPLIT) {
         skip.assign(F, 0);
@@ -503,7 +506,10 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
                    f < g && twin[f] < 0) {
                     twin[f] = (int32_t)g;
                     twin[g] = (int32_t)f;
-                    skip[g] = 1;
+                    if(want > shcode(g)) /* f has the larger code */
+                        skip[f] = 1;
+                    else
+                        skip[g] = 1;
                     break;
                 }
             }

@@ -119,6 +119,30 @@ def _csr_faces(mesh: Mesh, mask: np.ndarray) -> np.ndarray:
     return np.unique(mesh.cell_face_index[sel])
 
 
+def _periodic_twins(mesh: Mesh) -> np.ndarray:
+    """for each face across a periodic boundary, the other cell's copy of it
+    (left and right swapped, image shifted the other way); -1 elsewhere"""
+    twin = np.full(mesh.n_faces, -1, np.int64)
+    per = np.flatnonzero(mesh.face_kind == KIND_PERIODIC)
+    if per.size == 0:
+        return twin
+    L, R = mesh.face_left[per], mesh.face_right[per]
+    shift = np.rint(mesh.face_right_pos[per] - mesh.cell_pos[R]).astype(np.int64)
+    seen = {}
+    for k, f in enumerate(per):
+        seen[(int(L[k]), int(R[k]), tuple(shift[k]))] = f
+    for k, f in enumerate(per):
+        g = seen.get((int(R[k]), int(L[k]), tuple(-shift[k])))
+        if g is not None:
+            twin[f] = g
+    return twin
+
+
+def _with_twins(faces: np.ndarray, twin: np.ndarray) -> np.ndarray:
+    t = twin[faces]
+    return np.union1d(faces, t[t >= 0])
+
+
 def _rings(mesh: Mesh, owner: np.ndarray, rank: int):
     """masks of the owned, ring-1 and ring-2 cells of a rank"""
     own = owner == rank
@@ -133,8 +157,12 @@ def build_part(mesh: Mesh, owner: np.ndarray, rank: int) -> Part:
     n_own, n_grad = int(own.sum()), int(own.sum() + r1.sum())
     g2l = np.full(mesh.n_cells, -1, np.int64)
     g2l[cells] = np.arange(len(cells))
-    flux = _csr_faces(mesh, own)
-    need = _csr_faces(mesh, own | r1)
+    # the split pass computes one copy of each periodic face pair (chosen by
+    # its geometry) for both cells: a part holds both copies of every pair
+    # at its owned and ring-1 cells, the pairs at owned cells in the flux range
+    twin = _periodic_twins(mesh)
+    flux = _with_twins(_csr_faces(mesh, own), twin)
+    need = _with_twins(_csr_faces(mesh, own | r1), twin)
     faces = np.concatenate([flux, np.setdiff1d(need, flux, assume_unique=True)])
     f2l = np.full(mesh.n_faces, -1, np.int64)
     f2l[faces] = np.arange(len(faces))

@@ -36,9 +36,22 @@ def _check_part(mesh, owner, pt):
         g = pt.cells[c]
         assert np.array_equal(pt.faces[loc.cell_face_index[off[c]:off[c + 1]]],
                               mesh.cell_face_index[goff[g]:goff[g + 1]])
-    # faces [0, n_flux): exactly the faces of owned cells
+    # faces [0, n_flux): exactly the faces of owned cells and the other
+    # copies of their periodic faces (the split pass computes one copy of a
+    # pair for both cells)
     sel = np.repeat(own, np.diff(goff))
-    assert np.array_equal(np.sort(pt.faces[:pt.n_flux]), np.unique(mesh.cell_face_index[sel]))
+    mine = np.unique(mesh.cell_face_index[sel])
+    twin = P._periodic_twins(mesh)
+    want = np.union1d(mine, twin[mine][twin[mine] >= 0])
+    assert np.array_equal(np.sort(pt.faces[:pt.n_flux]), want)
+    # every periodic face of an owned or ring-1 cell has its twin in the part
+    part_faces = set(pt.faces.tolist())
+    for f in pt.faces:
+        if twin[f] >= 0 and (pt.cells[:pt.n_grad] == mesh.face_left[f]).any():
+            assert int(twin[f]) in part_faces
+    if mesh.periodic:
+        assert (twin >= 0).sum() == (mesh.face_kind == P.KIND_PERIODIC).sum()
+        assert np.all(twin[twin[twin >= 0]] == np.flatnonzero(twin >= 0))
     assert np.all(loc.face_left >= 0) and np.all(loc.face_left < loc.n_cells)
     real = loc.face_kind != P.KIND_MIRROR
     assert np.all(loc.face_right[real] >= 0) and np.all(loc.face_right[real] < loc.n_cells)
