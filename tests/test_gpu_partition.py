@@ -88,5 +88,7 @@ def test_ranges_are_checked(cuda_ok):
             fp.set_ranges(*bad)
     fp.set_ranges(n, F, n)          # the whole mesh: the unrestricted pass
     fp2 = FluxPass(_ctx(mesh, meta, precision=1), mesh)
+    twin = fp2.clone()
     with pytest.raises(SfxError):
-        fp2.set_ranges(n, F, n)     # plain FP64 only
+        twin.set_ranges(n, F, n)    # not a split clone: it shares the owner's tables
+    fp2.set_ranges(n, F, n)         # the split pass takes ranges
