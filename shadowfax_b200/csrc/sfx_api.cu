@@ -456,12 +456,15 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     /* Split pass only: a face across a periodic boundary is listed twice, once
      * owned by each cell (the reference computes it twice and lets each copy
      * update only its owner, src/VorFace.cpp:913-955).  The split pass
-     * computes such a pair once and the other copy's owner takes the negated
-     * flux, so mass and energy leave one cell exactly as they enter the other.
-     * The copy kept is chosen by geometry, not by face number: the one whose
-     * image shift has the smaller code.  Any numbering of the same faces --
-     * a part of the mesh (shadowfax_b200/partition.py) renumbers them -- then
-     * computes the same copy with the same rounding. */
+     * applies one copy's flux to both cells: the other copy's owner takes its
+     * negated flux (the CSR entry names the kept copy with the right-side
+     * bit), so mass and energy leave one cell exactly as they enter the other.
+     * Both copies are still solved; the dropped copy's flux reaches no cell
+     * and only the per-face export reads it.  The copy kept is chosen by
+     * geometry, not by face number: the one whose image shift has the smaller
+     * code.  Any numbering of the same faces -- a part of the mesh
+     * (shadowfax_b200/partition.py) renumbers them -- then applies the same
+     * copy with the same rounding. */
     std::vector<uint8_t> skip;
     std::vector<int32_t> idx_split;
     if(ctx->cfg.precision == SFX_PREC_SPLIT) {
@@ -629,7 +632,6 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
         }
         if(!rc) rc = h2d(d.nbe, nbe.data(), nnz, s);
     }
-    if(!rc && split) rc = h2d(d.fsh, skip.data(), F, s);
     if(!rc) rc = h2d(d.area, desc->face_area, F, s);
     if(!rc) rc = h2d(d.mid, t3.data(), t3.size(), s);
     if(!rc) rc = h2d(d.left, desc->face_left, F, s);

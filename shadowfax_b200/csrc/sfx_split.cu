@@ -205,10 +205,7 @@ __global__ void k_prep_faces(sfx_dmesh m) {
     for(int l = 0; l < D; ++l) rn2 += r[l] * r[l];
     const double rn64 = sqrt(rn2);
     for(int l = 0; l < D; ++l) m.an[(size_t)l * F + f] = m.area[f] * (-r[l] / rn64);
-    /* a periodic copy whose twin carries the flux (marked by the host in
-     * fsh bit 7) is switched off by a zero area */
-    const bool twin_skip = m.fsh[f] & 0x80;
-    const float A = twin_skip ? 0.f : (float)m.area[f];
+    const float A = (float)m.area[f];
     const float rn = (float)rn64;
     if(D == 3) {
         m.fg[2 * f] = make_float4(A, (float)c[0], (float)c[1], (float)c[2]);

@@ -157,8 +157,8 @@ def build_part(mesh: Mesh, owner: np.ndarray, rank: int) -> Part:
     n_own, n_grad = int(own.sum()), int(own.sum() + r1.sum())
     g2l = np.full(mesh.n_cells, -1, np.int64)
     g2l[cells] = np.arange(len(cells))
-    # the split pass computes one copy of each periodic face pair (chosen by
-    # its geometry) for both cells: a part holds both copies of every pair
+    # the split pass applies one copy of each periodic face pair (chosen by
+    # its geometry) to both cells: a part holds both copies of every pair
     # at its owned and ring-1 cells, the pairs at owned cells in the flux range
     twin = _periodic_twins(mesh)
     flux = _with_twins(_csr_faces(mesh, own), twin)

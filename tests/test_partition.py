@@ -37,8 +37,8 @@ def _check_part(mesh, owner, pt):
         assert np.array_equal(pt.faces[loc.cell_face_index[off[c]:off[c + 1]]],
                               mesh.cell_face_index[goff[g]:goff[g + 1]])
     # faces [0, n_flux): exactly the faces of owned cells and the other
-    # copies of their periodic faces (the split pass computes one copy of a
-    # pair for both cells)
+    # copies of their periodic faces (the split pass applies one copy of a
+    # pair to both cells)
     sel = np.repeat(own, np.diff(goff))
     mine = np.unique(mesh.cell_face_index[sel])
     twin = P._periodic_twins(mesh)
