@@ -312,8 +312,11 @@ int sfx_mesh_set_face_variant(sfx_mesh* mesh, int32_t variant);
  * partition and are not checked on every call: an index outside the mesh
  * is skipped (never dereferenced).  A split-precision mesh packs its FP32
  * states (exact in the doubles) and its FP64 mass, and its owned cells also
- * receive exactly the values of a split pass over the whole mesh;
- * SFX_ERR_UNSUPPORTED for a split clone. */
+ * receive exactly the values of a split pass over the whole mesh when the
+ * part also holds the other copy of every periodic face of its first two
+ * groups, those of owned cells inside [0, flux_faces): the split pass applies
+ * one copy of a periodic pair to both cells, the copy whose image shift has
+ * the smaller code; SFX_ERR_UNSUPPORTED for a split clone. */
 int sfx_mesh_set_ranges(sfx_mesh* mesh, int32_t grad_cells, int32_t flux_faces,
                         int32_t update_cells);
 int sfx_mesh_pack_cells(sfx_mesh* mesh, const int32_t* idx, int32_t count, double* out,
