@@ -93,6 +93,7 @@ struct PoolMesh {
 
 /* kernel settings of a class's launch group (sfx_server_set_tuning) */
 struct Tuning {
+    int32_t dim = 2;
     int32_t lanes = 0; /* 0: the library's default */
     int32_t face_variant = 0;
 };
@@ -105,6 +106,7 @@ struct Class {
     int reused = 0; /* rounds the current membership has run */
     std::atomic<int> tune_gen{0}; /* bumped by sfx_server_set_tuning */
     int applied_gen = 0;          /* worker thread: the tuning the group has */
+    int applied_lanes = 0;        /* worker thread: lanes the group runs, 0: its default */
     Tuning tune;                  /* under sfx_server::mu */
 };
 
@@ -389,7 +391,12 @@ int apply_tuning(sfx_server* s, Class& c) {
         std::lock_guard<std::mutex> lk(s->mu);
         t = c.tune;
     }
-    int rc = t.lanes ? sfx_group_set_lanes(c.group, t.lanes) : SFX_OK;
+    int rc = SFX_OK;
+    if(t.lanes != c.applied_lanes) {
+        /* 0 takes a group tuned before back to the library's default */
+        rc = sfx_group_set_lanes(c.group, t.lanes ? t.lanes : sfx_default_lanes(t.dim));
+        if(!rc) c.applied_lanes = t.lanes;
+    }
     if(!rc) rc = sfx_group_set_face_variant(c.group, t.face_variant);
     c.applied_gen = gen;
     c.reused = 0; /* the captured graph holds the old kernels */
@@ -415,6 +422,7 @@ int rebuild_group(sfx_server* s, Class& c) {
     int rc = sfx_group_create(c.ctx, n, ms.data(), dts.data(), &c.group);
     if(!rc) rc = sfx_group_set_steps(c.group, steps.data());
     c.applied_gen = 0;
+    c.applied_lanes = 0; /* a new group runs the default lanes */
     if(!rc && c.tune_gen.load() != 0) {
         c.applied_gen = -1; /* a new group: apply whatever tuning there is */
         rc = apply_tuning(s, c);
@@ -634,6 +642,7 @@ extern "C" int sfx_server_set_tuning(sfx_server* s, int32_t dim, int32_t solver,
     Class& c = s->cls[dim - 2][solver];
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        c.tune.dim = dim;
         c.tune.lanes = lanes;
         c.tune.face_variant = face_variant;
     }
