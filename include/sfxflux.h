@@ -171,7 +171,10 @@ int sfx_ctx_synchronize(sfx_ctx* ctx);
 
 /* ---- mesh: upload the face list once per tessellation ----
  * (VorTess::construct output, src/VorTess.cpp:153-396).  The caller keeps
- * ownership of the host arrays and may free them after return. */
+ * ownership of the host arrays and may free them after return.  A split
+ * context takes periodic meshes of the unit box only (a periodic image
+ * offset of 0 or +-1 on every axis, to 1e-9): SFX_ERR_UNSUPPORTED for
+ * others; the plain-FP64 pass takes any box. */
 int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out);
 int sfx_mesh_free(sfx_mesh* mesh);
 /* bytes of device memory a mesh of this size needs (admission control) */

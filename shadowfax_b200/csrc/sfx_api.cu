@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <atomic>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <unordered_map>
@@ -468,6 +469,17 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     std::vector<uint8_t> skip;
     std::vector<int32_t> idx_split;
     if(ctx->cfg.precision == SFX_PREC_SPLIT) {
+        /* the split kernels apply a periodic image's offset as one whole unit
+         * box per axis (a code per axis: 0, +1 or -1); a mesh of another box
+         * is refused rather than computed with the wrong offset */
+        for(int64_t f = 0; f < F; ++f) {
+            if(desc->face_kind[f] != SFX_FACE_PERIODIC) continue;
+            for(int l = 0; l < dim; ++l) {
+                const double a = std::fabs(desc->face_right_pos[f * dim + l] -
+                                           desc->cell_pos[(int64_t)desc->face_right[f] * dim + l]);
+                if(!(a <= 1e-9 || std::fabs(a - 1.) <= 1e-9)) return SFX_ERR_UNSUPPORTED;
+            }
+        }
         skip.assign(F, 0);
         idx_split = idx;
         auto shcode = [&](int64_t f) {

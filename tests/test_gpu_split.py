@@ -105,3 +105,27 @@ def test_split_on_reference_tessellation(cuda_ok, name):
     err = l1_rel(Q32, ref["ref_sfxpow_Q"])
     assert np.all(err <= TOL_L1), err
     assert abs(t1[0] - t0[0]) <= 1e-12 * abs(t0[0])
+
+
+def test_split_refuses_periodic_meshes_of_another_box(cuda_ok):
+    """the split kernels apply a periodic image offset as +-1 per axis: a
+    periodic mesh of a box of side 2 is refused by a split context and taken
+    by the plain-FP64 one; the same mesh in the unit box is taken by both"""
+    import dataclasses
+    from golden_util import load_case
+    from shadowfax_b200._lib import SfxError, SFX_ERR_UNSUPPORTED
+    from shadowfax_b200.hydro import Context, FluxPass, RiemannSolverFactory
+    mesh, meta, _ = load_case("random2d_periodic_exact")
+    D = mesh.dim
+    big = dataclasses.replace(
+        mesh, cell_pos=mesh.cell_pos * 2., cell_centroid=mesh.cell_centroid * 2.,
+        cell_volume=mesh.cell_volume * 2. ** D, cell_total_area=mesh.cell_total_area * 2. ** (D - 1),
+        face_area=mesh.face_area * 2. ** (D - 1), face_midpoint=mesh.face_midpoint * 2.,
+        face_right_pos=mesh.face_right_pos * 2.)
+    solver = RiemannSolverFactory.generate(meta["solver"], meta["gamma"])
+    for precision in (0, 1):
+        FluxPass(Context(D, solver, precision), mesh)
+    FluxPass(Context(D, solver, 0), big)
+    with pytest.raises(SfxError) as e:
+        FluxPass(Context(D, solver, 1), big)
+    assert e.value.status == SFX_ERR_UNSUPPORTED
