@@ -1119,7 +1119,7 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return
     if args.workload == "serve":
-        return run_reference_serve(args)
+        return run_reference_serve(args, world)
     pr = build_problem(args)
     # a bounded sample: 5 steps, or up to 3e6 face-steps on a small mesh
     steps = max(1, min(args.steps, max(5, int(3e6 // pr.mesh.n_active_faces))))
@@ -1141,13 +1141,15 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def run_reference_serve(args):
+def run_reference_serve(args, world=1):
     """--impl reference on the request stream: the reference CPU pass
     (oracle/_ref, the unmodified Shadowfax sources) on the host cores, one
     process per request for the stream's first P requests, each process
     --warmup untimed and --steps timed steps (a bounded sample: the reference
     has no request loop).  The meshes are made by the standalone sfx_meshgen
-    program and read with numpy, so this process never loads the GPU library."""
+    program and read with numpy, so this process never loads the GPU library.
+    Launched on N ranks, rank 0 alone runs it and its line carries N and the
+    config the GPU arm prints at N."""
     from oracle.oracle import ref_binary
     from shadowfax_b200 import workloads as wl
     if not (ref_binary(2, "libm").exists() and ref_binary(3, "libm").exists()):
@@ -1161,12 +1163,12 @@ def run_reference_serve(args):
                              library=False)
         cb = serve_cpu_sample(pool, reqs, args.steps, args.warmup)
     faces = sum(pool.meshes[r.mesh].n_active_faces for r in reqs[:P])
-    line = {"metric": METRIC_SERVE, "value": cb["value"], "unit": UNIT, "n_gpus": 1,
+    line = {"metric": METRIC_SERVE, "value": cb["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * faces / cb["value"],
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": serve_config(args, reqs, 1),
+            "config": serve_config(args, reqs, world),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -1180,17 +1182,16 @@ def run_reference_serve(args):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.impl == "reference":
+        # rank 0's host cores alone; the other ranks exit at once, so no
+        # process group (and no timeout while rank 0 runs its sample)
+        run_reference_arm(args, rank, world)
+        return
     import torch
     import torch.distributed as dist
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
     torch.cuda.set_device(local)
     if args.workload in ("batch2d", "serve"):
         fn = bench_batch if args.workload == "batch2d" else bench_serve
