@@ -4,6 +4,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import pytest
+
 ROOT = Path(__file__).resolve().parent.parent
 
 
@@ -76,3 +78,40 @@ def test_variant_counts_match_the_header():
 def test_server_tuning_rejects_bad_arguments_without_a_server():
     from shadowfax_b200 import _lib as L
     assert L.lib().sfx_server_set_tuning(None, 2, 0, 0, 0) == L.SFX_ERR_INVALID
+
+
+# entry points whose first argument is an object handle: a NULL handle is
+# refused before any device call (sfx_mesh_clone_bytes answers -1)
+NULL_HANDLE_ENTRY_POINTS = [
+    "sfx_ctx_destroy", "sfx_ctx_set_stream", "sfx_ctx_synchronize", "sfx_mesh_upload",
+    "sfx_mesh_free", "sfx_state_download", "sfx_step", "sfx_step_moving",
+    "sfx_mesh_set_timesteps", "sfx_mesh_get_timesteps", "sfx_mesh_set_gradients",
+    "sfx_mesh_get_gradients", "sfx_step_window", "sfx_timestep_bins", "sfx_step_timed",
+    "sfx_flux_pass", "sfx_riemann_eval", "sfx_mesh_clone", "sfx_mesh_clone_bytes",
+    "sfx_mesh_set_lanes", "sfx_mesh_set_face_variant", "sfx_mesh_set_ranges",
+    "sfx_mesh_pack_cells", "sfx_mesh_unpack_cells", "sfx_mesh_totals",
+    "sfx_group_create", "sfx_group_set_dt", "sfx_group_set_face_variant", "sfx_group_set_lanes",
+    "sfx_group_step", "sfx_group_step_timed", "sfx_group_status", "sfx_group_tune",
+    "sfx_group_tune_faces", "sfx_group_set_steps", "sfx_group_get_steps", "sfx_group_free",
+    "sfx_server_add_mesh", "sfx_server_submit", "sfx_server_poll", "sfx_server_drain",
+    "sfx_server_stats_get", "sfx_server_shutdown", "sfx_server_set_tuning",
+]
+
+
+def _plausible(argtype):
+    """a value of the argument's type that is valid on its own"""
+    if argtype in (ctypes.c_double, ctypes.c_float):
+        return 1.0
+    if argtype in (ctypes.c_int, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
+                   ctypes.c_uint64):
+        return 1
+    return None  # pointers and handles
+
+
+@pytest.mark.parametrize("name", NULL_HANDLE_ENTRY_POINTS)
+def test_null_handles_are_refused_without_a_gpu(name):
+    from shadowfax_b200 import _lib as L
+    res, argtypes = L.PROTOTYPES[name]
+    fn = getattr(L.lib(), name)
+    rc = fn(*[_plausible(a) for a in argtypes])
+    assert rc == (-1 if name == "sfx_mesh_clone_bytes" else L.SFX_ERR_INVALID), rc
