@@ -115,3 +115,33 @@ def test_null_handles_are_refused_without_a_gpu(name):
     fn = getattr(L.lib(), name)
     rc = fn(*[_plausible(a) for a in argtypes])
     assert rc == (-1 if name == "sfx_mesh_clone_bytes" else L.SFX_ERR_INVALID), rc
+
+
+def test_noalloc_pass_checks_its_arguments_before_any_device_call():
+    """sfx_flux_pass_noalloc refuses a bad call before it asks the runtime for
+    a device: these cases never reach the (here absent) GPU, and the host
+    arrays standing in for device pointers are never read"""
+    from shadowfax_b200 import _lib as L
+    buf = ctypes.create_string_buffer(64)
+    p = ctypes.cast(buf, ctypes.c_void_p)
+
+    def mesh(**kw):
+        d = dict(dim=2, n_cells=100, n_faces=300)
+        d.update(kw)
+        m = L.sfx_device_mesh(d["dim"], d["n_cells"], d["n_faces"], *([p] * 12))
+        return m
+
+    def call(m, cfg, dt=1e-4, W=p):
+        return L.lib().sfx_flux_pass_noalloc(ctypes.byref(m), ctypes.byref(cfg), dt, W, p, p, None)
+
+    limit = int(re.search(r"#define SFX_NOALLOC_MAX_CELLS (\d+)",
+                          (ROOT / "include" / "sfxflux.h").read_text()).group(1))
+    cfg = L.sfx_config(2, 0, 5 / 3, 1e-8, -5.0, 0, 0)
+    assert call(mesh(n_cells=limit + 1), cfg) == L.SFX_ERR_TOO_LARGE
+    assert call(mesh(dim=4), cfg) == L.SFX_ERR_INVALID
+    assert call(mesh(), L.sfx_config(3, 0, 5 / 3, 1e-8, -5.0, 0, 0)) == L.SFX_ERR_INVALID
+    assert call(mesh(), L.sfx_config(2, 7, 5 / 3, 1e-8, -5.0, 0, 0)) == L.SFX_ERR_UNSUPPORTED
+    assert call(mesh(), L.sfx_config(2, 0, 1.0, 1e-8, -5.0, 0, 0)) == L.SFX_ERR_INVALID
+    assert call(mesh(), cfg, dt=0.0) == L.SFX_ERR_INVALID
+    assert call(mesh(), cfg, W=None) == L.SFX_ERR_INVALID
+    assert call(mesh(n_cells=0), cfg) == L.SFX_ERR_INVALID
