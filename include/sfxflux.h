@@ -176,6 +176,14 @@ int sfx_ctx_synchronize(sfx_ctx* ctx);
  * offset of 0 or +-1 on every axis, to 1e-9): SFX_ERR_UNSUPPORTED for
  * others; the plain-FP64 pass takes any box. */
 int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out);
+/* the checks sfx_mesh_upload makes of a face list before it allocates, on the
+ * host alone (no context, no device): SFX_OK or the status the upload to a
+ * context of this precision would return -- SFX_ERR_INVALID for missing
+ * arrays or sizes, SFX_ERR_BOUNDS for an index out of range or a cell listing
+ * a face it is not on, SFX_ERR_UNSUPPORTED for a periodic mesh outside the
+ * unit box in SFX_PREC_SPLIT.  For checking an exporter's output where no
+ * GPU is. */
+int sfx_mesh_check(const sfx_mesh_desc* desc, int32_t precision);
 int sfx_mesh_free(sfx_mesh* mesh);
 /* bytes of device memory a mesh of this size needs (admission control) */
 int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,

@@ -113,6 +113,7 @@ PROTOTYPES = {
     "sfx_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sfx_ctx_synchronize": (C.c_int, [C.c_void_p]),
     "sfx_mesh_upload": (C.c_int, [C.c_void_p, C.POINTER(sfx_mesh_desc), C.POINTER(C.c_void_p)]),
+    "sfx_mesh_check": (C.c_int, [C.POINTER(sfx_mesh_desc), C.c_int32]),
     "sfx_mesh_free": (C.c_int, [C.c_void_p]),
     "sfx_mesh_device_bytes": (C.c_int64, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
     "sfx_state_upload_W": (C.c_int, [C.c_void_p, _dp]),

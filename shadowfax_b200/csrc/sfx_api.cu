@@ -391,11 +391,14 @@ int64_t sfx_mesh_device_bytes(int32_t dim, int32_t n_cells, int32_t n_faces,
     return bytes;
 }
 
-int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
-    if(!ctx || !desc || !out) return SFX_ERR_INVALID;
-    *out = nullptr;
+namespace {
+
+/* The host checks of a face list (sfx_mesh_check, and sfx_mesh_upload before
+ * it allocates anything): every index a kernel will dereference, so device
+ * code needs no bounds checks on mesh indices, and the one geometric
+ * condition the split kernels rely on. */
+int check_desc(const sfx_mesh_desc* desc, int precision) {
     const int dim = desc->dim;
-    if(dim != ctx->cfg.dim) return SFX_ERR_INVALID;
     const int64_t n = desc->n_cells, F = desc->n_faces;
     if(n <= 0 || F < 0) return SFX_ERR_INVALID;
     if(!desc->cell_pos || !desc->cell_centroid || !desc->cell_volume ||
@@ -403,12 +406,10 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
        (F && (!desc->face_area || !desc->face_midpoint || !desc->face_left ||
               !desc->face_right || !desc->face_kind || !desc->face_right_pos)))
         return SFX_ERR_INVALID;
-    /* validate every index the kernels will dereference */
     const int32_t* off = desc->cell_face_offset;
     if(off[0] != 0) return SFX_ERR_BOUNDS;
     for(int64_t i = 0; i < n; ++i)
         if(off[i + 1] < off[i]) return SFX_ERR_BOUNDS;
-    const int64_t nnz = off[n];
     for(int64_t f = 0; f < F; ++f) {
         int L = desc->face_left[f], R = desc->face_right[f], k = desc->face_kind[f];
         if(L < 0 || L >= n) return SFX_ERR_BOUNDS;
@@ -418,6 +419,49 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
             return SFX_ERR_BOUNDS;
         }
     }
+    /* a cell lists the faces it owns and the real faces it is the right side of */
+    for(int64_t i = 0; i < n; ++i)
+        for(int64_t j = off[i]; j < off[i + 1]; ++j) {
+            const int32_t f = desc->cell_face_index[j];
+            if(f < 0 || f >= F) return SFX_ERR_BOUNDS;
+            if(desc->face_left[f] != i &&
+               !(desc->face_right[f] == i && desc->face_kind[f] == SFX_FACE_REAL))
+                return SFX_ERR_BOUNDS;
+        }
+    if(precision == SFX_PREC_SPLIT) {
+        /* the split kernels apply a periodic image's offset as one whole unit
+         * box per axis (a code per axis: 0, +1 or -1); a mesh of another box
+         * is refused rather than computed with the wrong offset */
+        for(int64_t f = 0; f < F; ++f) {
+            if(desc->face_kind[f] != SFX_FACE_PERIODIC) continue;
+            for(int l = 0; l < dim; ++l) {
+                const double a = std::fabs(desc->face_right_pos[f * dim + l] -
+                                           desc->cell_pos[(int64_t)desc->face_right[f] * dim + l]);
+                if(!(a <= 1e-9 || std::fabs(a - 1.) <= 1e-9)) return SFX_ERR_UNSUPPORTED;
+            }
+        }
+    }
+    return SFX_OK;
+}
+
+}  // namespace
+
+int sfx_mesh_check(const sfx_mesh_desc* desc, int32_t precision) {
+    if(!desc || (desc->dim != 2 && desc->dim != 3) ||
+       (precision != SFX_PREC_FP64 && precision != SFX_PREC_SPLIT))
+        return SFX_ERR_INVALID;
+    return check_desc(desc, precision);
+}
+
+int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
+    if(!ctx || !desc || !out) return SFX_ERR_INVALID;
+    *out = nullptr;
+    const int dim = desc->dim;
+    if(dim != ctx->cfg.dim) return SFX_ERR_INVALID;
+    SFX_TRY(check_desc(desc, ctx->cfg.precision));
+    const int64_t n = desc->n_cells, F = desc->n_faces;
+    const int32_t* off = desc->cell_face_offset;
+    const int64_t nnz = off[n];
     std::vector<int32_t> idx(nnz);
     for(int64_t i = 0; i < n; ++i) {
         for(int64_t j = off[i]; j < off[i + 1]; ++j) {
@@ -469,17 +513,6 @@ int sfx_mesh_upload(sfx_ctx* ctx, const sfx_mesh_desc* desc, sfx_mesh** out) {
     std::vector<uint8_t> skip;
     std::vector<int32_t> idx_split;
     if(ctx->cfg.precision == SFX_PREC_SPLIT) {
-        /* the split kernels apply a periodic image's offset as one whole unit
-         * box per axis (a code per axis: 0, +1 or -1); a mesh of another box
-         * is refused rather than computed with the wrong offset */
-        for(int64_t f = 0; f < F; ++f) {
-            if(desc->face_kind[f] != SFX_FACE_PERIODIC) continue;
-            for(int l = 0; l < dim; ++l) {
-                const double a = std::fabs(desc->face_right_pos[f * dim + l] -
-                                           desc->cell_pos[(int64_t)desc->face_right[f] * dim + l]);
-                if(!(a <= 1e-9 || std::fabs(a - 1.) <= 1e-9)) return SFX_ERR_UNSUPPORTED;
-            }
-        }
         skip.assign(F, 0);
         idx_split = idx;
         auto shcode = [&](int64_t f) {

@@ -111,6 +111,13 @@ class Mesh:
         return cls(dim=dim, periodic=bool(periodic),
                    **{n: z[n] for n in cls._ARRAYS}).normalized()
 
+    def check(self, precision: int = L.PREC_FP64) -> None:
+        """the checks an upload to a context of this precision makes, on the
+        host alone (sfx_mesh_check); raises SfxError with the status the
+        upload would return"""
+        d = self.desc()
+        L.check(L.lib().sfx_mesh_check(C.byref(d), int(precision)), "sfx_mesh_check")
+
     def write_file(self, path: str | Path) -> None:
         """the library's versioned binary mesh file (sfx_meshfile_write)"""
         L.check(L.lib().sfx_meshfile_write(str(path).encode(), C.byref(self.desc()),
