@@ -5,7 +5,8 @@ own CPU flux-pass results on them (oracle/_ref/refharness_*, the unmodified
 Shadowfax sources), with both glibc pow and sfx_pow, plus the reference
 solvers' outputs on Riemann state pairs, and one step with moving generators
 (the reference built without -DSTATIC; ``--moving`` makes only those) and
-one system step of local time steps (``--local``).  They
+one system step of local time steps (``--local``), and the pass and solvers
+at gamma = 1.4 (``--gamma``).  They
 let the CPU test suite pin the oracle restatement on machines without the
 reference tree.
 """
@@ -223,12 +224,61 @@ def main():
         print("wrote riemann", dim)
 
 
+GAMMA_ALT = 1.4
+
+
+def gamma_cases():
+    """the pass at another adiabatic index than the factory default (the
+    solvers' gamma-dependent constants, get_Q/get_W's energy)"""
+    import dataclasses
+    yield "gamma14_sod2d_exact", dataclasses.replace(
+        wl.sod2d(n=400, nsteps=8, solver="Exact"), gamma=GAMMA_ALT)
+    yield "gamma14_random3d_hllc", dataclasses.replace(
+        wl.random_field3d(n=300, nsteps=2, solver="HLLC"), gamma=GAMMA_ALT)
+    yield "gamma14_random3d_exact", dataclasses.replace(
+        wl.random_field3d(n=300, nsteps=2, solver="Exact"), gamma=GAMMA_ALT)
+
+
+def main_gamma():
+    """tests/golden/gamma14_*.npz and riemann_gamma14_{2,3}d.npz: the
+    reference's pass and solvers at gamma = 1.4"""
+    for name, pr in gamma_cases():
+        out = {}
+        for powk in ("libm", "sfxpow"):
+            p = Params(solver=pr.solver, gamma=pr.gamma)
+            r = run_reference(pr.mesh, p, pr.dt, pr.nsteps, pr.W0, pow_kind=powk)
+            assert r["status"] == 0 and r["steps"] == pr.nsteps, (name, r["status"])
+            for key in ("W", "Q", "grad", "dQ"):
+                out[f"ref_{powk}_{key}"] = r[key]
+        m = pr.mesh
+        np.savez_compressed(
+            OUT / f"{name}.npz", dim=m.dim, periodic=int(m.periodic), solver=pr.solver,
+            gamma=pr.gamma, dt=pr.dt, nsteps=pr.nsteps, W0=pr.W0,
+            **{a: getattr(m, a) for a in m._ARRAYS}, **out)
+        print("wrote", name, m.n_cells, m.n_faces)
+    for dim in (2, 3):
+        WL, WR, nrm = riemann_pairs(dim, 200, 200 + dim)
+        out = dict(WL=WL, WR=WR, normal=nrm, gamma=GAMMA_ALT)
+        for solver in ("Exact", "HLLC"):
+            for powk in ("libm", "sfxpow"):
+                r = riemann_reference(dim, Params(solver=solver, gamma=GAMMA_ALT), WL, WR, nrm,
+                                      pow_kind=powk)
+                out[f"{solver}_{powk}_status"] = r["status"]
+                out[f"{solver}_{powk}_half"] = r["half"]
+                out[f"{solver}_{powk}_flux"] = r["flux"]
+        np.savez_compressed(OUT / f"riemann_gamma14_{dim}d.npz", **out)
+        print("wrote riemann gamma 1.4", dim)
+
+
 if __name__ == "__main__":
     if "--moving" in sys.argv:
         main_moving()
     elif "--local" in sys.argv:
         main_local()
+    elif "--gamma" in sys.argv:
+        main_gamma()
     else:
         main()
         main_moving()
         main_local()
+        main_gamma()

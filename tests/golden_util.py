@@ -15,6 +15,8 @@ LOCAL_CASES = [f"local_{d}d_{s}" for d in (2, 3) for s in ("exact", "hllc")]
 # meshes the reference's own DelTess/VorTess built (tests/golden/make_reftess.py)
 REFTESS_CASES = ["reftess_sod2d_reflective_exact", "reftess_random2d_periodic_hllc",
                  "reftess_sedov3d_reflective_hllc", "reftess_random3d_periodic_exact"]
+# the pass at gamma = 1.4 (the factory default is 5/3): oracle pins on the CPU
+GAMMA_CASES = ["gamma14_sod2d_exact", "gamma14_random3d_hllc", "gamma14_random3d_exact"]
 MESH_CASES = ["sod2d_exact", "sod2d_hllc", "sedov3d_hllc", "random3d_exact",
               "random2d_periodic_exact"]
 

@@ -4,8 +4,9 @@ and against the reference's Riemann-solver unit-test vectors."""
 import numpy as np
 import pytest
 
-from golden_util import (MESH_CASES, MOVING_CASES, MOVING_FAILS, TORO_HALF_STATES,
-                         assert_values_equal, load_case, load_riemann, toro_pairs)
+from golden_util import (GAMMA_CASES, GOLDEN, MESH_CASES, MOVING_CASES, MOVING_FAILS,
+                         TORO_HALF_STATES, assert_values_equal, load_case, load_riemann,
+                         toro_pairs)
 from oracle.oracle import Params
 
 
@@ -18,6 +19,33 @@ def test_oracle_matches_reference_bitwise(oracle, name, powk):
     assert out["status"] == 0 and out["steps"] == meta["nsteps"]
     for key in ("W", "Q", "grad", "dQ"):
         np.testing.assert_array_equal(out[key], ref[f"ref_{powk}_{key}"], err_msg=key)
+
+
+@pytest.mark.parametrize("name", GAMMA_CASES)
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_matches_reference_at_another_gamma(oracle, name, powk):
+    """gamma = 1.4: the solvers' gamma-dependent constants and get_Q/get_W's
+    energy, step by step as the reference forms them"""
+    mesh, meta, ref = load_case(name)
+    assert meta["gamma"] == 1.4
+    p = Params(solver=meta["solver"], gamma=meta["gamma"], use_libm_pow=(powk == "libm"))
+    out = oracle.run(mesh, p, meta["dt"], meta["nsteps"], meta["W0"])
+    assert out["status"] == 0 and out["steps"] == meta["nsteps"]
+    for key in ("W", "Q", "grad", "dQ"):
+        np.testing.assert_array_equal(out[key], ref[f"ref_{powk}_{key}"], err_msg=key)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("solver", ["Exact", "HLLC"])
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_riemann_matches_reference_at_another_gamma(oracle, dim, solver, powk):
+    z = np.load(GOLDEN / f"riemann_gamma14_{dim}d.npz")
+    p = Params(solver=solver, gamma=float(z["gamma"]), use_libm_pow=(powk == "libm"))
+    half, flux, code = oracle.riemann(dim, p, z["WL"], z["WR"], z["normal"])
+    assert np.all(code >= 0) and np.all(z[f"{solver}_{powk}_status"] == 0)
+    np.testing.assert_array_equal(flux, z[f"{solver}_{powk}_flux"])
+    if solver == "Exact":
+        np.testing.assert_array_equal(half, z[f"{solver}_{powk}_half"])
 
 
 @pytest.mark.parametrize("dim", [2, 3])
