@@ -6,7 +6,8 @@ Shadowfax sources), with both glibc pow and sfx_pow, plus the reference
 solvers' outputs on Riemann state pairs, and one step with moving generators
 (the reference built without -DSTATIC; ``--moving`` makes only those) and
 one system step of local time steps (``--local``), and the pass and solvers
-at gamma = 1.4 (``--gamma``).  They
+at gamma = 1.4 (``--gamma``) and the exact solver at another tolerance and
+cutoff (``--tolerance``).  They
 let the CPU test suite pin the oracle restatement on machines without the
 reference tree.
 """
@@ -270,6 +271,41 @@ def main_gamma():
         print("wrote riemann gamma 1.4", dim)
 
 
+TOL_ALT, CUTOFF_ALT = 1e-6, -2.0
+
+
+def main_tolerance():
+    """tests/golden/tol6_random3d_exact.npz and riemann_tol6_{2,3}d.npz: the
+    exact solver at another tolerance and Newton-only cutoff than the factory
+    defaults (1e-8, -5), which moves the Newton-only/Newton/Brent choice and
+    the point where the iteration stops"""
+    pr = wl.random_field3d(n=300, nsteps=2, solver="Exact")
+    out = {}
+    for powk in ("libm", "sfxpow"):
+        p = Params(solver="Exact", gamma=pr.gamma, tolerance=TOL_ALT, cutoff=CUTOFF_ALT)
+        r = run_reference(pr.mesh, p, pr.dt, pr.nsteps, pr.W0, pow_kind=powk)
+        assert r["status"] == 0 and r["steps"] == pr.nsteps, r["status"]
+        for key in ("W", "Q", "grad", "dQ"):
+            out[f"ref_{powk}_{key}"] = r[key]
+    m = pr.mesh
+    np.savez_compressed(
+        OUT / "tol6_random3d_exact.npz", dim=m.dim, periodic=int(m.periodic), solver="Exact",
+        gamma=pr.gamma, tolerance=TOL_ALT, cutoff=CUTOFF_ALT, dt=pr.dt, nsteps=pr.nsteps,
+        W0=pr.W0, **{a: getattr(m, a) for a in m._ARRAYS}, **out)
+    print("wrote tol6_random3d_exact", m.n_cells, m.n_faces)
+    for dim in (2, 3):
+        WL, WR, nrm = riemann_pairs(dim, 200, 300 + dim)
+        out = dict(WL=WL, WR=WR, normal=nrm, tolerance=TOL_ALT, cutoff=CUTOFF_ALT)
+        for powk in ("libm", "sfxpow"):
+            r = riemann_reference(dim, Params(solver="Exact", tolerance=TOL_ALT, cutoff=CUTOFF_ALT),
+                                  WL, WR, nrm, pow_kind=powk)
+            out[f"Exact_{powk}_status"] = r["status"]
+            out[f"Exact_{powk}_half"] = r["half"]
+            out[f"Exact_{powk}_flux"] = r["flux"]
+        np.savez_compressed(OUT / f"riemann_tol6_{dim}d.npz", **out)
+        print("wrote riemann tolerance 1e-6", dim)
+
+
 if __name__ == "__main__":
     if "--moving" in sys.argv:
         main_moving()
@@ -277,8 +313,11 @@ if __name__ == "__main__":
         main_local()
     elif "--gamma" in sys.argv:
         main_gamma()
+    elif "--tolerance" in sys.argv:
+        main_tolerance()
     else:
         main()
         main_moving()
         main_local()
         main_gamma()
+        main_tolerance()

@@ -48,6 +48,40 @@ def test_oracle_riemann_matches_reference_at_another_gamma(oracle, dim, solver, 
         np.testing.assert_array_equal(half, z[f"{solver}_{powk}_half"])
 
 
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_matches_reference_at_another_tolerance(oracle, powk):
+    """the exact solver at tolerance 1e-6 and cutoff -2 (defaults 1e-8, -5)"""
+    mesh, meta, ref = load_case("tol6_random3d_exact")
+    z = np.load(GOLDEN / "tol6_random3d_exact.npz")
+    p = Params(solver="Exact", gamma=meta["gamma"], tolerance=float(z["tolerance"]),
+               cutoff=float(z["cutoff"]), use_libm_pow=(powk == "libm"))
+    out = oracle.run(mesh, p, meta["dt"], meta["nsteps"], meta["W0"])
+    assert out["status"] == 0 and out["steps"] == meta["nsteps"]
+    for key in ("W", "Q", "grad", "dQ"):
+        np.testing.assert_array_equal(out[key], ref[f"ref_{powk}_{key}"], err_msg=key)
+    # the parameters matter: the defaults end elsewhere
+    out0 = oracle.run(mesh, Params(solver="Exact", gamma=meta["gamma"],
+                                   use_libm_pow=(powk == "libm")),
+                      meta["dt"], meta["nsteps"], meta["W0"])
+    assert np.any(out0["Q"] != out["Q"])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("powk", ["sfxpow", "libm"])
+def test_oracle_riemann_matches_reference_at_another_tolerance(oracle, dim, powk):
+    z = np.load(GOLDEN / f"riemann_tol6_{dim}d.npz")
+    p = Params(solver="Exact", tolerance=float(z["tolerance"]), cutoff=float(z["cutoff"]),
+               use_libm_pow=(powk == "libm"))
+    half, flux, code = oracle.riemann(dim, p, z["WL"], z["WR"], z["normal"])
+    assert np.all(code >= 0) and np.all(z[f"Exact_{powk}_status"] == 0)
+    np.testing.assert_array_equal(flux, z[f"Exact_{powk}_flux"])
+    np.testing.assert_array_equal(half, z[f"Exact_{powk}_half"])
+    # the parameters matter: the defaults give other fluxes on some pairs
+    _, flux0, _ = oracle.riemann(dim, Params(solver="Exact", use_libm_pow=(powk == "libm")),
+                                 z["WL"], z["WR"], z["normal"])
+    assert np.any(flux0 != flux)
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 @pytest.mark.parametrize("solver", ["Exact", "HLLC"])
 @pytest.mark.parametrize("powk", ["sfxpow", "libm"])
