@@ -128,3 +128,21 @@ def test_split_takes_periodic_meshes_of_the_unit_box_only(periodic2d):
     refl = build_voronoi(random_generators(300, 2, 5), periodic=False)
     big_refl = _with(refl, cell_pos=refl.cell_pos * 2., face_right_pos=refl.face_right_pos * 2.)
     assert _status(big_refl, L.PREC_SPLIT) == 0
+
+
+def test_empty_and_ragged_face_lists():
+    """no faces at all (one isolated cell, every face array empty) is a valid
+    face list; so is one whose cells list very different numbers of faces"""
+    one = Mesh(dim=2, periodic=False, cell_pos=np.array([[0.5, 0.5]]),
+               cell_centroid=np.array([[0.5, 0.5]]), cell_volume=np.array([1.0]),
+               cell_total_area=np.array([4.0]), cell_face_offset=np.array([0, 0], np.int32),
+               cell_face_index=np.zeros(0, np.int32), face_area=np.zeros(0),
+               face_midpoint=np.zeros((0, 2)), face_left=np.zeros(0, np.int32),
+               face_right=np.zeros(0, np.int32), face_kind=np.zeros(0, np.int32),
+               face_right_pos=np.zeros((0, 2))).normalized()
+    for precision in (L.PREC_FP64, L.PREC_SPLIT):
+        assert _status(one, precision) == 0
+    m = build_voronoi(random_generators(300, 3, 9), periodic=False)
+    counts = np.diff(m.cell_face_offset)
+    assert counts.min() < counts.max()     # ragged by construction
+    assert _status(m, L.PREC_SPLIT) == 0
