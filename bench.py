@@ -809,8 +809,6 @@ def split_traffic(role: str, dim: int, solver: str, faces: int):
     return TRAFFIC_B_PER_FACE[key] * faces if key in TRAFFIC_B_PER_FACE else None
 
 
-
-
 def resident_roofline(pool, reqs, inst, classes, cctx):
     """per-kernel device times of every class (all of its requests in one
     launch group, CUDA events around each launch): the dominant kernel of the
