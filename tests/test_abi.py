@@ -145,3 +145,58 @@ def test_noalloc_pass_checks_its_arguments_before_any_device_call():
     assert call(mesh(), cfg, dt=0.0) == L.SFX_ERR_INVALID
     assert call(mesh(), cfg, W=None) == L.SFX_ERR_INVALID
     assert call(mesh(n_cells=0), cfg) == L.SFX_ERR_INVALID
+
+
+C_HOST = r"""
+#include <stdio.h>
+#include <string.h>
+#include "sfxflux.h"
+
+int main(void) {
+    double pos[2] = {0.5, 0.5}, cen[2] = {0.5, 0.5}, vol = 1.0, tarea = 4.0;
+    int32_t off[2] = {0, 0}, idx[1] = {0};
+    sfx_mesh_desc d;
+    memset(&d, 0, sizeof d);
+    d.dim = 2;
+    d.n_cells = 1;
+    d.n_faces = 0;
+    d.cell_pos = pos;
+    d.cell_centroid = cen;
+    d.cell_volume = &vol;
+    d.cell_total_area = &tarea;
+    d.cell_face_offset = off;
+    d.cell_face_index = idx;
+    int ok = sfx_mesh_check(&d, SFX_PREC_FP64);
+    d.cell_face_offset = NULL;
+    int bad = sfx_mesh_check(&d, SFX_PREC_FP64);
+    printf("%s|%d|%d\n", sfx_version(), ok, bad);
+    return !(ok == SFX_OK && bad == SFX_ERR_INVALID);
+}
+"""
+
+
+def test_a_c_host_links_and_calls_the_library(tmp_path):
+    """the boundary as a C or cgo host sees it: the header compiles as strict
+    C99 and C++11, and a C program linked against the shared library calls
+    it (host-only entry points: no GPU here)"""
+    import shutil
+    import subprocess
+    from shadowfax_b200 import _lib as L
+    if shutil.which("gcc") is None or shutil.which("g++") is None:
+        pytest.skip("no C compiler")
+    L.lib()   # the library is built
+    inc, libdir = ROOT / "include", ROOT / "shadowfax_b200"
+    src = tmp_path / "host.c"
+    src.write_text(C_HOST)
+    exe = tmp_path / "host"
+    cmd = ["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", f"-I{inc}", str(src),
+           f"-L{libdir}", "-lsfxflux", f"-Wl,-rpath,{libdir}", "-o", str(exe)]
+    subprocess.run(cmd, check=True, capture_output=True)
+    cpp = tmp_path / "host.cpp"
+    cpp.write_text('#include "sfxflux.h"\nint main() { return sizeof(sfx_mesh_desc) == 0; }\n')
+    subprocess.run(["g++", "-std=c++11", "-Wall", "-Werror", "-pedantic", f"-I{inc}", "-c",
+                    str(cpp), "-o", str(tmp_path / "host_cpp.o")], check=True, capture_output=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    version, ok, bad = r.stdout.strip().split("|")
+    assert version.startswith("sfxflux") and int(ok) == 0 and int(bad) == L.SFX_ERR_INVALID
