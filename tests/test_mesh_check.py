@@ -146,3 +146,64 @@ def test_empty_and_ragged_face_lists():
     counts = np.diff(m.cell_face_offset)
     assert counts.min() < counts.max()     # ragged by construction
     assert _status(m, L.PREC_SPLIT) == 0
+
+
+def _expected_status(m, split):
+    """the face-list rules, stated independently of the library"""
+    n, F = m.n_cells, m.n_faces
+    off, idx = m.cell_face_offset, m.cell_face_index
+    if off[0] != 0 or np.any(np.diff(off) < 0):
+        return L.SFX_ERR_BOUNDS
+    L_, R_, K_ = m.face_left, m.face_right, m.face_kind
+    if np.any((L_ < 0) | (L_ >= n)) or np.any(~np.isin(K_, [0, 1, 2])):
+        return L.SFX_ERR_BOUNDS
+    has_r = (K_ == 0) | (K_ == 1)
+    if np.any(has_r & ((R_ < 0) | (R_ >= n))):
+        return L.SFX_ERR_BOUNDS
+    if off[-1] > len(idx):
+        return None                        # the arrays themselves are too short: not fuzzed
+    for i in range(n):
+        for j in range(off[i], off[i + 1]):
+            f = idx[j]
+            if f < 0 or f >= F:
+                return L.SFX_ERR_BOUNDS
+            if L_[f] != i and not (R_[f] == i and K_[f] == 0):
+                return L.SFX_ERR_BOUNDS
+    if split:
+        per = np.flatnonzero(K_ == 1)
+        a = np.abs(m.face_right_pos[per] - m.cell_pos[R_[per]])
+        if np.any(~((a <= 1e-9) | (np.abs(a - 1.0) <= 1e-9))):
+            return L.SFX_ERR_UNSUPPORTED
+    return 0
+
+
+def test_random_corruptions_get_the_rules_status(periodic2d):
+    m0 = periodic2d
+    rng = np.random.Generator(np.random.PCG64(77))
+    fields = ["face_left", "face_right", "face_kind", "cell_face_index", "cell_face_offset",
+              "face_right_pos"]
+    seen = set()
+    for trial in range(150):
+        arrays = {}
+        for _ in range(int(rng.integers(1, 3))):
+            name = fields[int(rng.integers(len(fields)))]
+            a = arrays.get(name, getattr(m0, name)).copy()
+            k = int(rng.integers(a.shape[0]))
+            if name == "face_right_pos":
+                a[k, int(rng.integers(a.shape[1]))] += rng.choice([0.5, 1.0, 1e-12, 2.0])
+            elif name == "cell_face_offset":
+                if k == len(a) - 1:
+                    k -= 1          # the last offset sizes the index array itself
+                a[k] += int(rng.integers(-3, 4))
+            else:
+                a[k] = int(rng.integers(-2, max(m0.n_cells, m0.n_faces) + 2))
+            arrays[name] = a
+        m = _with(m0, **arrays)
+        for split in (False, True):
+            want = _expected_status(m, split)
+            if want is None:
+                continue
+            got = _status(m, L.PREC_SPLIT if split else L.PREC_FP64)
+            assert got == want, (trial, split, sorted(arrays), got, want)
+            seen.add(want)
+    assert seen == {0, L.SFX_ERR_BOUNDS, L.SFX_ERR_UNSUPPORTED}
